@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the lomacte RK3 step on B200 (Mpts.RK3-steps/s).
+
+Workload (default): nx = nz = 256 Fourier modes (3/2 dealiased: mgalx =
+mgalz = 384), ny = 257 on y = 12 sinh(2 eta)/sinh(2), FP64 plain path,
+seeded initial condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed
+Deltat = 0.01.  One "step" = one full RK3 step (3 substeps).  The metric is
+(nx*ny*nz/1e6) * steps / seconds.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
+time is the max over ranks and the value the aggregate over ranks.
+``--impl reference`` times the CPU restatement of the reference algorithm
+(the reference Fortran cannot be built in this environment) on the host
+cores, on bounded samples (one RK3 substep each) of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic HBM bytes per launch, in units of the spectral (S = nplanes *
+# mz * ny complex), z-padded (Z = nplanes * mgalz * ny complex) and physical
+# (P = mgalx * mgalz * ny real) counts; w = bytes per complex value (16 in
+# FP64).  Compulsory reads + writes of each kernel:
+#   zinv : 6 spectral fields read (rho u, rho v, rho w, lap T, dT/dy, T), 8 Z written
+#   xphys: 8 Z read, 11 Z written, RHS(T) physical accumulator read + written
+#   zfwd : 11 Z read, 11 S written
+#   lapv : phi read, m_y and dm_y/dy written (+ 7 doubles/point mode tables read)
+#   assemble: vor, dm_y, psi, m_y, R_om, phi, R_phi read; rho u, rho v, rho w, vor, phi written
+#   tder : T read; T, dT/dy, lap T written
+#   post1: T, DT, rho vv, rho uv, rho vw, rho uu, rho uw, rho ww read; T, N_x, N_y, N_z written
+#   post2: u, v, w, N_x, N_y, N_z, vor, phi read; R_om, R_phi, vor, phi written
+#   psi  : drho read, psi written (+ 7 doubles/point mode tables read)
+ALGO = {
+    "zinv": lambda S, Z, P, w: 6 * S * w + 8 * Z * w,
+    "xphys": lambda S, Z, P, w: 19 * Z * w + 2 * P * 8,
+    "zfwd": lambda S, Z, P, w: 11 * Z * w + 11 * S * w,
+    "lapv": lambda S, Z, P, w: 3 * S * w + S * 7 * 8 // 2,
+    "assemble": lambda S, Z, P, w: 12 * S * w,
+    "tder": lambda S, Z, P, w: 4 * S * w,
+    "post1": lambda S, Z, P, w: 12 * S * w,
+    "post2": lambda S, Z, P, w: 12 * S * w,
+    "psi": lambda S, Z, P, w: 2 * S * w + S * 7 * 8 // 2,
+}
+# Kernel launches per RK3 step (3 substeps x 9 kernels).
+LAUNCHES_PER_STEP = 27
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=257)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--json-only", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        try:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+        except Exception:
+            pass
+        try:
+            rows = [l.strip().split(",") for l in open(self.path) if l.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+def mpts(a):
+    return a.nx * a.ny * a.nz / 1e6
+
+
+def sizes(p):
+    S = p.nplanes * p.mz * p.my
+    Z = p.nplanes * p.mgalz * p.my
+    P = p.mgalx * p.mgalz * p.my
+    return S, Z, P
+
+
+def cpu_baseline(a, p, y, st):
+    """The FP64 CPU restatement (oracle) on the host cores: a bounded sample
+    of the same workload (one RK3 substep), scaled to steps."""
+    from oracle.oracle import Oracle
+    nth = os.cpu_count() or 1
+    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=p.dt_mode, dt0=p.dt, nthreads=nth)
+    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    t0 = time.perf_counter()
+    o.substep(0)
+    dt = time.perf_counter() - t0
+    steps = 1.0 / 3.0
+    return {"value": mpts(a) * steps / dt, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port",
+            "sample": f"one RK3 substep of the {a.nx}x{a.ny}x{a.nz} workload ({dt:.2f} s), FP64 CPU "
+                      f"restatement of cross.f:307-1141 with OpenMP ({nth} threads)"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from loma_phd_b200 import ICParams, Params, make_ic, stretched_mesh
+    from oracle.oracle import Oracle
+    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01)
+    y = stretched_mesh(p.my)
+    st = make_ic(p, y, ICParams(s=4.0, seed=0))
+    nth = os.cpu_count() or 1
+    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=1, dt0=0.01, nthreads=nth)
+    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    for _ in range(a.warmup):
+        o.substep(0)
+    t0 = time.perf_counter()
+    for k in range(a.steps):
+        o.substep(k % 3)
+    dt = time.perf_counter() - t0
+    steps = a.steps / 3.0
+    val = mpts(a) * steps / dt
+    line = {
+        "impl": "reference", "metric": "Mpts*RK3-steps/s", "value": val, "unit": "Mpts*RK3-steps/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded initial condition)",
+        "config": {"workload": f"lomacte FP64 {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
+                   "sample": "each step = one RK3 substep", "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": val, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port",
+                         "sample": f"{a.steps} RK3 substeps of the workload, FP64 CPU restatement "
+                                   f"(the Fortran reference cannot be compiled here), {nth} threads"},
+        "e2e": {"value": val, "unit": "Mpts*RK3-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    from loma_phd_b200 import ICParams, Lomacte, Params, make_ic, stretched_mesh
+    from loma_phd_b200.lomacte import KERNEL_NAMES
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev)
+    y = stretched_mesh(p.my)
+    st = make_ic(p, y, ICParams(s=4.0, seed=rank))
+    g = Lomacte(p, y)
+    g.load_state(st)
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        g.step(1)
+    g.sync()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    g.profile_start()
+    e0.record(stream)
+    g.step(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    prof = g.profile_read()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    secs = ms / 1e3
+    value = mpts(a) * a.steps * world / secs
+    diag = g.diag()
+    if not np.isfinite(diag["dm"]):
+        raise RuntimeError("non-finite diagnostics after the timed steps")
+
+    # end-to-end through the public API with host buffers: every step loads
+    # the state from pinned host memory, advances one RK3 step and reads the
+    # state back.
+    e2e = None
+    if not a.no_e2e:
+        S, Z, P = sizes(p)
+        host = {k: torch.from_numpy(np.ascontiguousarray(st[k]).view(np.float64).copy()).pin_memory()
+                for k in ("vor", "phi", "psi", "scal")}
+        h00 = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64).copy()).pin_memory()
+               for k in ("u00", "v00", "w00")}
+        ptrs = [host[k].data_ptr() for k in ("vor", "phi", "psi", "scal")] + \
+               [h00[k].data_ptr() for k in ("u00", "v00", "w00")]
+        ne = max(1, min(a.steps, 5))
+        for _ in range(2):
+            g.load_state_ptrs(*ptrs)
+            g.step(1)
+            g.get_state_ptrs(*ptrs)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne):
+            g.load_state_ptrs(*ptrs)
+            g.step(1)
+            g.get_state_ptrs(*ptrs)
+        el = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([el], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        nbytes = 4 * S * 16 + 3 * p.my * 8
+        e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
+
+    # roofline of the dominant kernel, live CUDA-event times of the timed region
+    S, Z, P = sizes(p)
+    top = max((k for k in KERNEL_NAMES if k in ALGO), key=lambda k: prof[k][0])
+    tot_ms, cnt = prof[top]
+    avg_s = tot_ms / max(cnt, 1) / 1e3
+    algo = ALGO[top](S, Z, P, 16)
+    peak, kind = peaks()
+    achieved = algo / avg_s / 1e9
+    share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES}
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a, p, y, st)
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": "Mpts*RK3-steps/s", "value": value, "unit": "Mpts*RK3-steps/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded initial condition)",
+            "config": {"workload": f"lomacte FP64 plain path {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), "
+                                   f"s=4, Re=160, dt=0.01", "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (
+                           3 * sum(f(S, Z, P, 16) for f in ALGO.values()) / 1e9)},
+            "gpu_launches": LAUNCHES_PER_STEP * a.steps,
+            "clocks": ck, "roofline": roofline, "kernel_share": share,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

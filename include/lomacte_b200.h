@@ -1,0 +1,156 @@
+/*
+ * lomacte_b200.h -- C ABI of the B200-native lomacte substep library
+ * (liblomacte_b200.so).
+ *
+ * The library replaces the time loop of the reference Fortran subroutine
+ * cross1 (Beovulfo/LoMa_phD trunk/lomacte3/src/cross.f:24-45, called once
+ * from trunk/lomacte3/src/main.f:215) with a device-resident RK3 stepper.
+ * Every entry point returns an int status (LMC_OK = 0, < 0 on error); no
+ * C++ exception crosses this boundary.  Arrays are plain host or device
+ * pointers with sizes implied by the grid; no torch types appear here.
+ *
+ * Grid conventions follow trunk/lomacte3/src/ctes3D:18-36:
+ *   mx = 2*(mgalx/3), nplanes = mx/2 (kx planes), mz = 2*(mgalz/3)-1 (kz
+ *   modes, kz = 0..nz1, -nz1..-1 with nz1 = (mz-1)/2), my points in y.
+ * Spectral fields use the reference layout vor(0:my-1, 0:mz-1, 1:nplanes):
+ *   complex values (re, im interleaved), y fastest, then kz, then kx plane.
+ * One handle = one case = one CUDA stream; calls on one handle must come
+ * from one host thread at a time.
+ */
+#ifndef LOMACTE_B200_H
+#define LOMACTE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  LMC_OK = 0,
+  LMC_EINVAL = -1,   /* bad argument or grid */
+  LMC_ENOMEM = -2,   /* device allocation failed */
+  LMC_ENAN = -3,     /* non-finite value detected in the state */
+  LMC_ETIMEOUT = -4, /* a bounded device wait gave up */
+  LMC_ECUDA = -5,    /* CUDA runtime error */
+  LMC_ENODEV = -6    /* no CUDA device (the library has no CPU path) */
+};
+
+/* Run parameters: the hre.dat records parsed by initcr
+ * (trunk/lomacte3/src/main.f:502-570) plus the build's own switches. */
+typedef struct lmc_params {
+  int mgalx, mgalz, my; /* physical grid (ctes3D:18-20) */
+  double Re, alp, bet;  /* hre.dat line 1 (main.f:506,555-557) */
+  double peclet;        /* <= 0: Re*0.7f as main.f:569 */
+  double cfl;           /* hre.dat CFL (main.f:517,560) */
+  int ncfl;             /* steps between CFL updates (main.f:564) */
+  int dt_mode;          /* 0: reference CFL mode, 1: fixed Deltat */
+  double dt;            /* initial Deltat (reference: 1e-4, main.f:559) or the fixed Deltat */
+  int precision;        /* 0: FP64 (the plain path) */
+  int device;           /* CUDA device ordinal */
+} lmc_params;
+
+/* Per-step diagnostics (the .cf record of cross.f:1172-1176 without the
+ * stats-only energies). */
+typedef struct lmc_diag {
+  double time;        /* time at the start of the step */
+  double Deltat;      /* Deltat used by the step */
+  double dm;          /* momentum thickness (cross.f:1416-1429) */
+  double dw;          /* vorticity thickness (cross.f:692-699) */
+  double Redw;        /* Re*dw */
+  double trapz;       /* -int d(rho)/dt dy (cross.f:1046) */
+  double masst;       /* int <rho>_xz dy (escru.f:372-376) */
+  double massu, massv, massw; /* int rho u_i,00 dy (cross.f:1013-1020) */
+  double H00u, H00w;  /* 0.25 int RHS(u00), RHS(w00) dy (cross.f:713-722) */
+  double Deltat_next; /* Deltat of the next step */
+  int step;           /* steps taken by the handle */
+  int status;         /* device status word (0 ok) */
+} lmc_diag;
+
+typedef struct lmc_handle lmc_handle;
+
+/* Create a case: coefficients (cfdiff.f derivadas), wavenumbers, per-mode
+ * Poisson factors, device buffers and the stream.  y has my entries.
+ * Replaces initcr's grid set-up (main.f:461-800) and cross1's set-up
+ * (cross.f:125-220). */
+int lmc_create(const lmc_params *p, const double *y, lmc_handle **out);
+int lmc_destroy(lmc_handle *h);
+
+/* Load the state (getfil, main.f:329-455, then cross.f:211-215,276-280).
+ * FP64 variant: complex*16 fields in the reference layout.  FP32 variant:
+ * complex*8 fields exactly as the restart file stores them.  Both zero
+ * the RK3 memory (main.f:171-174). */
+int lmc_load_state_f64(lmc_handle *h, const double *vor, const double *phi,
+                       const double *psi, const double *scal,
+                       const double *u00, const double *v00,
+                       const double *w00, double time);
+int lmc_load_state_f32(lmc_handle *h, const float *vor, const float *phi,
+                       const float *psi, const float *scal, const double *u00,
+                       const double *v00, const double *w00, double time);
+/* Read the state back (for escru, escru.f:11-193).  NULL pointers skip. */
+int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi,
+                      double *scal, double *u00, double *v00, double *w00,
+                      double *time);
+int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi,
+                      float *scal, double *u00, double *v00, double *w00,
+                      double *time);
+
+/* Advance nsteps full RK3 steps (the body of cross.f:225-1226, 3
+ * substeps of cross.f:307-1141 each).  Asynchronous on the handle's
+ * stream; Deltat is computed on the device. */
+int lmc_step(lmc_handle *h, int nsteps);
+int lmc_sync(lmc_handle *h);
+/* Diagnostics of the last completed step (synchronises). */
+int lmc_get_diag(lmc_handle *h, lmc_diag *d);
+/* Device status word (0 ok, else an LMC_E* code); synchronises. */
+int lmc_status(lmc_handle *h);
+const char *lmc_strerror(int code);
+
+/* The handle's CUDA stream (cudaStream_t as void*) and device pointers of
+ * the state, for zero-copy use by a host framework. */
+void *lmc_stream(lmc_handle *h);
+int lmc_state_device_ptrs(lmc_handle *h, double **vor, double **phi,
+                          double **psi, double **scal);
+
+/* Per-kernel timing with CUDA events on the handle's stream.  After
+ * lmc_profile_start every lmc_step records an event before each kernel;
+ * lmc_profile_read synchronises, returns the summed milliseconds and the
+ * launch counts per kernel id and stops recording.  Kernel ids:
+ *   0 lapv (Lapvdvhom), 1 assemble (rho u_i), 2 tder (T derivatives),
+ *   3 zinv (inverse z transforms), 4 xphys (x transforms + products),
+ *   5 zfwd (direct z transforms), 6 post1 (N_i), 7 post2 (vorticity,
+ *   RHS, RK3 update), 8 psi (solvepsi + 00 modes), 9 memsets. */
+int lmc_profile_start(lmc_handle *h);
+int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count);
+
+/* Seeded initial condition (host only, no GPU): the structure of the
+ * reference generator trunk/initloma3/src/main.f:95-609 with a
+ * counter-based PRNG keyed by seed.  Mean profiles rho00 = 1 +
+ * (s-1)/(s+1) tanh(-y/(2 dm0)), T00 = 1/rho00, rho u00 = rho00 u0
+ * tanh(y/(2 dm0)); solenoidal noise on 1 <= |k| <= nkmax (mode-index
+ * units) windowed by exp(-(y/swin)^2), scaled to rms amp at y = 0. */
+typedef struct lmc_ic_params {
+  double s;     /* density ratio rho_bot/rho_top = T_top/T_bot */
+  double u0;    /* mean velocity amplitude (reference sign: negative) */
+  double dm0;   /* initial thickness scale */
+  double amp;   /* rms of the perturbation velocity at y = 0 */
+  double swin;  /* y window width */
+  int nkmax;    /* largest |k| (mode-index units) carrying noise */
+  int nymax;    /* number of random y-harmonics per mode */
+  unsigned long long seed;
+} lmc_ic_params;
+int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_params *ic,
+                double *vor, double *phi, double *psi, double *scal,
+                double *u00, double *v00, double *w00);
+
+/* Single-operator entry points on device buffers in the reference layout
+ * (all nplanes*mz modes at once), on the handle's stream:
+ *   op 1: deryr2   (cfdiff.f:518-601)   out = d in/dy
+ *   op 2: deryyr2  (cfdiff.f:735-797)   out = d2 in/dy2
+ *   op 3: Lapvdvhom (laps.f:319-477)    out = v, out2 = dv/dy
+ *   op 4: solvepsi  (laps.f:580-730)    out = psi
+ * Used by the parity tests of the y-kernels. */
+int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev,
+             double *out2_dev);
+#ifdef __cplusplus
+}
+#endif
+#endif

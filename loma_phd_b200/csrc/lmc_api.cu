@@ -1,0 +1,449 @@
+// lmc_api.cu -- C ABI of liblomacte_b200 (declared in include/lomacte_b200.h).
+//
+// One handle = one case: the tables built by lmc_host.cpp are uploaded once,
+// the state lives in device memory, and lmc_step enqueues the substep
+// kernels of lmc_kernels.cu on the handle's stream.  There is no CPU path:
+// without a CUDA device lmc_create returns LMC_ENODEV.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "lmc_internal.h"
+#include "lmc_kernels.cuh"
+
+struct lmc_handle {
+  lmc::Grid g;
+  lmc_params p;
+  lmc::YOps ops;
+  lmc::PoissonTables pt;
+  lmc::RK3 rk;
+  lmc::Dev d;
+  cudaStream_t s = nullptr;
+  std::vector<void *> allocs;
+  int steps = 0;
+  int err = 0;
+  // per-kernel CUDA-event profiling (lmc_profile_start / lmc_profile_read)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_kid;
+  size_t ev_used = 0;
+};
+
+namespace {
+
+#define LMC_CK(call)                                     \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) {                             \
+      std::fprintf(stderr, "lomacte_b200: %s:%d %s\n", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+      return e_ == cudaErrorMemoryAllocation ? LMC_ENOMEM : LMC_ECUDA; \
+    }                                                    \
+  } while (0)
+
+template <class T>
+int dalloc(lmc_handle *h, T **p, size_t n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? LMC_ENOMEM : LMC_ECUDA;
+  h->allocs.push_back(q);
+  *p = (T *)q;
+  return LMC_OK;
+}
+template <class T>
+int dupload(lmc_handle *h, const T **p, const std::vector<T> &v) {
+  T *q = nullptr;
+  int r = dalloc(h, &q, v.size());
+  if (r) return r;
+  LMC_CK(cudaMemcpy(q, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *p = q;
+  return LMC_OK;
+}
+
+bool fft_ok(int n, lmcd::FFTPlan &P) {
+  P.n = n;
+  P.nst = 0;
+  int m = n;
+  while (m % 4 == 0 && P.nst < 16) { P.rad[P.nst++] = 4; m /= 4; }
+  while (m % 2 == 0 && P.nst < 16) { P.rad[P.nst++] = 2; m /= 2; }
+  while (m % 3 == 0 && P.nst < 16) { P.rad[P.nst++] = 3; m /= 3; }
+  return m == 1;
+}
+
+std::vector<double2> twiddles(int n) {
+  std::vector<double2> t(n);
+  for (int k = 0; k < n; k++) {
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+    t[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+  }
+  return t;
+}
+
+int pick_chunks(int my, int &C, int &lpm, int &base, int &extra) {
+  static const int Cs[] = {4, 5, 7, 9, 13, 17};
+  const int need = (my + 31) / 32;
+  C = 0;
+  for (int c : Cs)
+    if (c >= need) { C = c; break; }
+  if (!C) return LMC_EINVAL;
+  lpm = (my + C - 1) / C;
+  base = my / lpm;
+  extra = my % lpm;
+  if (lpm > 32 || base < 3) return LMC_EINVAL;
+  if (!(base == C - 1 || (base == C && extra == 0))) return LMC_EINVAL;
+  return LMC_OK;
+}
+
+// Record a profiling boundary: the work enqueued after it (until the next
+// boundary) is attributed to kernel id `kid`.
+void prof_mark(lmc_handle *h, int kid) {
+  if (!h->prof) return;
+  if (h->ev_used == h->ev_pool.size()) {
+    if (h->ev_pool.size() >= 65536) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    h->ev_pool.push_back(e);
+    h->ev_kid.push_back(-1);
+  }
+  cudaEventRecord(h->ev_pool[h->ev_used], h->s);
+  h->ev_kid[h->ev_used] = kid;
+  h->ev_used++;
+}
+
+int check_launch(lmc_handle *h) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "lomacte_b200: launch failed: %s\n", cudaGetErrorString(e));
+    h->err = LMC_ECUDA;
+    return LMC_ECUDA;
+  }
+  return LMC_OK;
+}
+
+int do_load(lmc_handle *h, const double *vor, const double *phi, const double *psi, const double *scal,
+            const double *u00, const double *v00, const double *w00, double time) {
+  const lmc::Dev &d = h->d;
+  const size_t ns = (size_t)d.nmode * d.my * sizeof(double2);
+  LMC_CK(cudaSetDevice(h->p.device));
+  LMC_CK(cudaMemcpyAsync(d.vor, vor, ns, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemcpyAsync(d.phi, phi, ns, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemcpyAsync(d.psi, psi, ns, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemcpyAsync(d.scal, scal, ns, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemsetAsync(d.Rom, 0, ns, h->s));
+  LMC_CK(cudaMemsetAsync(d.Rphi, 0, ns, h->s));
+  LMC_CK(cudaMemsetAsync(d.rhst, 0, (size_t)d.my * d.mgalz * d.mgalx * sizeof(double), h->s));
+  const size_t ny = (size_t)d.my * sizeof(double);
+  LMC_CK(cudaMemcpyAsync(d.u00, u00, ny, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemcpyAsync(d.v00, v00, ny, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemcpyAsync(d.w00, w00, ny, cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemsetAsync(d.rf0u, 0, ny, h->s));
+  LMC_CK(cudaMemsetAsync(d.rf0w, 0, ny, h->s));
+  LMC_CK(cudaMemsetAsync(d.rf0v, 0, ny, h->s));
+  // Densities at the walls from the 00 mode of T (cross.f:211-213).
+  const double tb = scal[0], tt = scal[2 * (size_t)(d.my - 1)];
+  if (!(tb > 0.0) || !(tt > 0.0)) return LMC_EINVAL;
+  double sc[8] = {h->p.dt, h->p.dt, time, 1.0 / tb, 1.0 / tt, 0, 0, 0};
+  LMC_CK(cudaMemcpyAsync(d.scal_d, sc, sizeof(sc), cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaMemsetAsync(d.diag, 0, 16 * sizeof(double), h->s));
+  LMC_CK(cudaMemsetAsync(d.status, 0, sizeof(int), h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  h->steps = 0;
+  h->err = 0;
+  return LMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lmc_strerror(int code) {
+  switch (code) {
+    case LMC_OK: return "ok";
+    case LMC_EINVAL: return "invalid argument or grid";
+    case LMC_ENOMEM: return "device out of memory";
+    case LMC_ENAN: return "non-finite value in the state";
+    case LMC_ETIMEOUT: return "device wait timed out";
+    case LMC_ECUDA: return "CUDA runtime error";
+    case LMC_ENODEV: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
+  if (!p || !y || !out) return LMC_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LMC_ENODEV;
+  }
+  if (p->device < 0 || p->device >= ndev) return LMC_EINVAL;
+  if (p->precision != 0) return LMC_EINVAL;
+  lmc_handle *h = new (std::nothrow) lmc_handle();
+  if (!h) return LMC_ENOMEM;
+  h->p = *p;
+  h->g.set(p->mgalx, p->mgalz, p->my);
+  lmc::Dev &d = h->d;
+  std::memset(&d, 0, sizeof(d));
+  const lmc::Grid &g = h->g;
+  int rc = LMC_OK;
+  lmcd::FFTPlan fx{}, fz{};
+  if (g.nkx < 1 || g.mz < 1 || !fft_ok(g.mgalx, fx) || !fft_ok(g.mgalz, fz) || g.mgalx % 2) rc = LMC_EINVAL;
+  if (!rc) rc = pick_chunks(g.my, d.C, d.lpm, d.base, d.extra);
+  if (rc) { delete h; return rc; }
+  try {
+    lmc::build_yops(g.my, y, h->ops);
+  } catch (...) {
+    delete h;
+    return LMC_EINVAL;
+  }
+  std::vector<double> kx(g.nkx), kz(g.mz);
+  for (int i = 0; i < g.nkx; i++) kx[i] = p->alp * i;                         // main.f:789-792
+  for (int k = 0; k < g.mz; k++) kz[k] = p->bet * ((k <= g.nz1) ? k : k - g.mz);  // main.f:769-778
+  lmc::build_poisson(g, h->ops, kx.data(), kz.data(), h->pt);
+
+  if (cudaSetDevice(p->device) != cudaSuccess) { delete h; return LMC_ECUDA; }
+  d.my = g.my; d.mgalx = g.mgalx; d.mgalz = g.mgalz; d.nkx = g.nkx; d.mz = g.mz; d.nz1 = g.nz1; d.nmode = g.nmode;
+  d.ire = 1.0 / p->Re;
+  d.peclet = p->peclet > 0 ? p->peclet : p->Re * (double)0.7f;  // main.f:569
+  d.cfl = (double)(float)p->cfl;
+  d.hxalp = p->alp * (g.mgalx - 1) / M_PI;  // cross.f:1498
+  d.hzbet = p->bet * (g.mgalz - 1) / M_PI;  // cross.f:1499
+  for (int r = 0; r < 3; r++) {
+    d.gama[r] = h->rk.gama[r]; d.xi[r] = h->rk.xi[r]; d.alpha[r] = h->rk.alpha[r]; d.beta[r] = h->rk.beta[r];
+  }
+  const lmc::YOps &o = h->ops;
+  if ((rc = dupload(h, &d.dt12, o.dt12)) || (rc = dupload(h, &d.dt11, o.dt11)) || (rc = dupload(h, &d.dt22, o.dt22)) ||
+      (rc = dupload(h, &d.dt21, o.dt21)) || (rc = dupload(h, &d.p1L, o.p1L)) || (rc = dupload(h, &d.p1U, o.p1U)) ||
+      (rc = dupload(h, &d.p3L, o.p3L)) || (rc = dupload(h, &d.p3U, o.p3U)) || (rc = dupload(h, &d.i8L, o.i8L)) ||
+      (rc = dupload(h, &d.i8U, o.i8U)) || (rc = dupload(h, &d.fmap, o.fmap)) || (rc = dupload(h, &d.hy, o.hy)) ||
+      (rc = dupload(h, &d.trp, o.trp)) || (rc = dupload(h, &d.y, o.y)) || (rc = dupload(h, &d.ebot, o.ebot)) ||
+      (rc = dupload(h, &d.etop, o.etop)) || (rc = dupload(h, &d.PL, h->pt.L)) || (rc = dupload(h, &d.PU, h->pt.U)) ||
+      (rc = dupload(h, &d.V12, h->pt.V12)) || (rc = dupload(h, &d.AAinv, h->pt.AAinv)) ||
+      (rc = dupload(h, &d.k2, h->pt.k2)) || (rc = dupload(h, &d.kx, kx)) || (rc = dupload(h, &d.kz, kz))) {
+    lmc_destroy(h);
+    return rc;
+  }
+  // the per-mode tables are on the device now
+  h->pt = lmc::PoissonTables();
+  {
+    const double2 *tx = nullptr, *tz = nullptr;
+    if ((rc = dupload(h, &tx, twiddles(g.mgalx))) || (rc = dupload(h, &tz, twiddles(g.mgalz)))) {
+      lmc_destroy(h);
+      return rc;
+    }
+    fx.tw = tx;
+    fz.tw = tz;
+    d.fx = fx;
+    d.fz = fz;
+  }
+  const size_t ns = (size_t)g.nmode * g.my, nzp = (size_t)g.nkx * g.my * g.mgalz;
+  double2 **spec[] = {&d.vor, &d.phi, &d.psi, &d.scal, &d.Rom, &d.Rphi};
+  for (auto q : spec)
+    if ((rc = dalloc(h, q, ns))) { lmc_destroy(h); return rc; }
+  for (int f = 0; f < 11; f++)
+    if ((rc = dalloc(h, &d.sb[f], ns)) || (rc = dalloc(h, &d.zb[f], nzp))) { lmc_destroy(h); return rc; }
+  double **vec[] = {&d.u00, &d.v00, &d.w00, &d.rf0u, &d.rf0w, &d.rf0v, &d.rhom};
+  for (auto q : vec)
+    if ((rc = dalloc(h, q, (size_t)g.my))) { lmc_destroy(h); return rc; }
+  if ((rc = dalloc(h, &d.rhst, (size_t)g.my * g.mgalz * g.mgalx)) || (rc = dalloc(h, &d.scal_d, (size_t)8)) ||
+      (rc = dalloc(h, &d.cflmax, (size_t)4)) || (rc = dalloc(h, &d.diag, (size_t)16)) ||
+      (rc = dalloc(h, &d.status, (size_t)1))) {
+    lmc_destroy(h);
+    return rc;
+  }
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess || lmc::kernels_init(d) != cudaSuccess) {
+    lmc_destroy(h);
+    return LMC_ECUDA;
+  }
+  cudaMemset(d.status, 0, sizeof(int));
+  cudaMemset(d.diag, 0, 16 * sizeof(double));
+  *out = h;
+  return LMC_OK;
+}
+
+int lmc_destroy(lmc_handle *h) {
+  if (!h) return LMC_EINVAL;
+  cudaSetDevice(h->p.device);
+  if (h->s) cudaStreamSynchronize(h->s);
+  for (void *q : h->allocs) cudaFree(q);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->s) cudaStreamDestroy(h->s);
+  delete h;
+  return LMC_OK;
+}
+
+int lmc_load_state_f64(lmc_handle *h, const double *vor, const double *phi, const double *psi, const double *scal,
+                       const double *u00, const double *v00, const double *w00, double time) {
+  if (!h || !vor || !phi || !psi || !scal || !u00 || !v00 || !w00) return LMC_EINVAL;
+  return do_load(h, vor, phi, psi, scal, u00, v00, w00, time);
+}
+
+int lmc_load_state_f32(lmc_handle *h, const float *vor, const float *phi, const float *psi, const float *scal,
+                       const double *u00, const double *v00, const double *w00, double time) {
+  if (!h || !vor || !phi || !psi || !scal || !u00 || !v00 || !w00) return LMC_EINVAL;
+  const size_t n = (size_t)h->d.nmode * h->d.my * 2;
+  std::vector<double> a(n), b(n), c(n), e(n);
+  for (size_t i = 0; i < n; i++) { a[i] = vor[i]; b[i] = phi[i]; c[i] = psi[i]; e[i] = scal[i]; }
+  return do_load(h, a.data(), b.data(), c.data(), e.data(), u00, v00, w00, time);
+}
+
+int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi, double *scal, double *u00, double *v00,
+                      double *w00, double *time) {
+  if (!h) return LMC_EINVAL;
+  const lmc::Dev &d = h->d;
+  const size_t ns = (size_t)d.nmode * d.my * sizeof(double2), ny = (size_t)d.my * sizeof(double);
+  LMC_CK(cudaSetDevice(h->p.device));
+  if (vor) LMC_CK(cudaMemcpyAsync(vor, d.vor, ns, cudaMemcpyDeviceToHost, h->s));
+  if (phi) LMC_CK(cudaMemcpyAsync(phi, d.phi, ns, cudaMemcpyDeviceToHost, h->s));
+  if (psi) LMC_CK(cudaMemcpyAsync(psi, d.psi, ns, cudaMemcpyDeviceToHost, h->s));
+  if (scal) LMC_CK(cudaMemcpyAsync(scal, d.scal, ns, cudaMemcpyDeviceToHost, h->s));
+  if (u00) LMC_CK(cudaMemcpyAsync(u00, d.u00, ny, cudaMemcpyDeviceToHost, h->s));
+  if (v00) LMC_CK(cudaMemcpyAsync(v00, d.v00, ny, cudaMemcpyDeviceToHost, h->s));
+  if (w00) LMC_CK(cudaMemcpyAsync(w00, d.w00, ny, cudaMemcpyDeviceToHost, h->s));
+  double sc[8];
+  LMC_CK(cudaMemcpyAsync(sc, d.scal_d, sizeof(sc), cudaMemcpyDeviceToHost, h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  if (time) *time = sc[2];
+  return h->err;
+}
+
+int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi, float *scal, double *u00, double *v00,
+                      double *w00, double *time) {
+  if (!h) return LMC_EINVAL;
+  const size_t n = (size_t)h->d.nmode * h->d.my * 2;
+  std::vector<double> a(vor ? n : 0), b(phi ? n : 0), c(psi ? n : 0), e(scal ? n : 0);
+  int rc = lmc_get_state_f64(h, vor ? a.data() : nullptr, phi ? b.data() : nullptr, psi ? c.data() : nullptr,
+                             scal ? e.data() : nullptr, u00, v00, w00, time);
+  if (rc) return rc;
+  for (size_t i = 0; i < n; i++) {
+    if (vor) vor[i] = (float)a[i];
+    if (phi) phi[i] = (float)b[i];
+    if (psi) psi[i] = (float)c[i];
+    if (scal) scal[i] = (float)e[i];
+  }
+  return LMC_OK;
+}
+
+int lmc_step(lmc_handle *h, int nsteps) {
+  if (!h || nsteps < 0) return LMC_EINVAL;
+  if (h->err) return h->err;
+  LMC_CK(cudaSetDevice(h->p.device));
+  const lmc::Dev &d = h->d;
+  cudaStream_t s = h->s;
+  const int ncfl = h->p.ncfl > 0 ? h->p.ncfl : 1;
+  for (int n = 0; n < nsteps; n++) {
+    const int cfl_step = (h->p.dt_mode == 0) && (h->steps % ncfl == 0);  // cross.f:240
+    for (int rk = 0; rk < 3; rk++) {
+      prof_mark(h, 0);
+      lmc::launch_lapv(d, s);
+      prof_mark(h, 1);
+      lmc::launch_assemble(d, rk, s);
+      prof_mark(h, 2);
+      lmc::launch_tder(d, s);
+      prof_mark(h, 3);
+      lmc::launch_zinv(d, s);
+      if (rk == 0) {
+        prof_mark(h, 9);
+        LMC_CK(cudaMemsetAsync(d.rhom, 0, (size_t)d.my * sizeof(double), s));
+        if (cfl_step) LMC_CK(cudaMemsetAsync(d.cflmax, 0, 4 * sizeof(unsigned long long), s));
+      }
+      const int do_cfl = cfl_step && rk == 0;
+      prof_mark(h, 4);
+      lmc::launch_xphys(d, rk, do_cfl, rk == 0, s);
+      prof_mark(h, 5);
+      lmc::launch_zfwd(d, s);
+      prof_mark(h, 6);
+      lmc::launch_post1(d, rk, do_cfl, 1, s);
+      prof_mark(h, 7);
+      lmc::launch_post2(d, rk, s);
+      prof_mark(h, 8);
+      lmc::launch_psi(d, rk, cfl_step, 1, s);
+      prof_mark(h, -1);
+    }
+    h->steps++;
+    if (check_launch(h)) return LMC_ECUDA;
+  }
+  return LMC_OK;
+}
+
+int lmc_sync(lmc_handle *h) {
+  if (!h) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return h->err;
+}
+
+int lmc_get_diag(lmc_handle *h, lmc_diag *out) {
+  if (!h || !out) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  double dg[16];
+  int st = 0;
+  LMC_CK(cudaMemcpyAsync(dg, h->d.diag, sizeof(dg), cudaMemcpyDeviceToHost, h->s));
+  LMC_CK(cudaMemcpyAsync(&st, h->d.status, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  out->time = dg[0]; out->Deltat = dg[1]; out->dm = dg[2]; out->dw = dg[3]; out->Redw = dg[4];
+  out->trapz = dg[5]; out->masst = dg[6]; out->massu = dg[7]; out->massv = dg[8]; out->massw = dg[9];
+  out->H00u = dg[10]; out->H00w = dg[11]; out->Deltat_next = dg[12];
+  out->step = h->steps;
+  out->status = st;
+  return h->err;
+}
+
+int lmc_status(lmc_handle *h) {
+  if (!h) return LMC_EINVAL;
+  lmc_diag dg;
+  int rc = lmc_get_diag(h, &dg);
+  return rc ? rc : dg.status;
+}
+
+void *lmc_stream(lmc_handle *h) { return h ? (void *)h->s : nullptr; }
+
+int lmc_state_device_ptrs(lmc_handle *h, double **vor, double **phi, double **psi, double **scal) {
+  if (!h) return LMC_EINVAL;
+  if (vor) *vor = (double *)h->d.vor;
+  if (phi) *phi = (double *)h->d.phi;
+  if (psi) *psi = (double *)h->d.psi;
+  if (scal) *scal = (double *)h->d.scal;
+  return LMC_OK;
+}
+
+int lmc_profile_start(lmc_handle *h) {
+  if (!h) return LMC_EINVAL;
+  h->prof = true;
+  h->ev_used = 0;
+  return LMC_OK;
+}
+
+int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count) {
+  if (!h || nk < 0 || (nk && (!ms || !count))) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  for (int k = 0; k < nk; k++) { ms[k] = 0.0; count[k] = 0; }
+  for (size_t i = 0; i + 1 < h->ev_used; i++) {
+    const int k = h->ev_kid[i];
+    if (k < 0 || k >= nk) continue;
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, h->ev_pool[i], h->ev_pool[i + 1]) == cudaSuccess) {
+      ms[k] += t;
+      count[k] += 1;
+    }
+  }
+  h->prof = false;
+  h->ev_used = 0;
+  return h->err;
+}
+
+int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev, double *out2_dev) {
+  if (!h || op < 1 || op > 4 || !in_dev || !out_dev || (op == 3 && !out2_dev)) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  lmc::launch_op_y(h->d, op, (const double2 *)in_dev, (double2 *)out_dev, (double2 *)out2_dev, h->s);
+  if (check_launch(h)) return LMC_ECUDA;
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return LMC_OK;
+}
+
+}  // extern "C"

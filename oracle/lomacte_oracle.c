@@ -1,0 +1,1179 @@
+/*
+ * lomacte_oracle.c -- CPU FP64 oracle for the lomacte RK3 substep.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline).  The
+ * product library never links or calls this file.  See lomacte_oracle.h for
+ * the list of reference files restated here.  Every routine cites the
+ * reference routine (file:line, paths inside Beovulfo/LoMa_phD) it follows.
+ *
+ * Parity pinning: the FFT conventions are pinned by the reference's own
+ * golden vectors (branches/reactml/benchmark_fft/ cfttest_double.txt, rffttest_double.txt); the compact
+ * derivatives by the analytic-derivative harness pattern of
+ * trunk/mixing/test/test.f:182-200 and benchmark_fft/main.f:46-74; the full
+ * substep is pinned by restatement only (the Fortran cannot be built here).
+ */
+#include "lomacte_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef double complex cplx;
+
+/* ------------------------------------------------------------------ */
+/* RK3 coefficients: modulos.f:193-209 (module rkcoef).                */
+/* ------------------------------------------------------------------ */
+static void rk_coefs(double gama[3], double xi[3], double alpha[3],
+                     double beta[3]) {
+  const double p0 = 5.0 / 66.0, p1 = -1.0;
+  xi[0] = 0.0;
+  xi[1] = -17.0 / 60.0;
+  xi[2] = -5.0 / 12.0;
+  gama[0] = 8.0 / 15.0;
+  gama[1] = 5.0 / 12.0;
+  gama[2] = 3.0 / 4.0;
+  double b3 = (p1 * (gama[0] * gama[2] + gama[1] * gama[2] + xi[1] * gama[2] +
+                     gama[0] * xi[2]) -
+               gama[0] * gama[1] * gama[2] - gama[0] * gama[1] * xi[2]) /
+              (p1 - gama[0] * gama[1]);
+  beta[0] = gama[0] - p0;
+  beta[1] = p1;
+  beta[2] = b3;
+  alpha[0] = p0;
+  alpha[1] = gama[1] + xi[1] - p1;
+  alpha[2] = gama[2] + xi[2] - beta[2];
+}
+
+/* ------------------------------------------------------------------ */
+/* FFT written from the DFT definition (mixed-radix, recursive DIT).   */
+/* Conventions follow cftsingle.f:2-68 and rftsingle.f:25-95: the      */
+/* direct transform (iopt<0) is exp(-i..) scaled by 1/n, the inverse   */
+/* is exp(+i..) unscaled.                                              */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  int n, nf, fac[40];
+  cplx *w; /* w[t] = exp(-2 pi i t / n) */
+} fftplan;
+
+static void plan_init(fftplan *p, int n) {
+  p->n = n;
+  p->nf = 0;
+  int m = n;
+  while (m % 4 == 0) { p->fac[p->nf++] = 4; m /= 4; }
+  while (m % 2 == 0) { p->fac[p->nf++] = 2; m /= 2; }
+  for (int f = 3; m > 1;) {
+    if (m % f == 0) { p->fac[p->nf++] = f; m /= f; }
+    else f += 2;
+  }
+  p->w = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+  for (int t = 0; t < n; t++) {
+    double a = 2.0 * M_PI * (double)t / (double)n;
+    p->w[t] = cos(a) - I * sin(a);
+  }
+}
+static void plan_free(fftplan *p) { free(p->w); }
+
+/* out[k] = sum_j in[j*is] W^{jk}, W = exp(sign*2 pi i/n); n divides P->n */
+static void dft_rec(const fftplan *P, int n, int fi, const cplx *in, int is,
+                    cplx *out, int sign) {
+  if (n == 1) { out[0] = in[0]; return; }
+  int p = P->fac[fi], m = n / p, N = P->n, step = N / n;
+  for (int r = 0; r < p; r++) dft_rec(P, m, fi + 1, in + (size_t)r * is, is * p, out + (size_t)r * m, sign);
+  cplx t[64];
+  for (int k = 0; k < m; k++) {
+    for (int r = 0; r < p; r++) {
+      cplx w = P->w[((size_t)r * k * step) % N];
+      if (sign > 0) w = conj(w);
+      t[r] = out[(size_t)r * m + k] * w;
+    }
+    for (int q = 0; q < p; q++) {
+      cplx s = 0;
+      for (int r = 0; r < p; r++) {
+        cplx w = P->w[((size_t)((r * q) % p) * (N / p)) % N];
+        if (sign > 0) w = conj(w);
+        s += t[r] * w;
+      }
+      out[(size_t)q * m + k] = s;
+    }
+  }
+}
+
+/* unnormalised c2c of length P->n: out = sum in exp(sign 2 pi i jk/n) */
+static void cfft(const fftplan *P, const cplx *in, cplx *out, int sign) {
+  dft_rec(P, P->n, 0, in, 1, out, sign);
+}
+
+/* ------------------------------------------------------------------ */
+/* Band storage helpers.  A(i,j) of the reference (band i, row j,      */
+/* 1-based) is a[(j-1)*nb + (i-1)] here.                               */
+/* ------------------------------------------------------------------ */
+#define B7(a, i, j) a[((j)-1) * 7 + ((i)-1)]
+#define B5(a, i, j) a[((j)-1) * 5 + ((i)-1)]
+
+/* gaussj: Gauss-Jordan elimination with full pivoting, the published
+ * algorithm used at cfdiff.f:1144-1223.  a is column-major a(np,np). */
+static void gaussj(double *a, int n, int np, double *b, int m, int mp) {
+  int indxc[64], indxr[64], ipiv[64];
+  int irow = 0, icol = 0;
+#define A(i, j) a[((j)-1) * np + ((i)-1)]
+#define BB(i, j) b[((j)-1) * np + ((i)-1)]
+  (void)mp;
+  for (int j = 1; j <= n; j++) ipiv[j] = 0;
+  for (int i = 1; i <= n; i++) {
+    double big = 0.0;
+    for (int j = 1; j <= n; j++)
+      if (ipiv[j] != 1)
+        for (int k = 1; k <= n; k++)
+          if (ipiv[k] == 0 && fabs(A(j, k)) >= big) {
+            big = fabs(A(j, k));
+            irow = j;
+            icol = k;
+          }
+    ipiv[icol] += 1;
+    if (irow != icol) {
+      for (int l = 1; l <= n; l++) { double d = A(irow, l); A(irow, l) = A(icol, l); A(icol, l) = d; }
+      for (int l = 1; l <= m; l++) { double d = BB(irow, l); BB(irow, l) = BB(icol, l); BB(icol, l) = d; }
+    }
+    indxr[i] = irow;
+    indxc[i] = icol;
+    double pivinv = 1.0 / A(icol, icol);
+    A(icol, icol) = 1.0;
+    for (int l = 1; l <= n; l++) A(icol, l) *= pivinv;
+    for (int l = 1; l <= m; l++) BB(icol, l) *= pivinv;
+    for (int ll = 1; ll <= n; ll++)
+      if (ll != icol) {
+        double dum = A(ll, icol);
+        A(ll, icol) = 0.0;
+        for (int l = 1; l <= n; l++) A(ll, l) -= A(icol, l) * dum;
+        for (int l = 1; l <= m; l++) BB(ll, l) -= BB(icol, l) * dum;
+      }
+  }
+  for (int l = n; l >= 1; l--)
+    if (indxr[l] != indxc[l])
+      for (int k = 1; k <= n; k++) {
+        double d = A(k, indxr[l]);
+        A(k, indxr[l]) = A(k, indxc[l]);
+        A(k, indxc[l]) = d;
+      }
+#undef A
+#undef BB
+}
+
+/* pred1m6o: cfdiff.f:24-182.  Columns of d(ny,7) for the LHS
+ * (den,ben,aln,one,alp,bep,dep) and RHS (a3n..a3p) of the first
+ * derivative on uniform eta in [-1,1]. */
+static void pred1m6o(int ny, double *l /*ny x 7*/, double *r /*ny x 7*/) {
+#define L(j, c) l[((c)-1) * ny + ((j)-1)]
+#define R(j, c) r[((c)-1) * ny + ((j)-1)]
+  double h = 2.0 / (double)(ny - 1);
+  double aaa = 0.56926818603810, bbb = 0.31997939759919, ccc = 0.03751544855390;
+  double alpha = -3.0 / 4.0 + (33.0 / 20.0) * ccc + (239.0 / 180.0) * aaa + (82.0 / 45.0) * bbb;
+  double beta = 3.0 / 10.0 + (24.0 / 25.0) * ccc - (88.0 / 225.0) * aaa + (34.0 / 225.0) * bbb;
+  double delta = -1.0 / 20.0 + (39.0 / 100.0) * ccc + (19.0 / 300.0) * aaa + (2.0 / 75.0) * bbb;
+  for (int j = 1; j <= ny; j++) L(j, 4) = 1.0;
+  for (int j = 4; j <= ny - 3; j++) {
+    L(j, 1) = delta; L(j, 2) = beta; L(j, 3) = alpha;
+    L(j, 5) = alpha; L(j, 6) = beta; L(j, 7) = delta;
+    R(j, 1) = -ccc / h; R(j, 2) = -bbb / h; R(j, 3) = -aaa / h; R(j, 4) = 0.0;
+    R(j, 5) = aaa / h; R(j, 6) = bbb / h; R(j, 7) = ccc / h;
+  }
+  /* j=1 (cfdiff.f:83-98) */
+  L(1, 1) = 0; L(1, 2) = 0; L(1, 3) = 0; L(1, 5) = 1; L(1, 6) = 0; L(1, 7) = 0;
+  R(1, 1) = 0; R(1, 2) = 0; R(1, 3) = 0; R(1, 4) = -2.0 / h; R(1, 5) = 2.0 / h; R(1, 6) = 0; R(1, 7) = 0;
+  /* j=2 (cfdiff.f:100-115) */
+  L(2, 1) = 0; L(2, 2) = 0; L(2, 3) = 0.25; L(2, 5) = 0.25; L(2, 6) = 0; L(2, 7) = 0;
+  R(2, 1) = 0; R(2, 2) = 0; R(2, 3) = -3.0 / 4.0 / h; R(2, 4) = 0; R(2, 5) = 3.0 / 4.0 / h; R(2, 6) = 0; R(2, 7) = 0;
+  /* j=3 (cfdiff.f:118-132) */
+  L(3, 1) = 0; L(3, 2) = 1.0 / 36.0; L(3, 3) = 4.0 / 9.0; L(3, 5) = 4.0 / 9.0; L(3, 6) = 1.0 / 36.0; L(3, 7) = 0;
+  R(3, 1) = 0; R(3, 2) = -25.0 / 216.0 / h; R(3, 3) = -20.0 / 27.0 / h; R(3, 4) = 0;
+  R(3, 5) = 20.0 / 27.0 / h; R(3, 6) = 25.0 / 216.0 / h; R(3, 7) = 0;
+  /* mirrored ends (cfdiff.f:136-179) */
+  for (int e = 1; e <= 3; e++) {
+    int j = ny + 1 - e;
+    L(j, 1) = L(e, 7); L(j, 2) = L(e, 6); L(j, 3) = L(e, 5);
+    L(j, 5) = L(e, 3); L(j, 6) = L(e, 2); L(j, 7) = L(e, 1);
+    R(j, 1) = -R(e, 7); R(j, 2) = -R(e, 6); R(j, 3) = -R(e, 5); R(j, 4) = -R(e, 4);
+    R(j, 5) = -R(e, 3); R(j, 6) = -R(e, 2); R(j, 7) = -R(e, 1);
+  }
+#undef L
+#undef R
+}
+
+/* prederiv2: cfdiff.f:196-501.  Second derivative on the actual y, from
+ * Taylor-matching systems solved with gaussj. */
+static void prederiv2(int ny, double *l /*ny x 5*/, double *r /*ny x 5*/,
+                      const double *x /*1-based via X()*/) {
+#define L(j, c) l[((c)-1) * ny + ((j)-1)]
+#define R(j, c) r[((c)-1) * ny + ((j)-1)]
+#define X(j) x[(j)-1]
+  double c[81], b[9];
+#define C(i, j) c[((j)-1) * 9 + ((i)-1)]
+  for (int j = 1; j <= ny; j++) L(j, 3) = 1.0;
+  for (int j = 3; j <= ny - 2; j++) {
+    double d[4] = {X(j - 2) - X(j), X(j - 1) - X(j), X(j + 1) - X(j), X(j + 2) - X(j)};
+    C(1, 1) = 0; C(1, 2) = 0; C(1, 3) = 0; C(1, 4) = 0; C(1, 5) = 1; C(1, 6) = 1; C(1, 7) = 1; C(1, 8) = 1; C(1, 9) = 1; b[0] = 0;
+    C(2, 1) = 0; C(2, 2) = 0; C(2, 3) = 0; C(2, 4) = 0; C(2, 5) = d[0]; C(2, 6) = d[1]; C(2, 7) = 0; C(2, 8) = d[2]; C(2, 9) = d[3]; b[1] = 0;
+    C(3, 1) = 2; C(3, 2) = 2; C(3, 3) = 2; C(3, 4) = 2;
+    C(3, 5) = -d[0] * d[0]; C(3, 6) = -d[1] * d[1]; C(3, 7) = 0; C(3, 8) = -d[2] * d[2]; C(3, 9) = -d[3] * d[3]; b[2] = -2;
+    for (int n = 3; n <= 8; n++) {
+      double nn = (double)(n * (n - 1));
+      C(n + 1, 1) = nn * pow(d[0], n - 2); C(n + 1, 2) = nn * pow(d[1], n - 2);
+      C(n + 1, 3) = nn * pow(d[2], n - 2); C(n + 1, 4) = nn * pow(d[3], n - 2);
+      C(n + 1, 5) = -pow(d[0], n); C(n + 1, 6) = -pow(d[1], n); C(n + 1, 7) = 0;
+      C(n + 1, 8) = -pow(d[2], n); C(n + 1, 9) = -pow(d[3], n); b[n] = 0;
+    }
+    gaussj(c, 9, 9, b, 1, 1);
+    L(j, 1) = b[0]; L(j, 2) = b[1]; L(j, 4) = b[2]; L(j, 5) = b[3];
+    R(j, 1) = b[4]; R(j, 2) = b[5]; R(j, 3) = b[6]; R(j, 4) = b[7]; R(j, 5) = b[8];
+  }
+  { /* j=1 (cfdiff.f:283-335) */
+    int j = 1;
+    double d1 = X(j + 1) - X(j), d2 = X(j + 2) - X(j);
+    C(1, 1) = 0; C(1, 2) = 0; C(1, 3) = 1; C(1, 4) = 1; C(1, 5) = 1; b[0] = 0;
+    C(2, 1) = 0; C(2, 2) = 0; C(2, 3) = 0; C(2, 4) = d1; C(2, 5) = d2; b[1] = 0;
+    C(3, 1) = 2; C(3, 2) = 2; C(3, 3) = 0; C(3, 4) = -d1 * d1; C(3, 5) = -d2 * d2; b[2] = -2;
+    for (int n = 3; n <= 4; n++) {
+      double nn = (double)(n * (n - 1));
+      C(n + 1, 1) = nn * pow(d1, n - 2); C(n + 1, 2) = nn * pow(d2, n - 2); C(n + 1, 3) = 0;
+      C(n + 1, 4) = -pow(d1, n); C(n + 1, 5) = -pow(d2, n); b[n] = 0;
+    }
+    gaussj(c, 5, 9, b, 1, 1);
+    L(j, 1) = 0; L(j, 2) = 0; L(j, 4) = b[0]; L(j, 5) = b[1];
+    R(j, 1) = 0; R(j, 2) = 0; R(j, 3) = b[2]; R(j, 4) = b[3]; R(j, 5) = b[4];
+  }
+  { /* j=2 (cfdiff.f:338-387) */
+    int j = 2;
+    double dm1 = X(j - 1) - X(j), d1 = X(j + 1) - X(j), d2 = X(j + 2) - X(j);
+    C(1, 1) = 0; C(1, 2) = 0; C(1, 3) = 0; C(1, 4) = 1; C(1, 5) = 1; C(1, 6) = 1; C(1, 7) = 1; b[0] = 0;
+    C(2, 1) = 0; C(2, 2) = 0; C(2, 3) = 0; C(2, 4) = dm1; C(2, 5) = 0; C(2, 6) = d1; C(2, 7) = d2; b[1] = 0;
+    C(3, 1) = 2; C(3, 2) = 2; C(3, 3) = 2; C(3, 4) = -dm1 * dm1; C(3, 5) = 0; C(3, 6) = -d1 * d1; C(3, 7) = -d2 * d2; b[2] = -2;
+    for (int n = 3; n <= 6; n++) {
+      double nn = (double)(n * (n - 1));
+      C(n + 1, 1) = nn * pow(dm1, n - 2); C(n + 1, 2) = nn * pow(d1, n - 2); C(n + 1, 3) = nn * pow(d2, n - 2);
+      C(n + 1, 4) = -pow(dm1, n); C(n + 1, 5) = 0; C(n + 1, 6) = -pow(d1, n); C(n + 1, 7) = -pow(d2, n); b[n] = 0;
+    }
+    gaussj(c, 7, 9, b, 1, 1);
+    L(j, 1) = 0; L(j, 2) = b[0]; L(j, 4) = b[1]; L(j, 5) = b[2];
+    R(j, 1) = 0; R(j, 2) = b[3]; R(j, 3) = b[4]; R(j, 4) = b[5]; R(j, 5) = b[6];
+  }
+  { /* j=ny-1 (cfdiff.f:391-441) */
+    int j = ny - 1;
+    double dm2 = X(j - 2) - X(j), dm1 = X(j - 1) - X(j), d1 = X(j + 1) - X(j);
+    C(1, 1) = 0; C(1, 2) = 0; C(1, 3) = 0; C(1, 4) = 1; C(1, 5) = 1; C(1, 6) = 1; C(1, 7) = 1; b[0] = 0;
+    C(2, 1) = 0; C(2, 2) = 0; C(2, 3) = 0; C(2, 4) = dm2; C(2, 5) = dm1; C(2, 6) = 0; C(2, 7) = d1; b[1] = 0;
+    C(3, 1) = 2; C(3, 2) = 2; C(3, 3) = 2; C(3, 4) = -dm2 * dm2; C(3, 5) = -dm1 * dm1; C(3, 6) = 0; C(3, 7) = -d1 * d1; b[2] = -2;
+    for (int n = 3; n <= 6; n++) {
+      double nn = (double)(n * (n - 1));
+      C(n + 1, 1) = nn * pow(dm2, n - 2); C(n + 1, 2) = nn * pow(dm1, n - 2); C(n + 1, 3) = nn * pow(d1, n - 2);
+      C(n + 1, 4) = -pow(dm2, n); C(n + 1, 5) = -pow(dm1, n); C(n + 1, 6) = 0; C(n + 1, 7) = -pow(d1, n); b[n] = 0;
+    }
+    gaussj(c, 7, 9, b, 1, 1);
+    L(j, 1) = b[0]; L(j, 2) = b[1]; L(j, 4) = b[2]; L(j, 5) = 0;
+    R(j, 1) = b[3]; R(j, 2) = b[4]; R(j, 3) = b[5]; R(j, 4) = b[6]; R(j, 5) = 0;
+  }
+  { /* j=ny (cfdiff.f:445-498) */
+    int j = ny;
+    double dm1 = X(j - 1) - X(j), dm2 = X(j - 2) - X(j);
+    C(1, 1) = 0; C(1, 2) = 0; C(1, 3) = 1; C(1, 4) = 1; C(1, 5) = 1; b[0] = 0;
+    C(2, 1) = 0; C(2, 2) = 0; C(2, 3) = 0; C(2, 4) = dm1; C(2, 5) = dm2; b[1] = 0;
+    C(3, 1) = 2; C(3, 2) = 2; C(3, 3) = 0; C(3, 4) = -dm1 * dm1; C(3, 5) = -dm2 * dm2; b[2] = -2;
+    for (int n = 3; n <= 4; n++) {
+      double nn = (double)(n * (n - 1));
+      C(n + 1, 1) = nn * pow(dm1, n - 2); C(n + 1, 2) = nn * pow(dm2, n - 2); C(n + 1, 3) = 0;
+      C(n + 1, 4) = -pow(dm1, n); C(n + 1, 5) = -pow(dm2, n); b[n] = 0;
+    }
+    gaussj(c, 5, 9, b, 1, 1);
+    L(j, 1) = b[1]; L(j, 2) = b[0]; L(j, 4) = 0; L(j, 5) = 0;
+    R(j, 1) = b[4]; R(j, 2) = b[3]; R(j, 3) = b[2]; R(j, 4) = 0; R(j, 5) = 0;
+  }
+#undef C
+#undef X
+#undef L
+#undef R
+}
+
+/* bandec / banbks (5-band, cfdiff.f:954-1022) */
+static void bandec(double *a, int n) {
+  for (int j = 1; j <= 3; j++) B5(a, j, 1) = B5(a, j + 2, 1);
+  for (int j = 1; j <= 4; j++) B5(a, j, 2) = B5(a, j + 1, 2);
+  for (int k = 1; k <= n - 2; k++) {
+    B5(a, 1, k) = 1.0 / B5(a, 1, k);
+    B5(a, 4, k) = B5(a, 1, k + 1) * B5(a, 1, k);
+    B5(a, 1, k + 1) = B5(a, 2, k + 1) - B5(a, 4, k) * B5(a, 2, k);
+    B5(a, 2, k + 1) = B5(a, 3, k + 1) - B5(a, 4, k) * B5(a, 3, k);
+    B5(a, 3, k + 1) = B5(a, 4, k + 1);
+    B5(a, 5, k) = B5(a, 1, k + 2) * B5(a, 1, k);
+    B5(a, 1, k + 2) = B5(a, 2, k + 2) - B5(a, 5, k) * B5(a, 2, k);
+    B5(a, 2, k + 2) = B5(a, 3, k + 2) - B5(a, 5, k) * B5(a, 3, k);
+    B5(a, 3, k + 2) = B5(a, 4, k + 2);
+    B5(a, 4, k + 2) = B5(a, 5, k + 2);
+  }
+  B5(a, 1, n - 1) = 1.0 / B5(a, 1, n - 1);
+  B5(a, 4, n - 1) = B5(a, 1, n) * B5(a, 1, n - 1);
+  B5(a, 1, n) = B5(a, 2, n) - B5(a, 4, n - 1) * B5(a, 2, n - 1);
+  B5(a, 2, n) = B5(a, 3, n) - B5(a, 4, n - 1) * B5(a, 3, n - 1);
+  B5(a, 3, n) = B5(a, 4, n);
+  B5(a, 1, n) = 1.0 / B5(a, 1, n);
+}
+
+/* works on a real vector b(1..n) stored 0-based */
+static void banbks(const double *a, int n, double *b) {
+#define V(k) b[(k)-1]
+  for (int k = 1; k <= n - 2; k++) {
+    V(k + 1) -= B5(a, 4, k) * V(k);
+    V(k + 2) -= B5(a, 5, k) * V(k);
+  }
+  V(n) -= B5(a, 4, n - 1) * V(n - 1);
+  V(n) = V(n) * B5(a, 1, n);
+  V(n - 1) = (V(n - 1) - B5(a, 2, n - 1) * V(n)) * B5(a, 1, n - 1);
+  for (int i = n - 2; i >= 1; i--) V(i) = (V(i) - B5(a, 2, i) * V(i + 1) - B5(a, 3, i) * V(i + 2)) * B5(a, 1, i);
+#undef V
+}
+
+/* banbks7 / bandec7 (cfdiff.f:1025-1137) */
+static void banbks7(const double *a, int n, double *b) {
+#define V(k) b[(k)-1]
+  for (int k = 1; k <= n - 3; k++) {
+    V(k + 1) -= B7(a, 5, k) * V(k);
+    V(k + 2) -= B7(a, 6, k) * V(k);
+    V(k + 3) -= B7(a, 7, k) * V(k);
+  }
+  V(n - 1) -= B7(a, 5, n - 2) * V(n - 2);
+  V(n) -= B7(a, 6, n - 2) * V(n - 2);
+  V(n) -= B7(a, 5, n - 1) * V(n - 1);
+  V(n) = V(n) * B7(a, 1, n);
+  V(n - 1) = (V(n - 1) - B7(a, 2, n - 1) * V(n)) * B7(a, 1, n - 1);
+  V(n - 2) = (V(n - 2) - B7(a, 2, n - 2) * V(n - 1) - B7(a, 3, n - 2) * V(n)) * B7(a, 1, n - 2);
+  for (int i = n - 3; i >= 1; i--)
+    V(i) = (V(i) - B7(a, 2, i) * V(i + 1) - B7(a, 3, i) * V(i + 2) - B7(a, 4, i) * V(i + 3)) * B7(a, 1, i);
+#undef V
+}
+
+static void bandec7(double *a, int n) {
+  for (int j = 1; j <= 4; j++) B7(a, j, 1) = B7(a, j + 3, 1);
+  for (int j = 1; j <= 5; j++) B7(a, j, 2) = B7(a, j + 2, 2);
+  for (int j = 1; j <= 6; j++) B7(a, j, 3) = B7(a, j + 1, 3);
+  for (int k = 1; k <= n - 3; k++) {
+    B7(a, 1, k) = 1.0 / B7(a, 1, k);
+    B7(a, 5, k) = B7(a, 1, k + 1) * B7(a, 1, k);
+    B7(a, 1, k + 1) = B7(a, 2, k + 1) - B7(a, 5, k) * B7(a, 2, k);
+    B7(a, 2, k + 1) = B7(a, 3, k + 1) - B7(a, 5, k) * B7(a, 3, k);
+    B7(a, 3, k + 1) = B7(a, 4, k + 1) - B7(a, 5, k) * B7(a, 4, k);
+    B7(a, 4, k + 1) = B7(a, 5, k + 1);
+    B7(a, 6, k) = B7(a, 1, k + 2) * B7(a, 1, k);
+    B7(a, 1, k + 2) = B7(a, 2, k + 2) - B7(a, 6, k) * B7(a, 2, k);
+    B7(a, 2, k + 2) = B7(a, 3, k + 2) - B7(a, 6, k) * B7(a, 3, k);
+    B7(a, 3, k + 2) = B7(a, 4, k + 2) - B7(a, 6, k) * B7(a, 4, k);
+    B7(a, 4, k + 2) = B7(a, 5, k + 2);
+    B7(a, 5, k + 2) = B7(a, 6, k + 2);
+    B7(a, 7, k) = B7(a, 1, k + 3) * B7(a, 1, k);
+    B7(a, 1, k + 3) = B7(a, 2, k + 3) - B7(a, 7, k) * B7(a, 2, k);
+    B7(a, 2, k + 3) = B7(a, 3, k + 3) - B7(a, 7, k) * B7(a, 3, k);
+    B7(a, 3, k + 3) = B7(a, 4, k + 3) - B7(a, 7, k) * B7(a, 4, k);
+    B7(a, 4, k + 3) = B7(a, 5, k + 3);
+    B7(a, 5, k + 3) = B7(a, 6, k + 3);
+    B7(a, 6, k + 3) = B7(a, 7, k + 3);
+  }
+  B7(a, 1, n - 2) = 1.0 / B7(a, 1, n - 2);
+  B7(a, 5, n - 2) = B7(a, 1, n - 1) * B7(a, 1, n - 2);
+  B7(a, 1, n - 1) = B7(a, 2, n - 1) - B7(a, 5, n - 2) * B7(a, 2, n - 2);
+  B7(a, 2, n - 1) = B7(a, 3, n - 1) - B7(a, 5, n - 2) * B7(a, 3, n - 2);
+  B7(a, 3, n - 1) = B7(a, 4, n - 1) - B7(a, 5, n - 2) * B7(a, 4, n - 2);
+  B7(a, 4, n - 1) = B7(a, 5, n - 1);
+  B7(a, 6, n - 2) = B7(a, 1, n) * B7(a, 1, n - 2);
+  B7(a, 1, n) = B7(a, 2, n) - B7(a, 6, n - 2) * B7(a, 2, n - 2);
+  B7(a, 2, n) = B7(a, 3, n) - B7(a, 6, n - 2) * B7(a, 3, n - 2);
+  B7(a, 3, n) = B7(a, 4, n) - B7(a, 6, n - 2) * B7(a, 4, n - 2);
+  B7(a, 4, n) = B7(a, 5, n);
+  B7(a, 5, n) = B7(a, 6, n);
+  B7(a, 1, n - 1) = 1.0 / B7(a, 1, n - 1);
+  B7(a, 5, n - 1) = B7(a, 1, n) * B7(a, 1, n - 1);
+  B7(a, 1, n) = B7(a, 2, n) - B7(a, 5, n - 1) * B7(a, 2, n - 1);
+  B7(a, 2, n) = B7(a, 3, n) - B7(a, 5, n - 1) * B7(a, 3, n - 1);
+  B7(a, 3, n) = B7(a, 4, n) - B7(a, 5, n - 1) * B7(a, 4, n - 1);
+  B7(a, 4, n) = B7(a, 5, n);
+  B7(a, 1, n) = 1.0 / B7(a, 1, n);
+}
+
+/* Band matrix-vector products with the reference's truncated edge rows:
+ * the 7-band one of deryr2 / calcrhsd1 (cfdiff.f:533-584, laps.f:97-127)
+ * and the 5-band one of deryyr2 (cfdiff.f:750-781).  Edge rows only use
+ * the in-range columns, exactly as the reference spells them out. */
+static void matvec7(const double *m, int n, const double *u, double *out) {
+  for (int j = 1; j <= n; j++) {
+    double s = 0.0;
+    int lo = j - 3 < 1 ? 1 : j - 3, hi = j + 3 > n ? n : j + 3;
+    for (int c = lo; c <= hi; c++) s += B7(m, c - j + 4, j) * u[c - 1];
+    out[j - 1] = s;
+  }
+}
+static void matvec5(const double *m, int n, const double *u, double *out) {
+  for (int j = 1; j <= n; j++) {
+    double s = 0.0;
+    int lo = j - 2 < 1 ? 1 : j - 2, hi = j + 2 > n ? n : j + 2;
+    for (int c = lo; c <= hi; c++) s += B5(m, c - j + 3, j) * u[c - 1];
+    out[j - 1] = s;
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Oracle object                                                       */
+/* ------------------------------------------------------------------ */
+struct lmo {
+  int mgalx, mgalz, my, mx, nkx, mz, nz1, nz2, nmode;
+  double Re, alp, bet, peclet, cfl, ire;
+  int ncfl, dtmode, nthreads;
+  double *y, *hy, *trp, *fmap;
+  double *prem1, *dt11, *dt12, *prem3, *dt21, *dt22; /* band [row][band] */
+  double *kxv, *kzv; /* wavenumbers: kx(i)=alp*i, kz(k) signed */
+  double gama[3], xi[3], alpha[3], beta[3];
+  /* state, reference layout [kx][kz][y] */
+  cplx *vor, *phi, *psi, *scal;
+  cplx *ten12p, *ten13p; /* RHS(Omega_y), RHS(phi) of the previous substep */
+  double *rhst;          /* physical RHS(T) of the previous substep [line][x] */
+  double *u00wk, *v00wk, *w00wk, *rf0u, *rf0w, *rf0v;
+  double Deltat, time, dtr, rhobot, rhotop;
+  int icfl, istep_total;
+  double diag[LMO_NDIAG];
+  fftplan px, pz;
+  /* work buffers: spectral [kx][kz][y] (size nmode*my) */
+  cplx *w_mx, *w_my, *w_mz, *w_nx, *w_ny, *w_nz, *w_t12, *w_t13, *w_t23, *w_drho, *w_chwk, *w_chwk2;
+  /* line buffers [line][kx] complex, line = z + mgalz*y */
+  cplx *ln[11];
+};
+
+#define SIDX(o, i, k, j) (((size_t)(i) * (o)->mz + (k)) * (o)->my + (j))
+
+static void *xcalloc(size_t n, size_t s) { return calloc(n ? n : 1, s); }
+
+lmo *lmo_create(int mgalx, int mgalz, int my, const double *y, double Re,
+                double alp, double bet, double peclet, double cfl, int ncfl,
+                int dtmode, double dt0, int nthreads) {
+  if (mgalx < 6 || mgalz < 3 || my < 9) return NULL;
+  lmo *o = (lmo *)xcalloc(1, sizeof(lmo));
+  o->mgalx = mgalx; o->mgalz = mgalz; o->my = my;
+  o->mx = 2 * (mgalx / 3); o->nkx = o->mx / 2;
+  o->mz = 2 * (mgalz / 3) - 1; o->nz1 = (o->mz - 1) / 2; o->nz2 = mgalz - o->nz1;
+  o->nmode = o->nkx * o->mz;
+  o->Re = Re; o->alp = alp; o->bet = bet; o->peclet = peclet; o->cfl = cfl;
+  o->ire = 1.0 / Re; o->ncfl = ncfl < 1 ? 1 : ncfl; o->dtmode = dtmode;
+  o->nthreads = nthreads;
+  rk_coefs(o->gama, o->xi, o->alpha, o->beta);
+  o->y = (double *)xcalloc(my, 8); memcpy(o->y, y, sizeof(double) * my);
+  o->hy = (double *)xcalloc(my, 8); o->trp = (double *)xcalloc(my, 8); o->fmap = (double *)xcalloc(my, 8);
+  /* main.f:689-696 */
+  for (int j = 2; j <= my - 1; j++) {
+    o->trp[j - 1] = 0.25 * (y[j] - y[j - 2]);
+    o->hy[j - 1] = (y[j] - y[j - 2]) / 2.0;
+  }
+  o->trp[0] = 0.25 * (y[1] - y[0]);
+  o->trp[my - 1] = 0.25 * (y[my - 1] - y[my - 2]);
+  o->hy[0] = (y[1] - y[0]) / 2.0;
+  o->hy[my - 1] = (y[my - 1] - y[my - 2]) / 2.0;
+  /* derivadas: cfdiff.f:869-941 */
+  double *d11 = xcalloc((size_t)my * 7, 8), *d12 = xcalloc((size_t)my * 7, 8);
+  double *d21 = xcalloc((size_t)my * 5, 8), *d22 = xcalloc((size_t)my * 5, 8);
+  pred1m6o(my, d11, d12);
+  prederiv2(my, d21, d22, y);
+  o->prem1 = xcalloc((size_t)my * 7, 8); o->dt11 = xcalloc((size_t)my * 7, 8); o->dt12 = xcalloc((size_t)my * 7, 8);
+  o->prem3 = xcalloc((size_t)my * 5, 8); o->dt21 = xcalloc((size_t)my * 5, 8); o->dt22 = xcalloc((size_t)my * 5, 8);
+  for (int j = 1; j <= my; j++)
+    for (int i = 1; i <= 7; i++) {
+      B7(o->prem1, i, j) = d11[(i - 1) * my + j - 1];
+      B7(o->dt11, i, j) = d11[(i - 1) * my + j - 1];
+      B7(o->dt12, i, j) = d12[(i - 1) * my + j - 1];
+    }
+  for (int j = 1; j <= my; j++)
+    for (int i = 1; i <= 5; i++) {
+      B5(o->prem3, i, j) = d21[(i - 1) * my + j - 1];
+      B5(o->dt21, i, j) = d21[(i - 1) * my + j - 1];
+      B5(o->dt22, i, j) = d22[(i - 1) * my + j - 1];
+    }
+  free(d11); free(d12); free(d21); free(d22);
+  bandec7(o->prem1, my);
+  bandec(o->prem3, my);
+  matvec7(o->dt12, my, o->y, o->fmap);
+  banbks7(o->prem1, my, o->fmap);
+  for (int j = 0; j < my; j++) o->fmap[j] = 1.0 / o->fmap[j];
+  /* wavenumbers: main.f:769-800 */
+  o->kxv = xcalloc(o->nkx, 8); o->kzv = xcalloc(o->mz, 8);
+  for (int i = 0; i < o->nkx; i++) o->kxv[i] = alp * i;
+  for (int k = 0; k <= o->nz1; k++) o->kzv[k] = bet * k;
+  for (int k = o->nz1 + 1; k < o->mz; k++) o->kzv[k] = -bet * (o->mz - k);
+  size_t ns = (size_t)o->nmode * my;
+  cplx **bufs[] = {&o->vor, &o->phi, &o->psi, &o->scal, &o->ten12p, &o->ten13p,
+                   &o->w_mx, &o->w_my, &o->w_mz, &o->w_nx, &o->w_ny, &o->w_nz,
+                   &o->w_t12, &o->w_t13, &o->w_t23, &o->w_drho, &o->w_chwk, &o->w_chwk2};
+  for (size_t b = 0; b < sizeof(bufs) / sizeof(bufs[0]); b++) *bufs[b] = xcalloc(ns, sizeof(cplx));
+  size_t nl = (size_t)mgalz * my;
+  for (int f = 0; f < 11; f++) o->ln[f] = xcalloc(nl * o->nkx, sizeof(cplx));
+  o->rhst = xcalloc(nl * mgalx, 8);
+  o->u00wk = xcalloc(my, 8); o->v00wk = xcalloc(my, 8); o->w00wk = xcalloc(my, 8);
+  o->rf0u = xcalloc(my, 8); o->rf0w = xcalloc(my, 8); o->rf0v = xcalloc(my, 8);
+  plan_init(&o->px, mgalx);
+  plan_init(&o->pz, mgalz);
+  o->Deltat = dt0; o->icfl = 1; o->dtr = dt0;
+  return o;
+}
+
+void lmo_destroy(lmo *o) {
+  if (!o) return;
+  void *p[] = {o->y, o->hy, o->trp, o->fmap, o->prem1, o->dt11, o->dt12, o->prem3, o->dt21, o->dt22,
+               o->kxv, o->kzv, o->vor, o->phi, o->psi, o->scal, o->ten12p, o->ten13p, o->rhst,
+               o->u00wk, o->v00wk, o->w00wk, o->rf0u, o->rf0w, o->rf0v, o->w_mx, o->w_my, o->w_mz,
+               o->w_nx, o->w_ny, o->w_nz, o->w_t12, o->w_t13, o->w_t23, o->w_drho, o->w_chwk, o->w_chwk2};
+  for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
+  for (int f = 0; f < 11; f++) free(o->ln[f]);
+  plan_free(&o->px); plan_free(&o->pz);
+  free(o);
+}
+
+/* State I/O.  The RK3 memory (previous RHS) is reset, as in a fresh run:
+ * main.f zeroes the whole work pool before cross1 (main.f:171-174). */
+int lmo_set_state(lmo *o, const double *vor, const double *phi, const double *psi,
+                  const double *scal, const double *u00, const double *v00,
+                  const double *w00, double time) {
+  size_t ns = (size_t)o->nmode * o->my;
+  memcpy(o->vor, vor, ns * sizeof(cplx)); memcpy(o->phi, phi, ns * sizeof(cplx));
+  memcpy(o->psi, psi, ns * sizeof(cplx)); memcpy(o->scal, scal, ns * sizeof(cplx));
+  memset(o->ten12p, 0, ns * sizeof(cplx)); memset(o->ten13p, 0, ns * sizeof(cplx));
+  memset(o->rhst, 0, (size_t)o->mgalz * o->my * o->mgalx * 8);
+  /* cross.f:276-280 (first step copies the 00 modes to the work vectors) */
+  memcpy(o->u00wk, u00, o->my * 8); memcpy(o->v00wk, v00, o->my * 8); memcpy(o->w00wk, w00, o->my * 8);
+  memset(o->rf0u, 0, o->my * 8); memset(o->rf0w, 0, o->my * 8); memset(o->rf0v, 0, o->my * 8);
+  o->time = time;
+  /* cross.f:211-213 */
+  o->rhobot = 1.0 / creal(o->scal[SIDX(o, 0, 0, 0)]);
+  o->rhotop = 1.0 / creal(o->scal[SIDX(o, 0, 0, o->my - 1)]);
+  o->icfl = 1; o->istep_total = 0;
+  return 0;
+}
+
+int lmo_get_state(const lmo *o, double *vor, double *phi, double *psi, double *scal,
+                  double *u00, double *v00, double *w00, double *time) {
+  size_t ns = (size_t)o->nmode * o->my;
+  if (vor) memcpy(vor, o->vor, ns * sizeof(cplx));
+  if (phi) memcpy(phi, o->phi, ns * sizeof(cplx));
+  if (psi) memcpy(psi, o->psi, ns * sizeof(cplx));
+  if (scal) memcpy(scal, o->scal, ns * sizeof(cplx));
+  if (u00) memcpy(u00, o->u00wk, o->my * 8);
+  if (v00) memcpy(v00, o->v00wk, o->my * 8);
+  if (w00) memcpy(w00, o->w00wk, o->my * 8);
+  if (time) *time = o->time;
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* y-operators on complex pencils (componentwise, real operators).     */
+/* ------------------------------------------------------------------ */
+/* deryr2: cfdiff.f:518-601 */
+static void deryr2_c(const lmo *o, const cplx *u, cplx *du, double *w1, double *w2, double *t1, double *t2) {
+  int my = o->my;
+  for (int j = 0; j < my; j++) { t1[j] = creal(u[j]); t2[j] = cimag(u[j]); }
+  matvec7(o->dt12, my, t1, w1); matvec7(o->dt12, my, t2, w2);
+  banbks7(o->prem1, my, w1); banbks7(o->prem1, my, w2);
+  for (int j = 0; j < my; j++) du[j] = w1[j] * o->fmap[j] + I * (w2[j] * o->fmap[j]);
+}
+/* deryyr2: cfdiff.f:735-797 */
+static void deryyr2_c(const lmo *o, const cplx *u, cplx *du, double *w1, double *w2, double *t1, double *t2) {
+  int my = o->my;
+  for (int j = 0; j < my; j++) { t1[j] = creal(u[j]); t2[j] = cimag(u[j]); }
+  matvec5(o->dt22, my, t1, w1); matvec5(o->dt22, my, t2, w2);
+  banbks(o->prem3, my, w1); banbks(o->prem3, my, w2);
+  for (int j = 0; j < my; j++) du[j] = w1[j] + I * w2[j];
+}
+
+/* deryr / deryyr on one real FP64 vector: cfdiff.f:615-710 */
+void lmo_deryr(const lmo *o, const double *u, double *du) {
+  double *f = malloc(sizeof(double) * o->my);
+  matvec7(o->dt12, o->my, u, f);
+  banbks7(o->prem1, o->my, f);
+  for (int j = 0; j < o->my; j++) du[j] = f[j] * o->fmap[j];
+  free(f);
+}
+void lmo_deryyr(const lmo *o, const double *u, double *du) {
+  double *f = malloc(sizeof(double) * o->my);
+  matvec5(o->dt22, o->my, u, f);
+  banbks(o->prem3, o->my, f);
+  memcpy(du, f, sizeof(double) * o->my);
+  free(f);
+}
+
+/* inty8: laps.f:484-575.  Integrates du once with the compact scheme,
+ * u(1) = 0. */
+void lmo_inty8(const lmo *o, const double *du, double *u) {
+  int my = o->my;
+  double *wk2 = malloc(sizeof(double) * 7 * my), *f = malloc(sizeof(double) * my), *v = malloc(sizeof(double) * my);
+  memcpy(wk2, o->dt12, sizeof(double) * 7 * my);
+  bandec7(wk2, my);
+  /* dt12 annihilates constants, so the last pivot of its LU is zero in
+   * exact arithmetic and round-off as computed by laps.f:523.  Only
+   * u - u(1) is used (laps.f:567-571) and it does not depend on the last
+   * unknown: set the reciprocal last pivot to 0 (last unknown = 0). */
+  B7(wk2, 1, my) = 0.0;
+  for (int j = 0; j < my; j++) f[j] = du[j] / o->fmap[j];
+  matvec7(o->dt11, my, f, v);
+  banbks7(wk2, my, v);
+  for (int j = 0; j < my; j++) u[j] = v[j] - v[0];
+  free(wk2); free(f); free(v);
+}
+
+/* calcrhslap: laps.f:17-47 (rows 1 and my zeroed) */
+static void calcrhslap(const lmo *o, const double *f, double *r) {
+  int my = o->my;
+  matvec5(o->dt21, my, f, r);
+  r[0] = 0.0;
+  r[my - 1] = 0.0;
+}
+
+/* Poisson operator wk1 = dt22 - rK*dt21 with identity rows 1 and my,
+ * factorised with bandec: laps.f:349-366 / laps.f:648-665. */
+static void poisson_factor(const lmo *o, double rk, double *wk1) {
+  int my = o->my;
+  for (int j = 2; j <= my - 1; j++)
+    for (int i = 1; i <= 5; i++) B5(wk1, i, j) = B5(o->dt22, i, j) - rk * B5(o->dt21, i, j);
+  for (int i = 1; i <= 5; i++) { B5(wk1, i, 1) = 0.0; B5(wk1, i, my) = 0.0; }
+  B5(wk1, 3, 1) = 1.0;
+  B5(wk1, 3, my) = 1.0;
+  bandec(wk1, my);
+}
+
+/* Lapvdvhom: laps.f:319-477.  Solves v'' - rK v = phi with v=0 at both
+ * walls and returns v and dv/dy (rK=0 -> zeros). */
+static void lapvdvhom_c(const lmo *o, const cplx *phi, cplx *v, cplx *dvdy, double rk, double *scratch) {
+  int my = o->my;
+  if (rk == 0.0) {
+    for (int j = 0; j < my; j++) { v[j] = 0; dvdy[j] = 0; }
+    return;
+  }
+  double *wk1 = scratch, *d1 = scratch + 5 * my, *d2 = d1 + my, *f1 = d2 + my, *f2 = f1 + my, *fw = f2 + my;
+  poisson_factor(o, rk, wk1);
+  for (int j = 0; j < my; j++) { d1[j] = creal(phi[j]); d2[j] = cimag(phi[j]); }
+  matvec5(o->dt21, my, d1, f1); matvec5(o->dt21, my, d2, f2);
+  f1[0] = 0; f2[0] = 0; f1[my - 1] = 0; f2[my - 1] = 0;
+  banbks(wk1, my, f1);
+  banbks(wk1, my, f2);
+  for (int j = 0; j < my; j++) v[j] = f1[j] + I * f2[j];
+  matvec7(o->dt12, my, f1, fw); banbks7(o->prem1, my, fw);
+  for (int j = 0; j < my; j++) d1[j] = fw[j] * o->fmap[j];
+  matvec7(o->dt12, my, f2, fw); banbks7(o->prem1, my, fw);
+  for (int j = 0; j < my; j++) dvdy[j] = d1[j] + I * (fw[j] * o->fmap[j]);
+}
+
+/* solvepsi: laps.f:580-730.  Solves psi'' - rK psi = phi with
+ * dpsi/dy = 0 at both walls (influence-matrix method with two
+ * homogeneous solutions and a 2x2 gaussj), returns psi and dpsi/dy. */
+static void solvepsi_c(const lmo *o, const cplx *phi, cplx *v, cplx *dvdy, double rk, double *scratch) {
+  int my = o->my;
+  if (rk == 0.0) {
+    for (int j = 0; j < my; j++) { v[j] = 0; dvdy[j] = 0; }
+    return;
+  }
+  const double Cvtop = 0.0, Cdyvtop = 1.0, BC_top = 0.0, Cvbot = 0.0, Cdyvbot = 1.0, BC_bot = 0.0;
+  double *wk1 = scratch, *v1 = wk1 + 5 * my, *v2 = v1 + my, *vpr = v2 + my, *vpi = vpr + my;
+  double *dvpr = vpi + my, *dvpi = dvpr + my, *dv1 = dvpi + my, *dv2 = dv1 + my;
+  poisson_factor(o, rk, wk1);
+  for (int j = 0; j < my; j++) { v1[j] = creal(phi[j]); v2[j] = cimag(phi[j]); }
+  calcrhslap(o, v1, vpr);
+  calcrhslap(o, v2, vpi);
+  v1[0] = 1.0; v2[0] = 0.0;
+  for (int j = 1; j < my - 1; j++) { v1[j] = 0.0; v2[j] = 0.0; }
+  v1[my - 1] = 0.0; v2[my - 1] = 1.0;
+  banbks(wk1, my, vpr); banbks(wk1, my, vpi); banbks(wk1, my, v1); banbks(wk1, my, v2);
+  matvec7(o->dt12, my, vpr, dvpr); matvec7(o->dt12, my, vpi, dvpi);
+  matvec7(o->dt12, my, v1, dv1); matvec7(o->dt12, my, v2, dv2);
+  banbks7(o->prem1, my, dvpr); banbks7(o->prem1, my, dvpi);
+  banbks7(o->prem1, my, dv1); banbks7(o->prem1, my, dv2);
+  double AA[4], coef[4];
+  const double *fm = o->fmap;
+  AA[0] = Cvbot + Cdyvbot * dv1[0] * fm[0];          /* AA(1,1) */
+  AA[2] = Cdyvbot * dv2[0] * fm[0];                  /* AA(1,2) */
+  AA[1] = Cdyvtop * dv1[my - 1] * fm[my - 1];        /* AA(2,1) */
+  AA[3] = Cvtop + Cdyvtop * dv2[my - 1] * fm[my - 1]; /* AA(2,2) */
+  coef[0] = BC_bot - Cdyvbot * dvpr[0] * fm[0];
+  coef[1] = BC_top - Cdyvtop * dvpr[my - 1] * fm[my - 1];
+  coef[2] = BC_bot - Cdyvbot * dvpi[0] * fm[0];
+  coef[3] = BC_top - Cdyvtop * dvpi[my - 1] * fm[my - 1];
+  gaussj(AA, 2, 2, coef, 2, 2);
+  for (int j = 0; j < my; j++) {
+    v[j] = (vpr[j] + coef[0] * v1[j] + coef[1] * v2[j]) + I * (vpi[j] + coef[2] * v1[j] + coef[3] * v2[j]);
+    dvdy[j] = fm[j] * (dvpr[j] + coef[0] * dv1[j] + coef[1] * dv2[j]) +
+              I * (fm[j] * (dvpi[j] + coef[2] * dv1[j] + coef[3] * dv2[j]));
+  }
+}
+
+void lmo_lapvdvhom(const lmo *o, const double *phi, double *v, double *dvdy, double rk) {
+  double *s = malloc(sizeof(double) * 16 * o->my);
+  lapvdvhom_c(o, (const cplx *)phi, (cplx *)v, (cplx *)dvdy, rk, s);
+  free(s);
+}
+void lmo_solvepsi(const lmo *o, const double *phi, double *v, double *dvdy, double rk) {
+  double *s = malloc(sizeof(double) * 16 * o->my);
+  solvepsi_c(o, (const cplx *)phi, (cplx *)v, (cplx *)dvdy, rk, s);
+  free(s);
+}
+
+/* ------------------------------------------------------------------ */
+/* Transforms (fou3D.f)                                                 */
+/* ------------------------------------------------------------------ */
+/* spectral kz index -> padded physical-FFT index (localyz2zy,
+ * fou3D.f:103-145): k<=nz1 stays, k>nz1 moves to k+(mgalz-mz). */
+static inline int kz_pad(const lmo *o, int k) { return k <= o->nz1 ? k : k + (o->mgalz - o->mz); }
+
+/* foup2 inverse half for one kx plane: localyz2zy + fourz(+1)
+ * (fou3D.f:80-145), writing the x-lines buffer [line][kx]. */
+static void zinv_plane(const lmo *o, int i, const cplx *spec, cplx *lines, cplx *buf, cplx *out) {
+  int my = o->my, mgalz = o->mgalz, nkx = o->nkx;
+  for (int j = 0; j < my; j++) {
+    for (int z = 0; z < mgalz; z++) buf[z] = 0;
+    for (int k = 0; k < o->mz; k++) buf[kz_pad(o, k)] = spec[SIDX(o, i, k, j)];
+    cfft(&o->pz, buf, out, +1);
+    for (int z = 0; z < mgalz; z++) lines[((size_t)j * mgalz + z) * nkx + i] = out[z];
+  }
+}
+/* foup2 forward half: fourz(-1) + truncation + localzy2yz (fou3D.f:149-189) */
+static void zfwd_plane(const lmo *o, int i, const cplx *lines, cplx *spec, cplx *buf, cplx *out) {
+  int my = o->my, mgalz = o->mgalz, nkx = o->nkx;
+  double dn = 1.0 / (double)mgalz;
+  for (int j = 0; j < my; j++) {
+    for (int z = 0; z < mgalz; z++) buf[z] = lines[((size_t)j * mgalz + z) * nkx + i];
+    cfft(&o->pz, buf, out, -1);
+    for (int k = 0; k < o->mz; k++) spec[SIDX(o, i, k, j)] = out[kz_pad(o, k)] * dn;
+  }
+}
+
+/* fourx inverse (fou3D.f:29-60 + rftsingle.f:25-95) of two lines at once:
+ * kx modes 0..nkx-1 (Im of mode 0 dropped, higher modes zero) -> two real
+ * lines, via one complex transform of A + iB. */
+static void xinv2(const lmo *o, const cplx *A, const cplx *B, double *a, double *b, cplx *buf, cplx *out) {
+  int n = o->mgalx, nk = o->nkx;
+  for (int k = 0; k < n; k++) buf[k] = 0;
+  buf[0] = creal(A[0]) + I * creal(B[0]);
+  for (int k = 1; k < nk; k++) {
+    buf[k] = A[k] + I * B[k];
+    buf[n - k] = conj(A[k]) + I * conj(B[k]);
+  }
+  cfft(&o->px, buf, out, +1);
+  for (int x = 0; x < n; x++) { a[x] = creal(out[x]); b[x] = cimag(out[x]); }
+}
+/* fourx direct of two real lines, scaled by 1/n, truncated to kx<nkx and
+ * Im(mode 0) = 0 (rftsingle.f:62-72, fou3D.f:43-46, cross.f:1723-1760). */
+static void xfwd2(const lmo *o, const double *a, const double *b, cplx *A, cplx *B, cplx *buf, cplx *out) {
+  int n = o->mgalx, nk = o->nkx;
+  double dn = 1.0 / (double)n;
+  for (int x = 0; x < n; x++) buf[x] = a[x] + I * (b ? b[x] : 0.0);
+  cfft(&o->px, buf, out, -1);
+  A[0] = creal(out[0]) * dn;
+  if (B) B[0] = cimag(out[0]) * dn;
+  for (int k = 1; k < nk; k++) {
+    cplx c1 = out[k], c2 = conj(out[n - k]);
+    A[k] = 0.5 * (c1 + c2) * dn;
+    if (B) B[k] = -0.5 * I * (c1 - c2) * dn;
+  }
+}
+
+/* Public single-vector FFT entry points for the golden-vector tests. */
+void lmo_cft(int n, double *c, int iopt) {
+  fftplan p; plan_init(&p, n);
+  cplx *in = malloc(sizeof(cplx) * n), *out = malloc(sizeof(cplx) * n);
+  memcpy(in, c, sizeof(cplx) * n);
+  cfft(&p, in, out, iopt < 0 ? -1 : +1);
+  double s = iopt < 0 ? 1.0 / n : 1.0;
+  for (int k = 0; k < n; k++) { c[2 * k] = creal(out[k]) * s; c[2 * k + 1] = cimag(out[k]) * s; }
+  free(in); free(out); plan_free(&p);
+}
+void lmo_rft(int n, double *c, int iopt) {
+  fftplan p; plan_init(&p, n);
+  cplx *in = malloc(sizeof(cplx) * n), *out = malloc(sizeof(cplx) * n);
+  if (iopt < 0) {
+    for (int x = 0; x < n; x++) in[x] = c[x];
+    cfft(&p, in, out, -1);
+    for (int k = 0; k <= n / 2; k++) { c[2 * k] = creal(out[k]) / n; c[2 * k + 1] = cimag(out[k]) / n; }
+    c[1] = 0.0;
+    c[n + 1] = 0.0;
+  } else {
+    for (int k = 0; k < n; k++) in[k] = 0;
+    in[0] = c[0];
+    for (int k = 1; k < n / 2; k++) { in[k] = c[2 * k] + I * c[2 * k + 1]; in[n - k] = conj(in[k]); }
+    in[n / 2] = c[n];
+    cfft(&p, in, out, +1);
+    for (int x = 0; x < n; x++) c[x] = creal(out[x]);
+  }
+  free(in); free(out); plan_free(&p);
+}
+
+/* ------------------------------------------------------------------ */
+/* phys2: cross.f:1440-1828.  Per (z,y) line: 8 inverse x-transforms,  */
+/* FP64 products, T update, d(rho)/dt source, CFL maxima, 11 direct    */
+/* x-transforms with dealiasing.                                       */
+/* lines in : 0 rhou 1 rhov 2 rhow 3 lapT 4 dTdx 5 dTdy 6 dTdz 7 T       */
+/* lines out: 0 u 1 v 2 w 3 rhouu 4 rhovv 5 rhoww 6 rhouv 7 rhouw       */
+/*            8 rhovw 9 drho 10 DT                                     */
+/* ------------------------------------------------------------------ */
+static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, int do_cfl, int do_mass,
+                  double *cflout /*4*/, double *rhom /*my*/) {
+  int mgalx = o->mgalx, mgalz = o->mgalz, my = o->my, nkx = o->nkx;
+  size_t nlines = (size_t)mgalz * my;
+  double cflx = 0, cfly = 0, cflz = 0, cflT = 0;
+  double hxalp = o->alp * (mgalx - 1) / M_PI, hzbet = o->bet * (mgalz - 1) / M_PI;
+  double ab = o->alpha[rk] / o->beta[rk];
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *ph = malloc(sizeof(double) * mgalx * 8), *out = malloc(sizeof(double) * mgalx * 12);
+    cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
+    cplx *spec = malloc(sizeof(cplx) * nkx * 12);
+#pragma omp for schedule(static)
+    for (long L = 0; L < (long)nlines; L++) {
+      int jj = (int)(L / mgalz); /* y index (cross.f:1583) */
+      cplx *sp[8];
+      for (int f = 0; f < 8; f++) sp[f] = o->ln[f] + (size_t)L * nkx;
+      double *p[8];
+      for (int f = 0; f < 8; f++) p[f] = ph + (size_t)f * mgalx;
+      xinv2(o, sp[0], sp[1], p[0], p[1], buf, fo);
+      xinv2(o, sp[2], sp[3], p[2], p[3], buf, fo);
+      xinv2(o, sp[4], sp[5], p[4], p[5], buf, fo);
+      xinv2(o, sp[6], sp[7], p[6], p[7], buf, fo);
+      double *ru = p[0], *rv = p[1], *rw = p[2], *lapT = p[3], *tx = p[4], *ty = p[5], *tz = p[6], *T = p[7];
+      double *rh = o->rhst + (size_t)L * mgalx;
+      double *q[11];
+      for (int f = 0; f < 11; f++) q[f] = out + (size_t)f * mgalx;
+      double lmx = 0, lmy = 0, lmz = 0, Tmax = 0, rsum = 0;
+      for (int x = 0; x < mgalx; x++) {
+        double u = ru[x] * T[x], v = rv[x] * T[x], w = rw[x] * T[x]; /* cross.f:1613-1622 */
+        double tnext = T[x] + dtxi * rh[x];                            /* cross.f:1625-1629 */
+        double d8 = dtxi * rh[x];
+        double rhs = -u * tx[x] - v * ty[x] - w * tz[x] + T[x] * lapT[x] / o->peclet; /* cross.f:1631-1637 */
+        rh[x] = rhs;
+        tnext = tnext + dtgamma * rhs; /* cross.f:1640-1643 */
+        d8 = d8 + dtgamma * rhs;
+        q[10][x] = d8;                     /* DT (cross.f:1645-1647) */
+        q[0][x] = u; q[1][x] = v; q[2][x] = w;
+        q[3][x] = ru[x] * u; q[4][x] = rv[x] * v; q[5][x] = rw[x] * w; /* cross.f:1655-1659 */
+        q[6][x] = ru[x] * v; q[7][x] = ru[x] * w; q[8][x] = rv[x] * w; /* cross.f:1662-1666 */
+        q[9][x] = (d8 / (T[x] * tnext)) / dtbeta - ab * rhs / (T[x] * T[x]); /* cross.f:1669-1673 */
+        if (do_cfl) {
+          lmx = fmax(lmx, fabs(u)); lmy = fmax(lmy, fabs(v)); lmz = fmax(lmz, fabs(w)); Tmax = fmax(Tmax, T[x]);
+        }
+        if (do_mass) rsum += 1.0 / T[x];
+      }
+      if (do_cfl) { /* cross.f:1690-1708 */
+        double DD = 1.0 / o->peclet * Tmax;
+        double c0 = lmy / o->hy[jj];
+        double cT = 2 * DD * ((hxalp / 2) * (hxalp / 2) + (hzbet / 2) * (hzbet / 2) + (1 / o->hy[jj]) * (1 / o->hy[jj]));
+#pragma omp critical
+        {
+          cflx = fmax(cflx, lmx); cflz = fmax(cflz, lmz); cfly = fmax(cfly, c0); cflT = fmax(cflT, cT);
+        }
+      }
+      if (do_mass) {
+#pragma omp atomic
+        rhom[jj] += rsum;
+      }
+      cplx *so[11];
+      for (int f = 0; f < 11; f++) so[f] = spec + (size_t)f * nkx;
+      for (int f = 0; f < 10; f += 2) xfwd2(o, q[f], q[f + 1], so[f], so[f + 1], buf, fo);
+      xfwd2(o, q[10], NULL, so[10], NULL, buf, fo);
+      for (int f = 0; f < 11; f++) memcpy(o->ln[f] + (size_t)L * nkx, so[f], sizeof(cplx) * nkx);
+    }
+    free(ph); free(out); free(buf); free(fo); free(spec);
+  }
+  cflout[0] = cflx; cflout[1] = cfly; cflout[2] = cflz; cflout[3] = cflT;
+}
+
+/* foup2: cross.f:1282-1430 */
+static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, int do_cfl, int do_diag,
+                  cplx *in8[8], cplx *out11[11]) {
+  int nkx = o->nkx, mgalz = o->mgalz;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for collapse(2) schedule(static)
+    for (int f = 0; f < 8; f++)
+      for (int i = 0; i < nkx; i++) zinv_plane(o, i, in8[f], o->ln[f], buf, out);
+    free(buf); free(out);
+  }
+  double cfl[4];
+  double *rhom = xcalloc(o->my, 8);
+  phys2(o, rk, dtxi, dtgamma, dtbeta, do_cfl, do_diag, cfl, rhom);
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for collapse(2) schedule(static)
+    for (int f = 0; f < 11; f++)
+      for (int i = 0; i < nkx; i++) zfwd_plane(o, i, o->ln[f], out11[f], buf, out);
+    free(buf); free(out);
+  }
+  if (do_diag) {
+    /* momentum thickness: cross.f:1416-1429 (u00 = out11[0] mode 00) */
+    const cplx *u = out11[0];
+    int my = o->my;
+    double dm = 0.0;
+    for (int j = 1; j <= my - 2; j++) {
+      double a = creal(u[j + 1]), b = creal(u[j - 1]);
+      dm += o->trp[j] * (a * a + b * b);
+    }
+    {
+      double a = creal(u[1]), b = creal(u[0]), c = creal(u[my - 1]), d = creal(u[my - 2]);
+      dm += o->trp[0] * (a * a + b * b) + o->trp[my - 1] * (c * c + d * d);
+    }
+    double du = creal(u[my - 1]) - creal(u[0]);
+    o->diag[2] = 0.25 * (o->y[my - 1] - o->y[0]) - dm / (du * du);
+    /* masst: escru.f:372-376 with one accumulation (plane mean of 1/T) */
+    double fac = 1.0 / ((double)o->mgalx * o->mgalz), mt = 0.0;
+    for (int j = 0; j < my; j++) mt += fac * rhom[j] * o->hy[j];
+    o->diag[6] = mt;
+  }
+  free(rhom);
+  if (do_cfl) { /* cross.f:1778-1826, single compute rank */
+    double hxalp = o->alp * (o->mgalx - 1) / M_PI, hzbet = o->bet * (o->mgalz - 1) / M_PI;
+    double cflx = cfl[0] * hxalp * 0.5, cflz = cfl[2] * hzbet * 0.5;
+    double reig = cflx + cfl[1] + cflz + cfl[3];
+    o->dtr = (double)(float)(o->cfl / reig); /* dtr is real*4 */
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* One RK3 substep: cross.f:307-1141                                   */
+/* ------------------------------------------------------------------ */
+static void substep(lmo *o, int r /*0..2*/, int ihist) {
+  int my = o->my, nkx = o->nkx, mz = o->mz;
+  double dtxi = o->Deltat * o->xi[r], dtgamma = o->Deltat * o->gama[r], dtbeta = o->Deltat * o->beta[r];
+  double ire = o->ire;
+  /* BCs: cross.f:315-349 */
+  for (int m = 0; m < o->nmode; m++) {
+    cplx *vv = o->vor + (size_t)m * my, *pp = o->phi + (size_t)m * my, *ss = o->scal + (size_t)m * my;
+    vv[0] = vv[1];
+    vv[my - 1] = vv[my - 2];
+    pp[0] = 0; pp[my - 1] = 0;
+    ss[0] = 0; ss[my - 1] = 0;
+  }
+  o->scal[0] = 1.0 / o->rhobot;
+  o->scal[my - 1] = 1.0 / o->rhotop;
+
+  cplx *mxw = o->w_mx, *myw = o->w_my, *mzw = o->w_mz, *nxw = o->w_nx, *nyw = o->w_ny, *nzw = o->w_nz;
+  cplx *t12 = o->w_t12, *t13 = o->w_t13, *t23 = o->w_t23, *drho = o->w_drho, *chwk = o->w_chwk, *chwk2 = o->w_chwk2;
+
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 20 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
+      size_t b = (size_t)m * my;
+      /* save vor and psi: cross.f:353-360 */
+      for (int j = 0; j < my; j++) { nxw[b + j] = o->vor[b + j]; nyw[b + j] = o->psi[b + j]; }
+      /* (1) Lapvdvhom: cross.f:365-372 */
+      lapvdvhom_c(o, o->phi + b, myw + b, nzw + b, rK, sc);
+      /* (2) mx, mz: cross.f:395-407 ; tempa=i kx/k2, tempb=i kz/k2 (cross.f:133-154) */
+      cplx ta = 0, tb = 0;
+      if (rK != 0.0) { ta = I * kx / rK; tb = I * kz / rK; }
+      for (int j = 0; j < my; j++) {
+        mxw[b + j] = nzw[b + j] * ta - nxw[b + j] * tb;
+        mzw[b + j] = nzw[b + j] * tb + nxw[b + j] * ta;
+      }
+      /* drho = scal: cross.f:410-416 ; xi-update: cross.f:420-430 */
+      for (int j = 0; j < my; j++) {
+        drho[b + j] = o->scal[b + j];
+        o->vor[b + j] = o->vor[b + j] + o->ten12p[b + j] * dtxi;
+        o->phi[b + j] = o->phi[b + j] + o->ten13p[b + j] * dtxi;
+      }
+      /* d(psi)/dy: cross.f:434-437 */
+      deryr2_c(o, nyw + b, t23 + b, w1, w2, tt1, tt2);
+      /* rho u_i: cross.f:463-482 */
+      for (int j = 0; j < my; j++) {
+        mxw[b + j] = mxw[b + j] + I * kx * nyw[b + j];
+        mzw[b + j] = mzw[b + j] + I * kz * nyw[b + j];
+        myw[b + j] = myw[b + j] + t23[b + j];
+      }
+      /* T derivatives: cross.f:521-554 */
+      deryr2_c(o, drho + b, t13 + b, w1, w2, tt1, tt2);
+      deryyr2_c(o, drho + b, nyw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        nyw[b + j] = nyw[b + j] - rK * drho[b + j];
+        t23[b + j] = I * kz * drho[b + j];
+        t12[b + j] = I * kx * drho[b + j];
+      }
+    }
+    free(s);
+  }
+  /* 00 modes into rho u_i, then xi-update of u00/w00: cross.f:486-499 */
+  for (int j = 0; j < my; j++) {
+    mxw[j] = o->u00wk[j];
+    myw[j] = o->v00wk[j];
+    mzw[j] = o->w00wk[j];
+  }
+  for (int j = 1; j < my - 1; j++) {
+    o->u00wk[j] += dtxi * o->rf0u[j];
+    o->w00wk[j] += dtxi * o->rf0w[j];
+  }
+  /* (5) foup2 */
+  int do_cfl = (r == 0 && o->icfl == 1 && o->dtmode == 0);
+  cplx *in8[8] = {mxw, myw, mzw, nyw, t12, t13, t23, drho};
+  cplx *out11[11] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, drho, chwk2};
+  foup2(o, r, dtxi, dtgamma, dtbeta, do_cfl, ihist && r == 0, in8, out11);
+
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 20 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k];
+      size_t b = (size_t)m * my;
+      /* (6a) T update: cross.f:619-627 */
+      for (int j = 0; j < my; j++) o->scal[b + j] = o->scal[b + j] + chwk2[b + j];
+      /* (6b) Nx, Ny, Nz: cross.f:652-682 */
+      deryr2_c(o, nyw + b, nyw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) nyw[b + j] = -I * kx * t12[b + j] - nyw[b + j] - I * kz * t23[b + j];
+    }
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k];
+      size_t b = (size_t)m * my;
+      deryr2_c(o, t12 + b, t12 + b, w1, w2, tt1, tt2);
+      deryr2_c(o, t23 + b, t23 + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        nxw[b + j] = -I * kx * nxw[b + j] - t12[b + j] - I * kz * t13[b + j];
+        nzw[b + j] = -I * kx * t13[b + j] - t23[b + j] - I * kz * nzw[b + j];
+      }
+    }
+    free(s);
+  }
+  /* 00 modes: cross.f:686-722 */
+  {
+    double *dudy = xcalloc(my, 8);
+    for (int j = 0; j < my; j++) { o->rf0u[j] = creal(mxw[j]); o->rf0w[j] = creal(mzw[j]); }
+    if (r == 2 && ihist) {
+      lmo_deryr(o, o->rf0u, dudy);
+      double dw = 0.0;
+      for (int j = 0; j < my; j++) dw = fmax(fabs(dudy[j]), dw);
+      o->diag[3] = 1.0 / dw;
+      o->diag[4] = o->diag[3] * o->Re;
+    }
+    lmo_deryyr(o, o->rf0u, o->rf0u);
+    lmo_deryyr(o, o->rf0w, o->rf0w);
+    for (int j = 0; j < my; j++) {
+      o->rf0u[j] = -creal(t12[j]) + ire * o->rf0u[j];
+      o->rf0w[j] = -creal(t23[j]) + ire * o->rf0w[j];
+    }
+    if (r == 2 && ihist) {
+      double hu = 0, hw = 0;
+      for (int j = 0; j < my; j++) { hu += o->rf0u[j] * o->hy[j]; hw += o->rf0w[j] * o->hy[j]; }
+      o->diag[10] = 0.25 * hu;
+      o->diag[11] = 0.25 * hw;
+    }
+    free(dudy);
+  }
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 24 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
+      size_t b = (size_t)m * my;
+      /* vorticities: cross.f:748-767 */
+      deryr2_c(o, mxw + b, t12 + b, w1, w2, tt1, tt2);
+      deryr2_c(o, mzw + b, t23 + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        t23[b + j] = t23[b + j] - I * kz * myw[b + j];
+        t13[b + j] = I * kz * mxw[b + j] - I * kx * mzw[b + j];
+        t12[b + j] = I * kx * myw[b + j] - t12[b + j];
+      }
+      /* Laplacians: cross.f:821-857 */
+      deryyr2_c(o, t13 + b, chwk + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t13[b + j] = chwk[b + j] - rK * t13[b + j];
+      for (int j = 0; j < my; j++) t23[b + j] = I * kz * t23[b + j] - I * kx * t12[b + j];
+      deryyr2_c(o, t23 + b, chwk + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t23[b + j] = chwk[b + j] - rK * t23[b + j];
+      /* RHS(Omega_y), RHS(phi): cross.f:885-921 */
+      for (int j = 0; j < my; j++) t12[b + j] = I * kz * nxw[b + j] - I * kx * nzw[b + j] + ire * t13[b + j];
+      for (int j = 0; j < my; j++) nxw[b + j] = I * kx * nxw[b + j] + I * kz * nzw[b + j];
+      deryr2_c(o, nxw + b, nxw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t13[b + j] = -rK * nyw[b + j] - nxw[b + j] - ire * t23[b + j];
+      /* RK3 update: cross.f:966-981 */
+      for (int j = 0; j < my; j++) {
+        o->vor[b + j] = o->vor[b + j] + dtgamma * t12[b + j];
+        o->phi[b + j] = o->phi[b + j] + dtgamma * t13[b + j];
+        o->ten12p[b + j] = t12[b + j];
+        o->ten13p[b + j] = t13[b + j];
+      }
+      /* psi(n+1): cross.f:1092-1104 */
+      solvepsi_c(o, drho + b, o->psi + b, chwk + b, rK, sc);
+    }
+    free(s);
+  }
+  /* 00 modes: cross.f:1006-1074 */
+  {
+    for (int j = 1; j < my - 1; j++) {
+      o->u00wk[j] += dtgamma * o->rf0u[j];
+      o->w00wk[j] += dtgamma * o->rf0w[j];
+    }
+    double mu = 0, mv = 0, mw = 0;
+    for (int j = 0; j < my; j++) {
+      mu += o->u00wk[j] * o->hy[j];
+      mv += o->v00wk[j] * o->hy[j];
+      mw += o->w00wk[j] * o->hy[j];
+    }
+    o->diag[7] = mu; o->diag[8] = mv; o->diag[9] = mw;
+    double *d00 = xcalloc(my, 8);
+    for (int j = 0; j < my; j++) d00[j] = creal(drho[j]);
+    lmo_inty8(o, d00, o->rf0v);
+    double trapz = -o->rf0v[my - 1];
+    o->diag[5] = trapz;
+    for (int j = 0; j < my; j++) o->v00wk[j] = o->rf0v[j] + trapz / (1.0 + sqrt(o->rhotop / o->rhobot));
+    free(d00);
+  }
+  (void)nkx;
+}
+
+/* Time loop body: cross.f:225-1226 (stats, images and .cf output are the
+ * caller's business). */
+int lmo_step(lmo *o, int nsteps) {
+  for (int s = 0; s < nsteps; s++) {
+    int istep = ++o->istep_total;
+    if (o->dtmode == 0 && (istep - 1) % o->ncfl == 0) o->icfl = 1;
+    int ihist = 1; /* diagnostics every step */
+    o->diag[0] = o->time;
+    o->diag[1] = o->Deltat;
+    for (int r = 0; r < 3; r++) substep(o, r, ihist);
+    o->time += o->Deltat;
+    if (o->dtmode == 0 && o->icfl == 1) {
+      o->icfl = 0;
+      o->Deltat = o->dtr;
+    }
+    o->diag[12] = o->Deltat;
+  }
+  return 0;
+}
+
+/* One substep with RK coefficient r (0..2) on the current state, without
+ * the step bookkeeping: used only to time bounded CPU samples. */
+int lmo_substep(lmo *o, int r) {
+  if (r < 0 || r > 2) return -1;
+  substep(o, r, 0);
+  return 0;
+}
+
+void lmo_get_diag(const lmo *o, double *d) { memcpy(d, o->diag, sizeof(double) * LMO_NDIAG); }
+
+void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12, double *prem3_lu,
+                   double *dt21, double *dt22, double *fmap) {
+  size_t n7 = (size_t)7 * o->my, n5 = (size_t)5 * o->my;
+  if (prem1_lu) memcpy(prem1_lu, o->prem1, n7 * 8);
+  if (dt11) memcpy(dt11, o->dt11, n7 * 8);
+  if (dt12) memcpy(dt12, o->dt12, n7 * 8);
+  if (prem3_lu) memcpy(prem3_lu, o->prem3, n5 * 8);
+  if (dt21) memcpy(dt21, o->dt21, n5 * 8);
+  if (dt22) memcpy(dt22, o->dt22, n5 * 8);
+  if (fmap) memcpy(fmap, o->fmap, (size_t)o->my * 8);
+}

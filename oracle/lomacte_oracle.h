@@ -1,0 +1,84 @@
+/*
+ * lomacte_oracle.h -- CPU FP64 oracle for the lomacte RK3 substep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference legs of bench.py load this library, always as the
+ * checker or as the timed CPU baseline; the product (loma_phd_b200) never
+ * links, imports or executes it.
+ *
+ * What it is: a statement-by-statement FP64 restatement of the reference
+ * Fortran lomacte3 substep (Beovulfo/LoMa_phD trunk/lomacte3/src):
+ *   cross.f:307-1141 (cross1 RK3 substep), cross.f:1282-1430 (foup2),
+ *   cross.f:1440-1828 (phys2), laps.f:17-129,319-764 (Poisson solvers),
+ *   cfdiff.f:24-1223 (compact FD coefficients, band LU), fou3D.f:29-189
+ *   (transform wrappers, padding/truncation, kz ordering), main.f:689-800
+ *   (hy/trp weights, wavenumbers), modulos.f:193-209 (RK3 coefficients).
+ * The reference computes in FP32 with FP64 work vectors; this oracle keeps
+ * every quantity in FP64.  Its FFT is written from the DFT definition and
+ * pinned against the reference's own benchmark_fft golden vectors
+ * (branches/reactml/benchmark_fft/{cft,rfft}test_double.txt).  Parity of the
+ * full substep is pinned by restatement (the Fortran cannot be compiled in
+ * this environment: no Fortran compiler, no MPI).
+ *
+ * Field layout ("reference layout"): complex values interleaved re,im, in
+ * the order of the Fortran arrays vor(0:my-1,0:mz1,1:nplanes):
+ *   index(kx, kz, j) = ((kx*mz + kz)*my + j), y fastest.
+ */
+#ifndef LOMACTE_ORACLE_H
+#define LOMACTE_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lmo lmo;
+
+/* dtmode: 0 = reference CFL mode (Deltat starts at dt0 and is replaced by
+ * the CFL value computed every ncfl steps, rounded to FP32 as the
+ * reference's real*4 Deltat), 1 = fixed Deltat = dt0. */
+lmo *lmo_create(int mgalx, int mgalz, int my, const double *y, double Re,
+                double alp, double bet, double peclet, double cfl, int ncfl,
+                int dtmode, double dt0, int nthreads);
+void lmo_destroy(lmo *o);
+
+int lmo_set_state(lmo *o, const double *vor, const double *phi,
+                  const double *psi, const double *scal, const double *u00,
+                  const double *v00, const double *w00, double time);
+int lmo_get_state(const lmo *o, double *vor, double *phi, double *psi,
+                  double *scal, double *u00, double *v00, double *w00,
+                  double *time);
+/* Advance nsteps full RK3 steps (3 substeps each). */
+int lmo_step(lmo *o, int nsteps);
+
+/* One substep with RK coefficient r on the current state (timing samples). */
+int lmo_substep(lmo *o, int r);
+
+/* Diagnostics of the last step, in this order:
+ * 0 time (before the step), 1 Deltat used, 2 dm, 3 dw, 4 Re*dw, 5 trapz,
+ * 6 masst, 7 massu, 8 massv, 9 massw, 10 H00u, 11 H00w, 12 next Deltat */
+#define LMO_NDIAG 13
+void lmo_get_diag(const lmo *o, double *d);
+
+/* Coefficient access for tests (band storage row-major [row][band]). */
+void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12,
+                   double *prem3_lu, double *dt21, double *dt22, double *fmap);
+/* 1-D FP64 y-operators on one real vector (deryr / deryyr / inty8). */
+void lmo_deryr(const lmo *o, const double *u, double *du);
+void lmo_deryyr(const lmo *o, const double *u, double *du);
+void lmo_inty8(const lmo *o, const double *du, double *u);
+/* One (kx,kz) mode: Lapvdvhom / solvepsi on complex vectors (re,im). */
+void lmo_lapvdvhom(const lmo *o, const double *phi, double *v, double *dvdy,
+                   double rk);
+void lmo_solvepsi(const lmo *o, const double *phi, double *v, double *dvdy,
+                  double rk);
+
+/* FFT conventions of rftsingle.f / cftsingle.f (forward scaled by 1/n).
+ * c2c: in-place on n complex (re,im interleaved), sign<0 forward.
+ * rft forward: x[n] real -> packed[n+2] = (Re X0, 0, Re X1, Im X1, ...,
+ *   Re X_{n/2}, 0); rft inverse: packed -> x[n]. */
+void lmo_cft(int n, double *c, int iopt);
+void lmo_rft(int n, double *c, int iopt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

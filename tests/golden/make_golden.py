@@ -1,0 +1,51 @@
+"""Regenerate tests/golden/fft_rect_double.npz from the reference's own FFT
+golden vectors.
+
+Source (read as text; nothing of the reference is executed):
+  Beovulfo/LoMa_phD branches/reactml/benchmark_fft/cfttest_double.txt
+  Beovulfo/LoMa_phD branches/reactml/benchmark_fft/rffttest_double.txt
+written by branches/reactml/benchmark_fft/main.f:86-160 with Fortran format
+5E14.7 (several values per record, no separators between negative numbers).
+
+cfttest: triples (phys(k), Re fou(k), Im fou(k)), k=1..384: the rectangle
+  function and its direct c2c transform (cft, iopt=-1, scaled by 1/n).
+rffttest: pairs (physx(i), four(i)), i=1..768: four(1..768) is the packed
+  direct real transform (rft, iopt=-1) of the rectangle four(257:511)=1 with
+  four(385)=0.5 (main.f:128-138 sets four(k) with a stale index k=385, so the
+  two 0.5 end values land on element 385 and elements 256/512 stay 0).
+  physx(1) is overwritten by the transform's Nyquist slot (rft writes
+  element n+1 past the 768-long array), so only four(:) is kept.
+
+Usage: python tests/golden/make_golden.py [reference_root]
+"""
+import os
+import sys
+
+import numpy as np
+
+
+def parse_e14(path):
+    vals = []
+    with open(path) as f:
+        for line in f:
+            line = line.rstrip("\n")
+            for i in range(0, len(line), 14):
+                tok = line[i:i + 14].strip()
+                if tok:
+                    vals.append(float(tok))
+    return np.array(vals)
+
+
+def main():
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    d = os.path.join(root, "branches", "reactml", "benchmark_fft")
+    c = parse_e14(os.path.join(d, "cfttest_double.txt")).reshape(-1, 3)
+    r = parse_e14(os.path.join(d, "rffttest_double.txt")).reshape(-1, 2)
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "fft_rect_double.npz")
+    np.savez(out, cft_phys=c[:, 0], cft_re=c[:, 1], cft_im=c[:, 2],
+             rft_physx=r[:, 0], rft_four=r[:, 1])
+    print("wrote", out, c.shape, r.shape)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,79 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol of include/lomacte_b200.h, the seeded initial condition is
+deterministic and consistent, and the oracle advances it stably."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from loma_phd_b200 import ICParams, Params, make_ic, stretched_mesh
+from loma_phd_b200 import lomacte as lm
+from tests.helpers import case, oracle_for
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "lomacte_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(lmc_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol():
+    L = lm.lib()
+    syms = header_symbols()
+    assert set(syms) == set(lm.SYMBOLS)
+    for s in syms:
+        assert hasattr(L, s), s
+
+
+def test_strerror_and_nodev_paths():
+    L = lm.lib()
+    assert L.lmc_strerror(0) == b"ok"
+    assert L.lmc_strerror(-6) == b"no CUDA device"
+
+
+def test_create_without_gpu_fails_loudly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("GPU present")
+    except Exception:
+        pass
+    p = Params.from_modes(32, 32, 65)
+    with pytest.raises(lm.LomacteError) as e:
+        lm.Lomacte(p, stretched_mesh(p.my))
+    assert e.value.code == lm.LMC_ENODEV
+
+
+def test_ic_is_seeded_and_hermitian():
+    p, y, a = case(seed=3)
+    _, _, b = case(seed=3)
+    _, _, c = case(seed=4)
+    for k in ("vor", "phi", "psi", "scal"):
+        assert np.array_equal(a[k], b[k])
+    assert not np.array_equal(a["vor"], c["vor"])
+    # kx = 0 plane: field(-kz) = conj(field(kz)) so the physical field is real
+    mz = p.mz
+    for k in ("vor", "phi", "psi"):
+        f = a[k][0]
+        for kk in range(1, (mz - 1) // 2 + 1):
+            assert np.allclose(f[mz - kk], np.conj(f[kk]), atol=1e-15)
+    # T carries only the 00 mode, 1/rho00 with rho_bot/rho_top = s
+    assert np.count_nonzero(a["scal"]) == p.my
+    T = a["scal"][0, 0].real
+    assert abs(T[-1] / T[0] - 4.0) < 1e-3
+
+
+def test_oracle_runs_ic_stably():
+    p, y, st = case(nx=24, nz=24, ny=33)
+    o = oracle_for(p, y, st, nthreads=2)
+    o.step(3)
+    d = o.diag()
+    s = o.get_state()
+    for k in ("vor", "phi", "psi", "scal"):
+        assert np.isfinite(s[k]).all()
+    assert abs(d["masst"] - (y[-1] - y[0])) < 0.05
+    assert 3.5 < d["dw"] < 4.5
