@@ -255,9 +255,17 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     lmc_destroy(h);
     return rc;
   }
-  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess || lmc::kernels_init(d) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) {
     lmc_destroy(h);
     return LMC_ECUDA;
+  }
+  {
+    const cudaError_t e = lmc::kernels_init(d);
+    if (e != cudaSuccess) {
+      std::fprintf(stderr, "lomacte_b200: shared-memory opt-in failed: %s\n", cudaGetErrorString(e));
+      lmc_destroy(h);
+      return LMC_ECUDA;
+    }
   }
   cudaMemset(d.status, 0, sizeof(int));
   cudaMemset(d.diag, 0, 16 * sizeof(double));

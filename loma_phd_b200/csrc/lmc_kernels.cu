@@ -754,15 +754,26 @@ void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s)
   k_xphys<<<g, 256, xphys_smem(d), s>>>(d, zb, rk, do_cfl, do_diag);
 }
 
-// Opt-in to large dynamic shared memory (called once per process/device).
+// Opt-in to the largest dynamic shared memory each transform kernel can
+// use on this device (the opt-in limit minus the kernel's static shared
+// memory), so that handles of any grid size can launch them.
+static cudaError_t optin(const void *fn, int limit) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, limit - (int)fa.sharedSizeBytes);
+}
+
 cudaError_t kernels_init(const Dev &d) {
-  cudaError_t e = cudaFuncSetAttribute(k_xphys, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  int dev = 0, limit = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-  (void)d;
-  return e;
+  if ((size_t)limit < xphys_smem(d) + 1024 || (size_t)limit < zsmem(d) + 1024) return cudaErrorInvalidValue;
+  if ((e = optin((const void *)k_xphys, limit)) != cudaSuccess) return e;
+  if ((e = optin((const void *)k_zinv, limit)) != cudaSuccess) return e;
+  return optin((const void *)k_zfwd, limit);
 }
 
 }  // namespace lmc
