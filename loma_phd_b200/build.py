@@ -14,8 +14,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblomacte_b200.so")
-SOURCES = ["lmc_api.cu", "lmc_kernels.cu", "lmc_host.cpp"]
-HEADERS = ["lmc_internal.h", "lmc_kernels.cuh", "lmc_device.cuh"]
+SOURCES = ["lmc_api.cu", "lmc_dispatch.cu", "lmc_ykernels.cu", "lmc_fft_a.cu", "lmc_fft_b.cu",
+           "lmc_fft_c.cu", "lmc_host.cpp"]
+HEADERS = ["lmc_internal.h", "lmc_kernels.cuh", "lmc_device.cuh", "lmc_fft_impl.cuh"]
 
 
 def nvcc() -> str:
@@ -38,23 +39,40 @@ def _stale() -> bool:
     return any(os.path.getmtime(p) > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
-    cmd = [nvcc(), "-ccbin", host_cxx(), "-std=c++17", "-O3", "-lineinfo",
-           "-gencode", "arch=compute_100a,code=sm_100a",
-           "-Xcompiler", "-fPIC,-fopenmp", "-shared",
-           "-o", LIB + ".tmp"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
+         "-Xcompiler", "-fPIC,-fopenmp"]
+
+
+def _compile(src: str, obj: str, verbose: bool) -> str:
+    cmd = [nvcc(), "-ccbin", host_cxx()] + FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
-    cmd += ["-lgomp"]
+    r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}{r.stderr}")
+    return r.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel, then link the shared
+    library (sm_100a device code only)."""
+    if not force and not _stale():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+    odir = os.path.join(HERE, "_build")
+    os.makedirs(odir, exist_ok=True)
+    objs = [os.path.join(odir, os.path.splitext(f)[0] + ".o") for f in SOURCES]
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        logs = list(ex.map(lambda a: _compile(a[0], a[1], verbose), zip(SOURCES, objs)))
+    if verbose:
+        for f, l in zip(SOURCES, logs):
+            sys.stderr.write(f"==== {f}\n{l}")
+    cmd = [nvcc(), "-ccbin", host_cxx(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-Xcompiler", "-fopenmp", "-o", LIB + ".tmp"] + objs + ["-lgomp"]
     r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc build of liblomacte_b200 failed")
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc link of liblomacte_b200 failed")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -63,16 +63,6 @@ int dupload(lmc_handle *h, const T **p, const std::vector<T> &v) {
   return LMC_OK;
 }
 
-bool fft_ok(int n, lmcd::FFTPlan &P) {
-  P.n = n;
-  P.nst = 0;
-  int m = n;
-  while (m % 4 == 0 && P.nst < 16) { P.rad[P.nst++] = 4; m /= 4; }
-  while (m % 2 == 0 && P.nst < 16) { P.rad[P.nst++] = 2; m /= 2; }
-  while (m % 3 == 0 && P.nst < 16) { P.rad[P.nst++] = 3; m /= 3; }
-  return m == 1;
-}
-
 std::vector<double2> twiddles(int n) {
   std::vector<double2> t(n);
   for (int k = 0; k < n; k++) {
@@ -128,10 +118,13 @@ int do_load(lmc_handle *h, const double *vor, const double *phi, const double *p
   const lmc::Dev &d = h->d;
   const size_t ns = (size_t)d.nmode * d.my * sizeof(double2);
   LMC_CK(cudaSetDevice(h->p.device));
-  LMC_CK(cudaMemcpyAsync(d.vor, vor, ns, cudaMemcpyHostToDevice, h->s));
-  LMC_CK(cudaMemcpyAsync(d.phi, phi, ns, cudaMemcpyHostToDevice, h->s));
-  LMC_CK(cudaMemcpyAsync(d.psi, psi, ns, cudaMemcpyHostToDevice, h->s));
-  LMC_CK(cudaMemcpyAsync(d.scal, scal, ns, cudaMemcpyHostToDevice, h->s));
+  // reference layout [kx][kz][y] -> device layout [y][kx][kz]
+  const double *src[4] = {vor, phi, psi, scal};
+  double2 *dst[4] = {d.vor, d.phi, d.psi, d.scal};
+  for (int f = 0; f < 4; f++) {
+    LMC_CK(cudaMemcpyAsync(d.sb[f], src[f], ns, cudaMemcpyHostToDevice, h->s));
+    lmc::launch_ref2dev(d, d.sb[f], dst[f], h->s);
+  }
   LMC_CK(cudaMemsetAsync(d.Rom, 0, ns, h->s));
   LMC_CK(cudaMemsetAsync(d.Rphi, 0, ns, h->s));
   LMC_CK(cudaMemsetAsync(d.rhst, 0, (size_t)d.my * d.mgalz * d.mgalx * sizeof(double), h->s));
@@ -190,12 +183,12 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   std::memset(&d, 0, sizeof(d));
   const lmc::Grid &g = h->g;
   int rc = LMC_OK;
-  lmcd::FFTPlan fx{}, fz{};
-  if (g.nkx < 1 || g.mz < 1 || !fft_ok(g.mgalx, fx) || !fft_ok(g.mgalz, fz) || g.mgalx % 2) rc = LMC_EINVAL;
+  if (g.nkx < 1 || g.mz < 1 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) rc = LMC_EINVAL;
   if (!rc) rc = pick_chunks(g.my, d.C, d.lpm, d.base, d.extra);
   if (rc) { delete h; return rc; }
   try {
     lmc::build_yops(g.my, y, h->ops);
+    lmc::build_scans(h->ops, d.lpm, d.base, d.extra);
   } catch (...) {
     delete h;
     return LMC_EINVAL;
@@ -207,6 +200,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
 
   if (cudaSetDevice(p->device) != cudaSuccess) { delete h; return LMC_ECUDA; }
   d.my = g.my; d.mgalx = g.mgalx; d.mgalz = g.mgalz; d.nkx = g.nkx; d.mz = g.mz; d.nz1 = g.nz1; d.nmode = g.nmode;
+  d.ldy = g.my | 1;
   d.ire = 1.0 / p->Re;
   d.peclet = p->peclet > 0 ? p->peclet : p->Re * (double)0.7f;  // main.f:569
   d.cfl = (double)(float)p->cfl;
@@ -216,14 +210,33 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     d.gama[r] = h->rk.gama[r]; d.xi[r] = h->rk.xi[r]; d.alpha[r] = h->rk.alpha[r]; d.beta[r] = h->rk.beta[r];
   }
   const lmc::YOps &o = h->ops;
-  if ((rc = dupload(h, &d.dt12, o.dt12)) || (rc = dupload(h, &d.dt11, o.dt11)) || (rc = dupload(h, &d.dt22, o.dt22)) ||
-      (rc = dupload(h, &d.dt21, o.dt21)) || (rc = dupload(h, &d.p1L, o.p1L)) || (rc = dupload(h, &d.p1U, o.p1U)) ||
-      (rc = dupload(h, &d.p3L, o.p3L)) || (rc = dupload(h, &d.p3U, o.p3U)) || (rc = dupload(h, &d.i8L, o.i8L)) ||
-      (rc = dupload(h, &d.i8U, o.i8U)) || (rc = dupload(h, &d.fmap, o.fmap)) || (rc = dupload(h, &d.hy, o.hy)) ||
-      (rc = dupload(h, &d.trp, o.trp)) || (rc = dupload(h, &d.y, o.y)) || (rc = dupload(h, &d.ebot, o.ebot)) ||
-      (rc = dupload(h, &d.etop, o.etop)) || (rc = dupload(h, &d.PL, h->pt.L)) || (rc = dupload(h, &d.PU, h->pt.U)) ||
-      (rc = dupload(h, &d.V12, h->pt.V12)) || (rc = dupload(h, &d.AAinv, h->pt.AAinv)) ||
-      (rc = dupload(h, &d.k2, h->pt.k2)) || (rc = dupload(h, &d.kx, kx)) || (rc = dupload(h, &d.kz, kz))) {
+  // y-operator tables go to the device chunk-major (see lmcd::tab)
+  const int C = d.C, lpm = d.lpm, base = d.base, extra = d.extra, my = g.my;
+  auto cm = [&](const std::vector<double> &T, int W) { return lmc::chunk_major(T, my, W, C, lpm, base, extra); };
+  const size_t pm2 = (size_t)C * 2 * 32, pm3 = (size_t)C * 3 * 32;
+  std::vector<double> PLc((size_t)g.nmode * pm2), PUc((size_t)g.nmode * pm3), V12c((size_t)g.nmode * pm2);
+#pragma omp parallel for schedule(static)
+  for (int m = 0; m < g.nmode; m++) {
+    std::vector<double> a(h->pt.L.begin() + (size_t)m * my * 2, h->pt.L.begin() + (size_t)(m + 1) * my * 2);
+    std::vector<double> b(h->pt.U.begin() + (size_t)m * my * 3, h->pt.U.begin() + (size_t)(m + 1) * my * 3);
+    std::vector<double> v(h->pt.V12.begin() + (size_t)m * my * 2, h->pt.V12.begin() + (size_t)(m + 1) * my * 2);
+    const std::vector<double> ca = cm(a, 2), cb = cm(b, 3), cv = cm(v, 2);
+    std::copy(ca.begin(), ca.end(), PLc.begin() + (size_t)m * pm2);
+    std::copy(cb.begin(), cb.end(), PUc.begin() + (size_t)m * pm3);
+    std::copy(cv.begin(), cv.end(), V12c.begin() + (size_t)m * pm2);
+  }
+  if ((rc = dupload(h, &d.dt12, cm(o.dt12, 7))) || (rc = dupload(h, &d.dt11, cm(o.dt11, 7))) ||
+      (rc = dupload(h, &d.dt22, cm(o.dt22, 5))) || (rc = dupload(h, &d.dt21, cm(o.dt21, 5))) ||
+      (rc = dupload(h, &d.p1L, cm(o.p1L, 3))) || (rc = dupload(h, &d.p1U, cm(o.p1U, 4))) ||
+      (rc = dupload(h, &d.p3L, cm(o.p3L, 2))) || (rc = dupload(h, &d.p3U, cm(o.p3U, 3))) ||
+      (rc = dupload(h, &d.i8L, cm(o.i8L, 3))) || (rc = dupload(h, &d.i8U, cm(o.i8U, 4))) ||
+      (rc = dupload(h, &d.fmap, cm(o.fmap, 1))) || (rc = dupload(h, &d.hy, o.hy)) || (rc = dupload(h, &d.trp, o.trp)) ||
+      (rc = dupload(h, &d.y, o.y)) || (rc = dupload(h, &d.ebot, cm(o.ebot, 1))) || (rc = dupload(h, &d.etop, cm(o.etop, 1))) ||
+      (rc = dupload(h, &d.k1L, o.k1L)) || (rc = dupload(h, &d.k1U, o.k1U)) || (rc = dupload(h, &d.k3L, o.k3L)) ||
+      (rc = dupload(h, &d.k3U, o.k3U)) || (rc = dupload(h, &d.k8L, o.k8L)) || (rc = dupload(h, &d.k8U, o.k8U)) ||
+      (rc = dupload(h, &d.PL, PLc)) || (rc = dupload(h, &d.PU, PUc)) || (rc = dupload(h, &d.V12, V12c)) ||
+      (rc = dupload(h, &d.AAinv, h->pt.AAinv)) || (rc = dupload(h, &d.k2, h->pt.k2)) || (rc = dupload(h, &d.kx, kx)) ||
+      (rc = dupload(h, &d.kz, kz))) {
     lmc_destroy(h);
     return rc;
   }
@@ -235,10 +248,8 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
       lmc_destroy(h);
       return rc;
     }
-    fx.tw = tx;
-    fz.tw = tz;
-    d.fx = fx;
-    d.fz = fz;
+    d.twx = tx;
+    d.twz = tz;
   }
   const size_t ns = (size_t)g.nmode * g.my, nzp = (size_t)g.nkx * g.my * g.mgalz;
   double2 **spec[] = {&d.vor, &d.phi, &d.psi, &d.scal, &d.Rom, &d.Rphi};
@@ -305,10 +316,14 @@ int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi, doub
   const lmc::Dev &d = h->d;
   const size_t ns = (size_t)d.nmode * d.my * sizeof(double2), ny = (size_t)d.my * sizeof(double);
   LMC_CK(cudaSetDevice(h->p.device));
-  if (vor) LMC_CK(cudaMemcpyAsync(vor, d.vor, ns, cudaMemcpyDeviceToHost, h->s));
-  if (phi) LMC_CK(cudaMemcpyAsync(phi, d.phi, ns, cudaMemcpyDeviceToHost, h->s));
-  if (psi) LMC_CK(cudaMemcpyAsync(psi, d.psi, ns, cudaMemcpyDeviceToHost, h->s));
-  if (scal) LMC_CK(cudaMemcpyAsync(scal, d.scal, ns, cudaMemcpyDeviceToHost, h->s));
+  // device layout -> reference layout through the spectral work buffers
+  double *dsth[4] = {vor, phi, psi, scal};
+  const double2 *srcd[4] = {d.vor, d.phi, d.psi, d.scal};
+  for (int f = 0; f < 4; f++)
+    if (dsth[f]) {
+      lmc::launch_dev2ref(d, srcd[f], d.sb[f], h->s);
+      LMC_CK(cudaMemcpyAsync(dsth[f], d.sb[f], ns, cudaMemcpyDeviceToHost, h->s));
+    }
   if (u00) LMC_CK(cudaMemcpyAsync(u00, d.u00, ny, cudaMemcpyDeviceToHost, h->s));
   if (v00) LMC_CK(cudaMemcpyAsync(v00, d.v00, ny, cudaMemcpyDeviceToHost, h->s));
   if (w00) LMC_CK(cudaMemcpyAsync(w00, d.w00, ny, cudaMemcpyDeviceToHost, h->s));
@@ -448,7 +463,12 @@ int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count) {
 int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev, double *out2_dev) {
   if (!h || op < 1 || op > 4 || !in_dev || !out_dev || (op == 3 && !out2_dev)) return LMC_EINVAL;
   LMC_CK(cudaSetDevice(h->p.device));
-  lmc::launch_op_y(h->d, op, (const double2 *)in_dev, (double2 *)out_dev, (double2 *)out2_dev, h->s);
+  // the operands use the reference layout; the operator runs on the device layout
+  const lmc::Dev &d = h->d;
+  lmc::launch_ref2dev(d, (const double2 *)in_dev, d.sb[7], h->s);
+  lmc::launch_op_y(d, op, d.sb[7], d.sb[8], d.sb[9], h->s);
+  lmc::launch_dev2ref(d, d.sb[8], (double2 *)out_dev, h->s);
+  if (op == 3) lmc::launch_dev2ref(d, d.sb[9], (double2 *)out2_dev, h->s);
   if (check_launch(h)) return LMC_ECUDA;
   LMC_CK(cudaStreamSynchronize(h->s));
   return LMC_OK;

@@ -2,13 +2,21 @@
 //
 // y-direction operators: one warp per (kx,kz) mode.  The pencil of my
 // points is split into chunks of n in {C-1, C} consecutive points, one chunk
-// per active lane (LPM active lanes, my = sum of chunk sizes).  Banded
-// matrix-vector products exchange a halo of H points with the neighbour
-// lanes by shuffles.  Banded triangular solves run each chunk's recurrence
-// in registers and join the chunks with a Kogge-Stone scan of the affine
-// chunk maps state_out = M state_in + p (M from the homogeneous responses),
-// so no pencil ever leaves registers between the forward and backward
-// sweeps.
+// per active lane (LPM active lanes).  Banded matrix-vector products
+// exchange a halo of H points with the neighbour lanes by shuffles.  Banded
+// triangular solves run each chunk's recurrence in registers and join the
+// chunks with a Kogge-Stone scan of the affine chunk maps
+// state_out = M state_in + p.  For the mode-independent operators (the
+// compact-derivative LUs) the scan matrices are precomputed on the host, so
+// only the particular responses p travel between lanes; for the per-mode
+// Poisson LUs the 2x2 maps are built in registers.
+//
+// x/z transforms: four-step FFTs N = N1*N2 with both factors done by one
+// thread in registers, lines staged in shared memory with a skewed index
+// (one pad slot per N1 entries) so that both the strided and the
+// contiguous passes are free of bank conflicts.  The inverse ("nat2perm")
+// leaves the samples in a permuted order and the direct transform
+// ("perm2nat") is its transpose, so no permutation pass is needed.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -22,7 +30,7 @@ __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_dou
 // (i k) * a
 __device__ __forceinline__ double2 cik(double k, double2 a) { return make_double2(-k * a.y, k * a.x); }
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
@@ -34,7 +42,9 @@ __device__ __forceinline__ double2 shfl_down2(double2 v, int d) {
   return make_double2(__shfl_down_sync(LMC_FULL, v.x, d), __shfl_down_sync(LMC_FULL, v.y, d));
 }
 
-// Chunk geometry of one lane.
+// ---------------------------------------------------------------------
+// Chunk geometry of one lane
+// ---------------------------------------------------------------------
 struct Lane {
   int lane, s, n, lpm;
   bool full;  // n == C
@@ -56,34 +66,37 @@ __device__ __forceinline__ Lane make_lane(int lpm, int base, int extra) {
   return L;
 }
 
+// Row tables are stored chunk-major: entry (row s+t, coefficient c) of
+// lane l is T[(t*W + c)*32 + l], so a warp reads 32 consecutive doubles.
+__device__ __forceinline__ double tab(const double *__restrict__ T, int W, int t, int c, int lane) {
+  return __ldg(T + ((size_t)t * W + c) * 32 + lane);
+}
+
+// chunk <-> pencil held in shared memory (or any pointer)
 template <int C>
-__device__ __forceinline__ void ld(const double2 *__restrict__ p, const Lane &L, double2 (&v)[C]) {
+__device__ __forceinline__ void cld(const double2 *p, const Lane &L, double2 (&v)[C]) {
 #pragma unroll
-  for (int t = 0; t < C; t++) v[t] = (t < L.n) ? __ldg(p + L.s + t) : czero();
+  for (int t = 0; t < C; t++) v[t] = (t < L.n) ? p[L.s + t] : czero();
 }
 template <int C>
-__device__ __forceinline__ void st(double2 *__restrict__ p, const Lane &L, const double2 (&v)[C]) {
+__device__ __forceinline__ void cst(double2 *p, const Lane &L, const double2 (&v)[C]) {
 #pragma unroll
   for (int t = 0; t < C; t++)
     if (t < L.n) p[L.s + t] = v[t];
 }
 
 // out = band(A) * v, A rows of 2H+1 coefficients (column offsets -H..H).
-// Rows outside 0..my-1 do not exist; the coefficient tables hold zeros for
-// out-of-range columns, and the halos of the first/last lanes are zero.
+// The coefficient tables hold zeros for out-of-range columns and the halos
+// of the first/last lanes are zero.
 template <int C, int H>
 __device__ __forceinline__ void matvec(const double *__restrict__ A, const Lane &L, const double2 (&v)[C],
                                        double2 (&out)[C]) {
-  double2 tl[H], hd[H], lh[H], rh[H];
+  double2 lh[H], rh[H];
 #pragma unroll
   for (int q = 0; q < H; q++) {
-    tl[q] = L.full ? v[C - H + q] : v[C - 1 - H + q];
-    hd[q] = v[q];
-  }
-#pragma unroll
-  for (int q = 0; q < H; q++) {
-    lh[q] = shfl_up2(tl[q], 1);
-    rh[q] = shfl_down2(hd[q], 1);
+    const double2 tl = L.full ? v[C - H + q] : v[C - 1 - H + q];
+    lh[q] = shfl_up2(tl, 1);
+    rh[q] = shfl_down2(v[q], 1);
     if (L.lane == 0) lh[q] = czero();
     if (L.lane >= L.lpm - 1) rh[q] = czero();
   }
@@ -91,7 +104,6 @@ __device__ __forceinline__ void matvec(const double *__restrict__ A, const Lane 
   for (int t = 0; t < C; t++) {
     double2 acc = czero();
     if (t < L.n) {
-      const double *a = A + (size_t)(L.s + t) * (2 * H + 1);
 #pragma unroll
       for (int c = 0; c < 2 * H + 1; c++) {
         const int e = t - H + c;
@@ -100,10 +112,10 @@ __device__ __forceinline__ void matvec(const double *__restrict__ A, const Lane 
         else if (e < C - 1) u = v[e];
         else if (e == C - 1) u = L.full ? v[C - 1] : rh[0];
         else {
-          const int i0 = e - C, i1 = (e - C + 1 < H) ? e - C + 1 : H - 1;
-          u = L.full ? rh[i0 < H ? i0 : H - 1] : rh[i1];
+          const int i0 = (e - C < H) ? e - C : H - 1, i1 = (e - C + 1 < H) ? e - C + 1 : H - 1;
+          u = L.full ? rh[i0] : rh[i1];
         }
-        const double w = __ldg(a + c);
+        const double w = tab(A, 2 * H + 1, t, c, L.lane);
         acc.x = fma(w, u.x, acc.x);
         acc.y = fma(w, u.y, acc.y);
       }
@@ -112,226 +124,249 @@ __device__ __forceinline__ void matvec(const double *__restrict__ A, const Lane 
   }
 }
 
-// Lower unit-triangular band solve in place: x_j -= sum_{d=1..B} Lt[j][d-1] x_{j-d}.
+// In-place variant: a rolling window keeps the H original values that the
+// rows after them still need.
+template <int C, int H>
+__device__ __forceinline__ void matvec_ip(const double *__restrict__ A, const Lane &L, double2 (&v)[C]) {
+  double2 lh[H], rh[H];
+#pragma unroll
+  for (int q = 0; q < H; q++) {
+    const double2 tl = L.full ? v[C - H + q] : v[C - 1 - H + q];
+    lh[q] = shfl_up2(tl, 1);
+    rh[q] = shfl_down2(v[q], 1);
+    if (L.lane == 0) lh[q] = czero();
+    if (L.lane >= L.lpm - 1) rh[q] = czero();
+  }
+  double2 win[H];  // win[q] = original v[t-H+q] (left halo at first)
+#pragma unroll
+  for (int q = 0; q < H; q++) win[q] = lh[q];
+#pragma unroll
+  for (int t = 0; t < C; t++) {
+    const double2 orig = v[t];
+    double2 acc = czero();
+    if (t < L.n) {
+#pragma unroll
+      for (int c = 0; c < 2 * H + 1; c++) {
+        const int e = t - H + c;
+        double2 u;
+        if (c < H) u = win[c];
+        else if (c == H) u = orig;
+        else if (e < C - 1) u = v[e];
+        else if (e == C - 1) u = L.full ? v[C - 1] : rh[0];
+        else {
+          const int i0 = (e - C < H) ? e - C : H - 1, i1 = (e - C + 1 < H) ? e - C + 1 : H - 1;
+          u = L.full ? rh[i0] : rh[i1];
+        }
+        const double w = tab(A, 2 * H + 1, t, c, L.lane);
+        acc.x = fma(w, u.x, acc.x);
+        acc.y = fma(w, u.y, acc.y);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < H - 1; q++) win[q] = win[q + 1];
+    win[H - 1] = orig;
+    v[t] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Band triangular solves (tables chunk-major, see tab()).
+//   lower: x_j -= sum_{d=1..B} Lt[j][d-1] x_{j-d}
+//   upper: x_i = (x_i - sum_{d=1..B} Ut[i][d] x_{i+d}) * Ut[i][0]
+// Scan tables (constant operators): Ks[(s*32 + lane)*B*B] = the lane's
+// composed chunk map at Kogge-Stone step s (row-major B x B).
+// ---------------------------------------------------------------------
 template <int C, int B>
-__device__ __forceinline__ void lsolve(double2 (&x)[C], const double *__restrict__ Lt, const Lane &L) {
-  // 1) particular response with zero incoming state
+__device__ __forceinline__ void lrun(double2 (&x)[C], const double *__restrict__ Lt, const Lane &L, double2 (&S)[B],
+                                     bool write) {
+#pragma unroll
+  for (int t = 0; t < C; t++)
+    if (t < L.n) {
+      double2 v = x[t];
+#pragma unroll
+      for (int d = 0; d < B; d++) {
+        const double c = tab(Lt, B, t, d, L.lane);
+        v.x = fma(-c, S[d].x, v.x);
+        v.y = fma(-c, S[d].y, v.y);
+      }
+#pragma unroll
+      for (int d = B - 1; d > 0; d--) S[d] = S[d - 1];
+      S[0] = v;
+      if (write) x[t] = v;
+    }
+}
+template <int C, int B>
+__device__ __forceinline__ void urun(double2 (&x)[C], const double *__restrict__ Ut, const Lane &L, double2 (&S)[B],
+                                     bool write) {
+#pragma unroll
+  for (int t = C - 1; t >= 0; t--)
+    if (t < L.n) {
+      double2 v = x[t];
+#pragma unroll
+      for (int d = 0; d < B; d++) {
+        const double c = tab(Ut, B + 1, t, 1 + d, L.lane);
+        v.x = fma(-c, S[d].x, v.x);
+        v.y = fma(-c, S[d].y, v.y);
+      }
+      const double r = tab(Ut, B + 1, t, 0, L.lane);
+      v.x *= r;
+      v.y *= r;
+#pragma unroll
+      for (int d = B - 1; d > 0; d--) S[d] = S[d - 1];
+      S[0] = v;
+      if (write) x[t] = v;
+    }
+}
+
+// scan of the particular responses with precomputed composed maps
+template <int B, bool UP>
+__device__ __forceinline__ void scan_const(double2 (&S)[B], const double *__restrict__ Ks, int lane) {
+#pragma unroll
+  for (int s = 0; s < 5; s++) {
+    const int off = 1 << s;
+    double2 pp[B];
+#pragma unroll
+    for (int d = 0; d < B; d++) pp[d] = UP ? shfl_up2(S[d], off) : shfl_down2(S[d], off);
+    const bool act = UP ? (lane >= off) : (lane + off < 32);
+    if (act) {
+      const double *A = Ks + (size_t)(s * 32 + lane) * B * B;
+#pragma unroll
+      for (int r = 0; r < B; r++) {
+#pragma unroll
+        for (int q = 0; q < B; q++) {
+          const double a = __ldg(A + r * B + q);
+          S[r].x = fma(a, pp[q].x, S[r].x);
+          S[r].y = fma(a, pp[q].y, S[r].y);
+        }
+      }
+    }
+  }
+}
+
+template <int C, int B>
+__device__ __forceinline__ void lsolve_c(double2 (&x)[C], const double *__restrict__ Lt, const double *__restrict__ Ks,
+                                         const Lane &L) {
   double2 S[B];
 #pragma unroll
   for (int d = 0; d < B; d++) S[d] = czero();
-#pragma unroll
-  for (int t = 0; t < C; t++)
-    if (t < L.n) {
-      const double *l = Lt + (size_t)(L.s + t) * B;
-      double2 v = x[t];
-#pragma unroll
-      for (int d = 0; d < B; d++) {
-        const double c = __ldg(l + d);
-        v.x = fma(-c, S[d].x, v.x);
-        v.y = fma(-c, S[d].y, v.y);
-      }
-#pragma unroll
-      for (int d = B - 1; d > 0; d--) S[d] = S[d - 1];
-      S[0] = v;
-    }
-  // 2) homogeneous responses: M[r][q] = state r after the chunk from e_q
-  double M[B][B];
-#pragma unroll
-  for (int q = 0; q < B; q++) {
-    double T[B];
-#pragma unroll
-    for (int d = 0; d < B; d++) T[d] = (d == q) ? 1.0 : 0.0;
-#pragma unroll
-    for (int t = 0; t < C; t++)
-      if (t < L.n) {
-        const double *l = Lt + (size_t)(L.s + t) * B;
-        double v = 0.0;
-#pragma unroll
-        for (int d = 0; d < B; d++) v = fma(-__ldg(l + d), T[d], v);
-#pragma unroll
-        for (int d = B - 1; d > 0; d--) T[d] = T[d - 1];
-        T[0] = v;
-      }
-#pragma unroll
-    for (int r = 0; r < B; r++) M[r][q] = T[r];
-  }
-  // 3) inclusive scan over lanes (lane order = row order)
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    double2 pp[B];
-    double MM[B][B];
-#pragma unroll
-    for (int d = 0; d < B; d++) pp[d] = shfl_up2(S[d], off);
-#pragma unroll
-    for (int r = 0; r < B; r++)
-#pragma unroll
-      for (int q = 0; q < B; q++) MM[r][q] = __shfl_up_sync(LMC_FULL, M[r][q], off);
-    if (L.lane >= off) {
-      double2 np[B];
-      double nM[B][B];
-#pragma unroll
-      for (int r = 0; r < B; r++) {
-        double2 a = S[r];
-#pragma unroll
-        for (int q = 0; q < B; q++) {
-          a.x = fma(M[r][q], pp[q].x, a.x);
-          a.y = fma(M[r][q], pp[q].y, a.y);
-        }
-        np[r] = a;
-#pragma unroll
-        for (int q = 0; q < B; q++) {
-          double s = 0.0;
-#pragma unroll
-          for (int k = 0; k < B; k++) s = fma(M[r][k], MM[k][q], s);
-          nM[r][q] = s;
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < B; r++) {
-        S[r] = np[r];
-#pragma unroll
-        for (int q = 0; q < B; q++) M[r][q] = nM[r][q];
-      }
-    }
-  }
-  // 4) incoming state = inclusive result of the previous lane
-  double2 Sin[B];
+  lrun<C, B>(x, Lt, L, S, false);
+  scan_const<B, true>(S, Ks, L.lane);
 #pragma unroll
   for (int d = 0; d < B; d++) {
-    Sin[d] = shfl_up2(S[d], 1);
-    if (L.lane == 0) Sin[d] = czero();
+    S[d] = shfl_up2(S[d], 1);
+    if (L.lane == 0) S[d] = czero();
   }
-  // 5) final pass
-#pragma unroll
-  for (int t = 0; t < C; t++)
-    if (t < L.n) {
-      const double *l = Lt + (size_t)(L.s + t) * B;
-      double2 v = x[t];
-#pragma unroll
-      for (int d = 0; d < B; d++) {
-        const double c = __ldg(l + d);
-        v.x = fma(-c, Sin[d].x, v.x);
-        v.y = fma(-c, Sin[d].y, v.y);
-      }
-#pragma unroll
-      for (int d = B - 1; d > 0; d--) Sin[d] = Sin[d - 1];
-      Sin[0] = v;
-      x[t] = v;
-    }
+  lrun<C, B>(x, Lt, L, S, true);
 }
-
-// Upper band solve in place: x_i = (x_i - sum_{d=1..B} U[i][d] x_{i+d}) * U[i][0].
 template <int C, int B>
-__device__ __forceinline__ void usolve(double2 (&x)[C], const double *__restrict__ Ut, const Lane &L) {
-  double2 S[B];  // S[d] = x_{i+1+d}
+__device__ __forceinline__ void usolve_c(double2 (&x)[C], const double *__restrict__ Ut, const double *__restrict__ Ks,
+                                         const Lane &L) {
+  double2 S[B];
 #pragma unroll
   for (int d = 0; d < B; d++) S[d] = czero();
+  urun<C, B>(x, Ut, L, S, false);
+  scan_const<B, false>(S, Ks, L.lane);
 #pragma unroll
-  for (int t = C - 1; t >= 0; t--)
-    if (t < L.n) {
-      const double *u = Ut + (size_t)(L.s + t) * (B + 1);
-      double2 v = x[t];
-#pragma unroll
-      for (int d = 0; d < B; d++) {
-        const double c = __ldg(u + 1 + d);
-        v.x = fma(-c, S[d].x, v.x);
-        v.y = fma(-c, S[d].y, v.y);
-      }
-      const double r = __ldg(u);
-      v.x *= r;
-      v.y *= r;
-#pragma unroll
-      for (int d = B - 1; d > 0; d--) S[d] = S[d - 1];
-      S[0] = v;
-    }
-  double M[B][B];
-#pragma unroll
-  for (int q = 0; q < B; q++) {
-    double T[B];
-#pragma unroll
-    for (int d = 0; d < B; d++) T[d] = (d == q) ? 1.0 : 0.0;
-#pragma unroll
-    for (int t = C - 1; t >= 0; t--)
-      if (t < L.n) {
-        const double *u = Ut + (size_t)(L.s + t) * (B + 1);
-        double v = 0.0;
-#pragma unroll
-        for (int d = 0; d < B; d++) v = fma(-__ldg(u + 1 + d), T[d], v);
-        v *= __ldg(u);
-#pragma unroll
-        for (int d = B - 1; d > 0; d--) T[d] = T[d - 1];
-        T[0] = v;
-      }
-#pragma unroll
-    for (int r = 0; r < B; r++) M[r][q] = T[r];
+  for (int d = 0; d < B; d++) {
+    S[d] = shfl_down2(S[d], 1);
+    if (L.lane == 31) S[d] = czero();
   }
-  // scan from the last lane downwards
+  urun<C, B>(x, Ut, L, S, true);
+}
+
+// General solves (per-mode factors): the chunk maps are built in registers.
+template <int C, int B, bool UP>
+__device__ __forceinline__ void scan_gen(double2 (&S)[B], double (&M)[B][B], int lane) {
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
+  for (int s = 0; s < 5; s++) {
+    const int off = 1 << s;
     double2 pp[B];
     double MM[B][B];
 #pragma unroll
-    for (int d = 0; d < B; d++) pp[d] = shfl_down2(S[d], off);
+    for (int d = 0; d < B; d++) pp[d] = UP ? shfl_up2(S[d], off) : shfl_down2(S[d], off);
 #pragma unroll
     for (int r = 0; r < B; r++)
 #pragma unroll
-      for (int q = 0; q < B; q++) MM[r][q] = __shfl_down_sync(LMC_FULL, M[r][q], off);
-    if (L.lane + off < 32) {
-      double2 np[B];
+      for (int q = 0; q < B; q++)
+        MM[r][q] = UP ? __shfl_up_sync(LMC_FULL, M[r][q], off) : __shfl_down_sync(LMC_FULL, M[r][q], off);
+    const bool act = UP ? (lane >= off) : (lane + off < 32);
+    if (act) {
       double nM[B][B];
 #pragma unroll
       for (int r = 0; r < B; r++) {
-        double2 a = S[r];
 #pragma unroll
         for (int q = 0; q < B; q++) {
-          a.x = fma(M[r][q], pp[q].x, a.x);
-          a.y = fma(M[r][q], pp[q].y, a.y);
-        }
-        np[r] = a;
+          S[r].x = fma(M[r][q], pp[q].x, S[r].x);
+          S[r].y = fma(M[r][q], pp[q].y, S[r].y);
+          double a = 0.0;
 #pragma unroll
-        for (int q = 0; q < B; q++) {
-          double s = 0.0;
-#pragma unroll
-          for (int k = 0; k < B; k++) s = fma(M[r][k], MM[k][q], s);
-          nM[r][q] = s;
+          for (int k = 0; k < B; k++) a = fma(M[r][k], MM[k][q], a);
+          nM[r][q] = a;
         }
       }
 #pragma unroll
-      for (int r = 0; r < B; r++) {
-        S[r] = np[r];
+      for (int r = 0; r < B; r++)
 #pragma unroll
         for (int q = 0; q < B; q++) M[r][q] = nM[r][q];
-      }
     }
   }
-  double2 Sin[B];
-#pragma unroll
-  for (int d = 0; d < B; d++) {
-    Sin[d] = shfl_down2(S[d], 1);
-    if (L.lane == 31) Sin[d] = czero();
-  }
-#pragma unroll
-  for (int t = C - 1; t >= 0; t--)
-    if (t < L.n) {
-      const double *u = Ut + (size_t)(L.s + t) * (B + 1);
-      double2 v = x[t];
-#pragma unroll
-      for (int d = 0; d < B; d++) {
-        const double c = __ldg(u + 1 + d);
-        v.x = fma(-c, Sin[d].x, v.x);
-        v.y = fma(-c, Sin[d].y, v.y);
-      }
-      const double r = __ldg(u);
-      v.x *= r;
-      v.y *= r;
-#pragma unroll
-      for (int d = B - 1; d > 0; d--) Sin[d] = Sin[d - 1];
-      Sin[0] = v;
-      x[t] = v;
-    }
 }
 
-// Warp sum of a complex value over all lanes.
+template <int C, int B>
+__device__ __forceinline__ void lsolve_g(double2 (&x)[C], const double *__restrict__ Lt, const Lane &L) {
+  double2 S[B];
+#pragma unroll
+  for (int d = 0; d < B; d++) S[d] = czero();
+  lrun<C, B>(x, Lt, L, S, false);
+  double M[B][B];
+#pragma unroll
+  for (int q = 0; q < B; q++) {
+    double2 T[B];
+    double2 z[C];
+#pragma unroll
+    for (int t = 0; t < C; t++) z[t] = czero();
+#pragma unroll
+    for (int d = 0; d < B; d++) T[d] = make_double2(d == q ? 1.0 : 0.0, 0.0);
+    lrun<C, B>(z, Lt, L, T, false);
+#pragma unroll
+    for (int r = 0; r < B; r++) M[r][q] = T[r].x;
+  }
+  scan_gen<C, B, true>(S, M, L.lane);
+#pragma unroll
+  for (int d = 0; d < B; d++) {
+    S[d] = shfl_up2(S[d], 1);
+    if (L.lane == 0) S[d] = czero();
+  }
+  lrun<C, B>(x, Lt, L, S, true);
+}
+template <int C, int B>
+__device__ __forceinline__ void usolve_g(double2 (&x)[C], const double *__restrict__ Ut, const Lane &L) {
+  double2 S[B];
+#pragma unroll
+  for (int d = 0; d < B; d++) S[d] = czero();
+  urun<C, B>(x, Ut, L, S, false);
+  double M[B][B];
+#pragma unroll
+  for (int q = 0; q < B; q++) {
+    double2 T[B];
+    double2 z[C];
+#pragma unroll
+    for (int t = 0; t < C; t++) z[t] = czero();
+#pragma unroll
+    for (int d = 0; d < B; d++) T[d] = make_double2(d == q ? 1.0 : 0.0, 0.0);
+    urun<C, B>(z, Ut, L, T, false);
+#pragma unroll
+    for (int r = 0; r < B; r++) M[r][q] = T[r].x;
+  }
+  scan_gen<C, B, false>(S, M, L.lane);
+#pragma unroll
+  for (int d = 0; d < B; d++) {
+    S[d] = shfl_down2(S[d], 1);
+    if (L.lane == 31) S[d] = czero();
+  }
+  urun<C, B>(x, Ut, L, S, true);
+}
+
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -351,114 +386,164 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+#ifdef LMC_FFT_TU
 // ---------------------------------------------------------------------
-// Batched in-place mixed-radix FFT on shared memory.
-// DIF (natural order in, digit-reversed out) and its transpose DIT
-// (digit-reversed in, natural out).  The inverse transforms of the
-// substep run DIF and the direct transforms DIT, so the physical-space
-// samples sit in digit-reversed order and no permutation pass is needed.
+// Register DFTs of compile-time size R (natural order in and out):
+// y_k = sum_n x_n exp(SIGN 2 pi i nk/R), recursive mixed radix 4/2/3.
+// Twiddles exp(-2 pi i e/R) come from a constant table (c_tw), one block
+// per size, filled by the host at initialisation.
 // ---------------------------------------------------------------------
-struct FFTPlan {
-  int n, nst;
-  int rad[16];
-  const double2 *tw;  // tw[t] = exp(-2 pi i t/n)
-};
+constexpr int TW_SIZES[] = {4, 6, 8, 9, 12, 16, 18, 24, 32, 36};
+__host__ __device__ constexpr int tw_off(int R) {
+  return R == 4 ? 0 : R == 6 ? 4 : R == 8 ? 10 : R == 9 ? 18 : R == 12 ? 27 : R == 16 ? 39 : R == 18 ? 55
+       : R == 24 ? 73 : R == 32 ? 97 : R == 36 ? 129 : -1;
+}
+constexpr int TW_TOTAL = 4 + 6 + 8 + 9 + 12 + 16 + 18 + 24 + 32 + 36;
 
-__device__ __forceinline__ double2 twid(const FFTPlan &P, int e, int sign) {
-  double2 w = __ldg(P.tw + e);
-  return sign > 0 ? cconj(w) : w;
+static __constant__ double2 c_tw[TW_TOTAL];  // one copy per translation unit
+
+template <int R, int SIGN>
+__device__ __forceinline__ double2 ctw(int e) {
+  constexpr int o = tw_off(R);
+  static_assert(o >= 0, "register DFT size without twiddles");
+  const double2 w = c_tw[o + e];
+  return SIGN > 0 ? cconj(w) : w;
 }
 
 template <int R, int SIGN>
 __device__ __forceinline__ void bfly(double2 (&x)[R]) {
-  // y_q = sum_p x_p exp(SIGN 2 pi i pq/R), in place
-  if (R == 2) {
-    double2 a = x[0], b = x[1];
+  if constexpr (R == 2) {
+    const double2 a = x[0], b = x[1];
     x[0] = cadd(a, b);
     x[1] = csub(a, b);
-  } else if (R == 4) {
-    double2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
-    double2 d = csub(x[1], x[3]);
-    double2 t3 = (SIGN > 0) ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);  // d * (SIGN i)
+  } else if constexpr (R == 4) {
+    const double2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
+    const double2 d = csub(x[1], x[3]);
+    const double2 t3 = (SIGN > 0) ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);  // d * (SIGN i)
     x[0] = cadd(t0, t2);
     x[2] = csub(t0, t2);
     x[1] = cadd(t1, t3);
     x[3] = csub(t1, t3);
-  } else {  // R == 3
+  } else if constexpr (R == 3) {
     const double s3 = 0.86602540378443864676;  // sqrt(3)/2
-    double2 t = cadd(x[1], x[2]);
-    double2 d = csub(x[1], x[2]);
-    double2 u = (SIGN > 0) ? make_double2(-s3 * d.y, s3 * d.x) : make_double2(s3 * d.y, -s3 * d.x);
-    double2 a = make_double2(x[0].x - 0.5 * t.x, x[0].y - 0.5 * t.y);
+    const double2 t = cadd(x[1], x[2]);
+    const double2 d = csub(x[1], x[2]);
+    const double2 u = (SIGN > 0) ? make_double2(-s3 * d.y, s3 * d.x) : make_double2(s3 * d.y, -s3 * d.x);
+    const double2 a = make_double2(fma(-0.5, t.x, x[0].x), fma(-0.5, t.y, x[0].y));
     x[0] = cadd(x[0], t);
     x[1] = cadd(a, u);
     x[2] = csub(a, u);
   }
 }
 
-// One radix-R stage over nb transforms of length n (batch b at buf+b*ld);
-// Ns is the sub-transform length of this stage.
-template <int R, int SIGN, bool DIF>
-__device__ __forceinline__ void fft_stage(double2 *buf, int nb, int ld, const FFTPlan &P, int Ns) {
-  const int n = P.n, M = Ns / R, nbut = n / R, tot = nb * nbut, stride = n / Ns;
-  for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-    const int b = idx / nbut, rem = idx - b * nbut, blk = rem / M, m = rem - blk * M;
-    double2 *base = buf + (size_t)b * ld + blk * Ns + m;
-    double2 x[R];
-    if (DIF) {
+template <int R, int SIGN>
+__device__ __forceinline__ void rdft(double2 (&x)[R]) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2 || R == 3 || R == 4) {
+    bfly<R, SIGN>(x);
+  } else {
+    constexpr int p = (R % 4 == 0) ? 4 : ((R % 2 == 0) ? 2 : 3);
+    constexpr int m = R / p;
+    double2 sub[p][m];
 #pragma unroll
-      for (int p = 0; p < R; p++) x[p] = base[p * M];
-      bfly<R, SIGN>(x);
+    for (int r = 0; r < p; r++)
 #pragma unroll
-      for (int q = 0; q < R; q++) {
-        double2 v = x[q];
-        if (q > 0 && m > 0) v = cmul(v, twid(P, (q * m * stride) % n, SIGN));
-        base[q * M] = v;
-      }
-    } else {
+      for (int j = 0; j < m; j++) sub[r][j] = x[r + p * j];
 #pragma unroll
-      for (int q = 0; q < R; q++) {
-        double2 v = base[q * M];
-        if (q > 0 && m > 0) v = cmul(v, twid(P, (q * m * stride) % n, SIGN));
-        x[q] = v;
-      }
-      bfly<R, SIGN>(x);
+    for (int r = 0; r < p; r++) rdft<m, SIGN>(sub[r]);
 #pragma unroll
-      for (int p = 0; p < R; p++) base[p * M] = x[p];
+    for (int k = 0; k < m; k++) {
+      double2 t[p];
+#pragma unroll
+      for (int r = 0; r < p; r++) t[r] = (r == 0 || k == 0) ? sub[r][k] : cmul(sub[r][k], ctw<R, SIGN>(r * k));
+      bfly<p, SIGN>(t);
+#pragma unroll
+      for (int q = 0; q < p; q++) x[k + m * q] = t[q];
     }
   }
 }
 
-// nb transforms of length P.n, batch b at buf + b*ld.  All threads of the
-// block call these; each stage ends with a __syncthreads().
-template <int SIGN>
-__device__ void fft_dif(double2 *buf, int nb, int ld, const FFTPlan &P) {
-  int Ns = P.n;
-  for (int st = 0; st < P.nst; st++) {
-    const int r = P.rad[st];
-    if (r == 4) fft_stage<4, SIGN, true>(buf, nb, ld, P, Ns);
-    else if (r == 2) fft_stage<2, SIGN, true>(buf, nb, ld, P, Ns);
-    else fft_stage<3, SIGN, true>(buf, nb, ld, P, Ns);
-    __syncthreads();
-    Ns /= r;
-  }
-}
+// Four-step transform of nb lines of length N = N1*N2 in shared memory.
+// Line b starts at sm + b*ld; natural index n is stored at skew(n) =
+// n + n/N1.  twN[e] = exp(-2 pi i e/N).
+template <int N1, int N2>
+struct Four {
+  static constexpr int N = N1 * N2;
+  static constexpr int LD = N2 * (N1 + 1);  // skewed line length
+  __device__ static __forceinline__ int sk(int n) { return n + n / N1; }
 
-template <int SIGN>
-__device__ void fft_dit(double2 *buf, int nb, int ld, const FFTPlan &P) {
-  int sizes[16];
-  int Ns = P.n;
-  for (int st = 0; st < P.nst; st++) {
-    sizes[st] = Ns;
-    Ns /= P.rad[st];
-  }
-  for (int st = P.nst - 1; st >= 0; st--) {
-    const int r = P.rad[st];
-    if (r == 4) fft_stage<4, SIGN, false>(buf, nb, ld, P, sizes[st]);
-    else if (r == 2) fft_stage<2, SIGN, false>(buf, nb, ld, P, sizes[st]);
-    else fft_stage<3, SIGN, false>(buf, nb, ld, P, sizes[st]);
+  // natural -> permuted: X[k2 + N2 k1] lands at skew position k1 + N1 k2
+  template <int SIGN>
+  __device__ static void nat2perm(double2 *sm, int nb, int ld, const double2 *__restrict__ twN) {
+    for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
+      const int b = idx / N1, n1 = idx - b * N1;
+      double2 *p = sm + (size_t)b * ld + n1;
+      double2 x[N2];
+#pragma unroll
+      for (int j = 0; j < N2; j++) x[j] = p[j * (N1 + 1)];
+      rdft<N2, SIGN>(x);
+#pragma unroll
+      for (int k = 0; k < N2; k++) {
+        double2 v = x[k];
+        if (k > 0 && n1 > 0) {
+          double2 w = __ldg(twN + n1 * k);
+          if (SIGN > 0) w = cconj(w);
+          v = cmul(v, w);
+        }
+        p[k * (N1 + 1)] = v;
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
+      const int b = idx / N2, k2 = idx - b * N2;
+      double2 *p = sm + (size_t)b * ld + k2 * (N1 + 1);
+      double2 x[N1];
+#pragma unroll
+      for (int j = 0; j < N1; j++) x[j] = p[j];
+      rdft<N1, SIGN>(x);
+#pragma unroll
+      for (int j = 0; j < N1; j++) p[j] = x[j];
+    }
     __syncthreads();
   }
-}
+
+  // permuted -> natural (transpose of nat2perm)
+  template <int SIGN>
+  __device__ static void perm2nat(double2 *sm, int nb, int ld, const double2 *__restrict__ twN) {
+    for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
+      const int b = idx / N2, k2 = idx - b * N2;
+      double2 *p = sm + (size_t)b * ld + k2 * (N1 + 1);
+      double2 x[N1];
+#pragma unroll
+      for (int j = 0; j < N1; j++) x[j] = p[j];
+      rdft<N1, SIGN>(x);
+#pragma unroll
+      for (int j = 0; j < N1; j++) {
+        double2 v = x[j];
+        if (j > 0 && k2 > 0) {
+          double2 w = __ldg(twN + j * k2);
+          if (SIGN > 0) w = cconj(w);
+          v = cmul(v, w);
+        }
+        p[j] = v;
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
+      const int b = idx / N1, n1 = idx - b * N1;
+      double2 *p = sm + (size_t)b * ld + n1;
+      double2 x[N2];
+#pragma unroll
+      for (int j = 0; j < N2; j++) x[j] = p[j * (N1 + 1)];
+      rdft<N2, SIGN>(x);
+#pragma unroll
+      for (int j = 0; j < N2; j++) p[j * (N1 + 1)] = x[j];
+    }
+    __syncthreads();
+  }
+};
+
+#endif  // LMC_FFT_TU
 
 }  // namespace lmcd

@@ -1,0 +1,62 @@
+// lmc_dispatch.cu -- routes the transform launches to the translation unit
+// that instantiates the grid's transform lengths, and performs the one-time
+// per-device set-up of all kernels.
+#include <cuda_runtime.h>
+
+#include "lmc_kernels.cuh"
+
+namespace lmc {
+
+#define LMC_FFT_DECL(SUF)                                                              \
+  bool fft_has_##SUF(int n);                                                           \
+  bool fft_zinv_##SUF(const Dev &d, cudaStream_t s);                                   \
+  bool fft_zfwd_##SUF(const Dev &d, cudaStream_t s);                                   \
+  bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
+  size_t fft_zsm_##SUF(int n);                                                         \
+  size_t fft_xsm_##SUF(int n);                                                         \
+  cudaError_t fft_init_##SUF(int limit);
+LMC_FFT_DECL(a)
+LMC_FFT_DECL(b)
+LMC_FFT_DECL(c)
+cudaError_t ykernels_init(int limit);
+
+bool fft_supported(int n) { return fft_has_a(n) || fft_has_b(n) || fft_has_c(n); }
+
+void launch_zinv(const Dev &d, cudaStream_t s) {
+  if (!fft_zinv_a(d, s) && !fft_zinv_b(d, s)) fft_zinv_c(d, s);
+}
+void launch_zfwd(const Dev &d, cudaStream_t s) {
+  if (!fft_zfwd_a(d, s) && !fft_zfwd_b(d, s)) fft_zfwd_c(d, s);
+}
+void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+  if (!fft_xphys_a(d, rk, do_cfl, do_diag, s) && !fft_xphys_b(d, rk, do_cfl, do_diag, s))
+    fft_xphys_c(d, rk, do_cfl, do_diag, s);
+}
+size_t xphys_smem(const Dev &d) {
+  size_t v = fft_xsm_a(d.mgalx);
+  if (!v) v = fft_xsm_b(d.mgalx);
+  if (!v) v = fft_xsm_c(d.mgalx);
+  return v;
+}
+size_t z_smem(const Dev &d) {
+  size_t v = fft_zsm_a(d.mgalz);
+  if (!v) v = fft_zsm_b(d.mgalz);
+  if (!v) v = fft_zsm_c(d.mgalz);
+  return v;
+}
+
+cudaError_t kernels_init(const Dev &d) {
+  int dev = 0, limit = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+  const size_t need_y = (size_t)8 * d.ldy * sizeof(double2);
+  if ((size_t)limit < xphys_smem(d) + 1024 || (size_t)limit < z_smem(d) + 1024 || (size_t)limit < need_y + 1024)
+    return cudaErrorInvalidValue;
+  if ((e = fft_init_a(limit)) != cudaSuccess) return e;
+  if ((e = fft_init_b(limit)) != cudaSuccess) return e;
+  if ((e = fft_init_c(limit)) != cudaSuccess) return e;
+  return ykernels_init(limit);
+}
+
+}  // namespace lmc

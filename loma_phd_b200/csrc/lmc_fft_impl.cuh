@@ -1,0 +1,322 @@
+// lmc_fft_impl.cuh -- transform kernels of one lomacte RK3 substep (FP64),
+// templated on the four-step factorisation N = N1*N2 of the transform
+// length.  Included by the lmc_fft_*.cu translation units, each of which
+// instantiates a group of lengths (they compile in parallel).
+//
+//   zinv : localyz2zy + fourz(+1) (fou3D.f:80-145): spectral [y][kx][kz]
+//          -> zero-padded kz -> inverse c2c along z -> z-physical [y][z][kx]
+//   xphys: phys2 (cross.f:1440-1828): per (y,z) line, inverse real x
+//          transforms of 8 fields (two per complex transform), FP64
+//          products, T update, d(rho)/dt source, CFL maxima, direct x
+//          transforms of 11 fields truncated to kx < mx/2
+//   zfwd : fourz(-1) + localzy2yz (fou3D.f:149-189): direct c2c along z,
+//          truncation to the mz retained kz, back to [y][kx][kz]
+#pragma once
+#define LMC_FFT_TU
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "lmc_kernels.cuh"
+
+using namespace lmcd;
+
+namespace lmc {
+namespace LMC_FFT_NS {
+
+template <int N1, int N2>
+struct Geo {
+  static constexpr int N = N1 * N2;
+  static constexpr int LD = Four<N1, N2>::LD | 1;     // odd line stride
+  static constexpr int KB = (N <= 384) ? 16 : 8;      // kx lines per z-transform block
+  static constexpr int ZB = (64 / N1) > 0 ? (64 / N1) : 1;  // z lines per x-transform block
+  static constexpr int XT = ((4 * ZB * N1 + 31) / 32) * 32 > 256 ? 256 : ((4 * ZB * N1 + 31) / 32) * 32;
+};
+
+__device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ? k : k + (d.mgalz - d.mz); }
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_zinv(Dev d) {
+  using F = Four<N1, N2>;
+  using G = Geo<N1, N2>;
+  extern __shared__ double2 sm[];
+  const int f = blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
+  const int nb = min(G::KB, d.nkx - i0);
+  const double2 *src;
+  int mult = 0;  // 0: as is, 1: * i kx, 2: * i kz
+  switch (f) {
+    case 0: src = d.sb[SB_RU]; break;
+    case 1: src = d.sb[SB_RV]; break;
+    case 2: src = d.sb[SB_RW]; break;
+    case 3: src = d.sb[SB_LAPT]; break;
+    case 4: src = d.scal; mult = 1; break;
+    case 5: src = d.sb[SB_DTDY]; break;
+    case 6: src = d.scal; mult = 2; break;
+    default: src = d.scal; break;
+  }
+  for (int idx = threadIdx.x; idx < G::KB * G::LD; idx += blockDim.x) sm[idx] = czero();
+  __syncthreads();
+  for (int il = 0; il < nb; il++) {
+    const double kx = __ldg(d.kx + i0 + il);
+    const double2 *row = src + ((size_t)y * d.nkx + i0 + il) * d.mz;
+    for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
+      double2 v = __ldg(row + k);
+      if (mult == 1) v = cik(kx, v);
+      else if (mult == 2) v = cik(__ldg(d.kz + k), v);
+      sm[il * G::LD + F::sk(kz_pad(d, k))] = v;
+    }
+  }
+  __syncthreads();
+  F::template nat2perm<+1>(sm, nb, G::LD, d.twz);
+  double2 *dst = d.zb[f] + (size_t)y * N1 * N2 * d.nkx + i0;
+  for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
+    const int z = idx / G::KB, il = idx - z * G::KB;
+    if (il < nb) dst[(size_t)z * d.nkx + il] = sm[il * G::LD + F::sk(z)];
+  }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_zfwd(Dev d) {
+  using F = Four<N1, N2>;
+  using G = Geo<N1, N2>;
+  extern __shared__ double2 sm[];
+  const int f = blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
+  const int nb = min(G::KB, d.nkx - i0);
+  const double2 *src = d.zb[f] + (size_t)y * N1 * N2 * d.nkx + i0;
+  for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
+    const int z = idx / G::KB, il = idx - z * G::KB;
+    if (il < nb) sm[il * G::LD + F::sk(z)] = __ldg(src + (size_t)z * d.nkx + il);
+  }
+  __syncthreads();
+  F::template perm2nat<-1>(sm, nb, G::LD, d.twz);
+  const double dn = 1.0 / (double)F::N;
+  for (int il = 0; il < nb; il++) {
+    double2 *row = d.sb[f] + ((size_t)y * d.nkx + i0 + il) * d.mz;
+    for (int k = threadIdx.x; k < d.mz; k += blockDim.x) row[k] = cscale(dn, sm[il * G::LD + F::sk(kz_pad(d, k))]);
+  }
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// Input pairs (A + iB per complex transform):
+//   (rho u, rho v) (rho w, lap T) (dT/dx, dT/dy) (dT/dz, T)
+// Output pairs: (u, v) (w, rho uu) (rho vv, rho ww) (rho uv, rho uw)
+//               (rho vw, drho) (DT, 0)
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_xphys(Dev d, int rk, int do_cfl, int do_diag) {
+  using F = Four<N1, N2>;
+  using G = Geo<N1, N2>;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD;
+  extern __shared__ double2 sm[];
+  __shared__ unsigned long long s_tmax[ZB];
+  __shared__ double s_red[4][8];
+  const int y = blockIdx.y, z0 = blockIdx.x * ZB;
+  const int nzb = min(ZB, d.mgalz - z0), nkx = d.nkx;
+  for (int idx = threadIdx.x; idx < 4 * ZB * LD; idx += blockDim.x) sm[idx] = czero();
+  for (int idx = threadIdx.x; idx < ZB; idx += blockDim.x) s_tmax[idx] = 0ull;
+  __syncthreads();
+  for (int p = 0; p < 4; p++) {
+    const double2 *A = d.zb[2 * p], *B = d.zb[2 * p + 1];
+    for (int l = 0; l < nzb; l++) {
+      const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
+      double2 *line = sm + (size_t)(p * ZB + l) * LD;
+      for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
+        const double2 a = __ldg(A + g0 + k), b = __ldg(B + g0 + k);
+        if (k == 0) {
+          line[F::sk(0)] = make_double2(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
+        } else {
+          line[F::sk(k)] = make_double2(a.x - b.y, a.y + b.x);
+          line[F::sk(N - k)] = make_double2(a.x + b.y, b.x - a.y);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  F::template nat2perm<+1>(sm, 4 * ZB, LD, d.twx);
+
+  const double dt = d.scal_d[0];
+  const double dtxi = dt * d.xi[rk], dtg = dt * d.gama[rk], dtb = dt * d.beta[rk];
+  const double ab = d.alpha[rk] / d.beta[rk], ipe = 1.0 / d.peclet;
+  double mu = 0.0, mv = 0.0, mw = 0.0, rs = 0.0;
+  for (int l = 0; l < nzb; l++) {
+    double *rhl = d.rhst + ((size_t)y * d.mgalz + z0 + l) * N;
+    double tmax = 0.0;
+    for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
+      const int sp = F::sk(pos);
+      double2 *c0 = sm + (size_t)l * LD + sp;
+      double2 *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
+      double2 *c4 = c3 + (size_t)ZB * LD, *c5 = c4 + (size_t)ZB * LD;
+      const double2 p0 = *c0, p1 = *c1, p2 = *c2, p3 = *c3;
+      const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
+      const double rhp = rhl[pos];
+      const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
+      double tn = T + dtxi * rhp;                                      // cross.f:1626
+      double d8 = dtxi * rhp;                                          // cross.f:1627
+      const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
+      rhl[pos] = rhs;
+      tn = tn + dtg * rhs;                                             // cross.f:1641
+      d8 = d8 + dtg * rhs;                                             // cross.f:1642
+      const double drho = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);  // cross.f:1670-1671
+      *c0 = make_double2(u, v);
+      *c1 = make_double2(w, ru * u);
+      *c2 = make_double2(rv * v, rw * w);
+      *c3 = make_double2(ru * v, ru * w);
+      *c4 = make_double2(rv * w, drho);
+      *c5 = make_double2(d8, 0.0);
+      if (do_cfl) {
+        mu = fmax(mu, fabs(u));
+        mv = fmax(mv, fabs(v));
+        mw = fmax(mw, fabs(w));
+        tmax = fmax(tmax, T);
+      }
+      if (do_diag) rs += 1.0 / T;
+    }
+    if (do_cfl) {
+      tmax = warp_max(tmax);
+      if ((threadIdx.x & 31) == 0) atomic_max_pos(&s_tmax[l], tmax);
+    }
+  }
+  __syncthreads();
+  F::template perm2nat<-1>(sm, 6 * ZB, LD, d.twx);
+  const double dn = 1.0 / (double)N, hdn = 0.5 * dn;
+  for (int p = 0; p < 6; p++) {
+    double2 *A = d.zb[2 * p];
+    double2 *B = (2 * p + 1 < 11) ? d.zb[2 * p + 1] : nullptr;
+    for (int l = 0; l < nzb; l++) {
+      const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
+      const double2 *line = sm + (size_t)(p * ZB + l) * LD;
+      for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
+        const double2 c = line[F::sk(k)];
+        double2 a, b;
+        if (k == 0) {
+          a = make_double2(c.x * dn, 0.0);
+          b = make_double2(c.y * dn, 0.0);
+        } else {
+          const double2 q = line[F::sk(N - k)];
+          a = make_double2((c.x + q.x) * hdn, (c.y - q.y) * hdn);
+          b = make_double2((c.y + q.y) * hdn, (q.x - c.x) * hdn);
+        }
+        A[g0 + k] = a;
+        if (B) B[g0 + k] = b;
+      }
+    }
+  }
+  if (do_cfl || do_diag) {
+    mu = warp_max(mu); mv = warp_max(mv); mw = warp_max(mw); rs = warp_sum(rs);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { s_red[0][wid] = mu; s_red[1][wid] = mv; s_red[2][wid] = mw; s_red[3][wid] = rs; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nw = blockDim.x >> 5;
+      double a = 0, b = 0, c = 0, r = 0;
+      for (int q = 0; q < nw; q++) {
+        a = fmax(a, s_red[0][q]); b = fmax(b, s_red[1][q]); c = fmax(c, s_red[2][q]); r += s_red[3][q];
+      }
+      if (do_cfl) {
+        const double hy = d.hy[y];
+        double ct = 0.0;
+        for (int l = 0; l < nzb; l++) {
+          const double DD = ipe * __longlong_as_double((long long)s_tmax[l]);  // cross.f:1704
+          ct = fmax(ct, 2.0 * DD * ((d.hxalp / 2) * (d.hxalp / 2) + (d.hzbet / 2) * (d.hzbet / 2) + (1.0 / hy) * (1.0 / hy)));
+        }
+        atomic_max_pos(d.cflmax + 0, a);
+        atomic_max_pos(d.cflmax + 1, b / hy);
+        atomic_max_pos(d.cflmax + 2, c);
+        atomic_max_pos(d.cflmax + 3, ct);
+      }
+      if (do_diag) atomicAdd(d.rhom + y, r);
+    }
+  }
+}
+
+template <int N1, int N2>
+struct Launch {
+  using G = Geo<N1, N2>;
+  static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(double2); }
+  static size_t xsm() { return (size_t)6 * G::ZB * G::LD * sizeof(double2); }
+  static void zinv(const Dev &d, cudaStream_t s) {
+    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 8);
+    k_zinv<N1, N2><<<g, 256, zsm(), s>>>(d);
+  }
+  static void zfwd(const Dev &d, cudaStream_t s) {
+    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 11);
+    k_zfwd<N1, N2><<<g, 256, zsm(), s>>>(d);
+  }
+  static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+    dim3 g((d.mgalz + G::ZB - 1) / G::ZB, d.my);
+    k_xphys<N1, N2><<<g, G::XT, xsm(), s>>>(d, rk, do_cfl, do_diag);
+  }
+  static cudaError_t optin(int limit) {
+    cudaError_t e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_zinv<N1, N2>)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute((const void *)k_zinv<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  limit - (int)fa.sharedSizeBytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_zfwd<N1, N2>)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute((const void *)k_zfwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  limit - (int)fa.sharedSizeBytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_xphys<N1, N2>)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute((const void *)k_xphys<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                limit - (int)fa.sharedSizeBytes);
+  }
+};
+
+// register-DFT twiddles exp(-2 pi i e / R) of every block size
+inline cudaError_t upload_twiddles() {
+  std::vector<double2> t;
+  for (int R : TW_SIZES)
+    for (int e = 0; e < R; e++) {
+      const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)R;
+      t.push_back(make_double2((double)cosl(a), (double)(-sinl(a))));
+    }
+  return cudaMemcpyToSymbol(c_tw, t.data(), t.size() * sizeof(double2));
+}
+
+}  // namespace LMC_FFT_NS
+}  // namespace lmc
+
+// Each translation unit defines LMC_FFT_SIZES(X) as X(N, N1, N2) entries and
+// then expands LMC_FFT_TU_BODY(suffix) to get its dispatch functions.
+#define LMC_FFT_CASE_Z(N, N1, N2, WHAT) \
+  case N: Launch<N1, N2>::WHAT(d, s); return true;
+#define LMC_FFT_CASE_X(N, N1, N2) \
+  case N: Launch<N1, N2>::xphys(d, rk, do_cfl, do_diag, s); return true;
+#define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
+#define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
+#define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2>::zsm();
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2>::xsm();
+#define LMC_FFT_CASE_OPT(N, N1, N2) \
+  if ((e = Launch<N1, N2>::optin(limit)) != cudaSuccess) return e;
+#define LMC_FFT_CASE_HAS(N, N1, N2) case N: return true;
+
+#define LMC_FFT_TU_BODY(SUF)                                                                      \
+  namespace lmc {                                                                                 \
+  using namespace LMC_FFT_NS;                                                                     \
+  bool fft_has_##SUF(int n) {                                                                     \
+    switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_HAS) default: return false; }                         \
+  }                                                                                               \
+  bool fft_zinv_##SUF(const Dev &d, cudaStream_t s) {                                             \
+    switch (d.mgalz) { LMC_FFT_SIZES(LMC_FFT_CASE_ZI) default: return false; }                     \
+  }                                                                                               \
+  bool fft_zfwd_##SUF(const Dev &d, cudaStream_t s) {                                             \
+    switch (d.mgalz) { LMC_FFT_SIZES(LMC_FFT_CASE_ZF) default: return false; }                     \
+  }                                                                                               \
+  bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {           \
+    switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_X) default: return false; }                      \
+  }                                                                                               \
+  size_t fft_zsm_##SUF(int n) {                                                                   \
+    switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_ZS) default: return 0; }                             \
+  }                                                                                               \
+  size_t fft_xsm_##SUF(int n) {                                                                   \
+    switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_XS) default: return 0; }                              \
+  }                                                                                               \
+  cudaError_t fft_init_##SUF(int limit) {                                                         \
+    cudaError_t e = upload_twiddles();                                                            \
+    if (e != cudaSuccess) return e;                                                               \
+    LMC_FFT_SIZES(LMC_FFT_CASE_OPT)                                                               \
+    return cudaSuccess;                                                                           \
+  }                                                                                               \
+  }

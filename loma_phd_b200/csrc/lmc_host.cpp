@@ -225,6 +225,74 @@ void build_yops(int my, const double *y, YOps &o) {
   }
 }
 
+// Chunk transfer matrices and Kogge-Stone tables.  The device solves run
+// each lane's chunk of rows with an incoming state S (the last B solution
+// values, most recent first); the chunk maps S_in to S_out = M S_in + p.
+// At scan step s (offset 2^s) lane l composes with lane l -/+ 2^s, using
+// the map of the lanes already folded into it: the table holds that map.
+static std::vector<double> scan_table(int my, int B, const std::vector<double> &T, bool upper, int lpm, int base,
+                                      int extra) {
+  const int W = upper ? B + 1 : B;
+  std::vector<std::vector<double>> M(32, std::vector<double>(B * B, 0.0));
+  for (int l = 0; l < 32; l++) {
+    const int n = (l < lpm) ? base + (l < extra ? 1 : 0) : 0;
+    const int s0 = (l < lpm) ? l * base + (l < extra ? l : extra) : 0;
+    for (int q = 0; q < B; q++) {
+      std::vector<double> S(B, 0.0);
+      S[q] = 1.0;
+      for (int tt = 0; tt < n; tt++) {
+        const int row = upper ? s0 + n - 1 - tt : s0 + tt;
+        if (row >= my) break;
+        double v = 0.0;
+        for (int d = 0; d < B; d++) v -= T[(size_t)row * W + (upper ? 1 + d : d)] * S[d];
+        if (upper) v *= T[(size_t)row * W];
+        for (int d = B - 1; d > 0; d--) S[d] = S[d - 1];
+        S[0] = v;
+      }
+      for (int r = 0; r < B; r++) M[l][r * B + q] = S[r];
+    }
+  }
+  std::vector<double> tab((size_t)5 * 32 * B * B, 0.0);
+  for (int s = 0; s < 5; s++) {
+    const int off = 1 << s;
+    std::vector<std::vector<double>> nM = M;
+    for (int l = 0; l < 32; l++) {
+      const int o = upper ? l + off : l - off;
+      if (o < 0 || o >= 32) continue;
+      for (int i = 0; i < B * B; i++) tab[((size_t)s * 32 + l) * B * B + i] = M[l][i];
+      for (int r = 0; r < B; r++)
+        for (int q = 0; q < B; q++) {
+          double a = 0.0;
+          for (int k = 0; k < B; k++) a += M[l][r * B + k] * M[o][k * B + q];
+          nM[l][r * B + q] = a;
+        }
+    }
+    M = nM;
+  }
+  return tab;
+}
+
+std::vector<double> chunk_major(const std::vector<double> &T, int my, int W, int C, int lpm, int base, int extra) {
+  std::vector<double> out((size_t)C * W * 32, 0.0);
+  for (int l = 0; l < lpm && l < 32; l++) {
+    const int n = base + (l < extra ? 1 : 0), s0 = l * base + (l < extra ? l : extra);
+    for (int t = 0; t < n && t < C; t++)
+      for (int c = 0; c < W; c++)
+        if (s0 + t < my) out[((size_t)t * W + c) * 32 + l] = T[(size_t)(s0 + t) * W + c];
+  }
+  return out;
+}
+
+void build_scans(YOps &o, int lpm, int base, int extra) {
+  const int my = o.my;
+  o.k1L = scan_table(my, 3, o.p1L, false, lpm, base, extra);
+  o.k1U = scan_table(my, 3, o.p1U, true, lpm, base, extra);
+  o.k3L = scan_table(my, 2, o.p3L, false, lpm, base, extra);
+  o.k3U = scan_table(my, 2, o.p3U, true, lpm, base, extra);
+  o.k8L = scan_table(my, 3, o.i8L, false, lpm, base, extra);
+  o.k8U = scan_table(my, 3, o.i8U, true, lpm, base, extra);
+}
+
 // Per-mode data of the Poisson operator dt22 - k^2 dt21 with Dirichlet
 // (identity) wall rows: laps.f:349-366 (Lapvdvhom) and laps.f:648-728
 // (solvepsi, whose homogeneous solutions and 2x2 Neumann matrix depend on

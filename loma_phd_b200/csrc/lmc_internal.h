@@ -35,6 +35,8 @@ struct YOps {
   std::vector<double> p3L, p3U;                   // [my][2], [my][3]
   std::vector<double> i8L, i8U;                   // [my][3], [my][4]
   std::vector<double> ebot, etop;                 // dv/dy at the walls as linear functionals
+  // Kogge-Stone scan tables of the chunked device solves ([5][32][B][B])
+  std::vector<double> k1L, k1U, k3L, k3U, k8L, k8U;
 };
 
 // Per-mode Poisson data (operator dt22 - k^2 dt21 with identity wall rows).
@@ -47,6 +49,12 @@ struct PoissonTables {
 };
 
 void build_yops(int my, const double *y, YOps &ops);
+// Chunk-major copy of a row table T[my][W] for the lane split of a pencil:
+// out[(t*W + c)*32 + l] = T[s_l + t][c] (zero where lane l has no row t).
+std::vector<double> chunk_major(const std::vector<double> &T, int my, int W, int C, int lpm, int base, int extra);
+// Scan tables of the constant band solves for the chunk split of a pencil
+// over the lanes of a warp (lane l owns n_l rows starting at s_l).
+void build_scans(YOps &ops, int lpm, int base, int extra);
 void build_poisson(const Grid &g, const YOps &ops, const double *kx,
                    const double *kz, PoissonTables &pt);
 // Band helpers used by the host code (row-form LU, see build_yops).
