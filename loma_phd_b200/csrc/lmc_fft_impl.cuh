@@ -25,19 +25,25 @@ using namespace lmcd;
 namespace lmc {
 namespace LMC_FFT_NS {
 
+// Small blocks (about 64 threads, one task of the first FFT pass per
+// thread) so that several blocks share an SM and overlap their
+// barrier-separated phases.
+constexpr int round32(int v) { return ((v + 31) / 32) * 32; }
 template <int N1, int N2>
 struct Geo {
   static constexpr int N = N1 * N2;
-  static constexpr int LD = Four<N1, N2>::LD | 1;     // odd line stride
-  static constexpr int KB = (N <= 384) ? 16 : 8;      // kx lines per z-transform block
-  static constexpr int ZB = (64 / N1) > 0 ? (64 / N1) : 1;  // z lines per x-transform block
-  static constexpr int XT = ((4 * ZB * N1 + 31) / 32) * 32 > 256 ? 256 : ((4 * ZB * N1 + 31) / 32) * 32;
+  static constexpr int LD = Four<N1, N2>::LD | 1;           // odd line stride
+  static constexpr int KB = (64 / N1) > 0 ? (64 / N1) : 1;  // kx lines per z-transform block
+  static constexpr int ZT = round32(KB * N1);               // threads of a z-transform block
+  static constexpr int ZB = (16 / N1) > 0 ? (16 / N1) : 1;  // z lines per x-transform block
+  static constexpr int XT = round32(4 * ZB * N1);           // threads of an x-transform block
+  static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
 };
 
 __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ? k : k + (d.mgalz - d.mz); }
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_zinv(Dev d) {
+__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d) {
   using F = Four<N1, N2>;
   using G = Geo<N1, N2>;
   extern __shared__ double2 sm[];
@@ -77,7 +83,7 @@ __global__ void __launch_bounds__(256) k_zinv(Dev d) {
 }
 
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_zfwd(Dev d) {
+__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zfwd(Dev d) {
   using F = Four<N1, N2>;
   using G = Geo<N1, N2>;
   extern __shared__ double2 sm[];
@@ -103,13 +109,42 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) 
 
 // Input pairs (A + iB per complex transform):
 //   (rho u, rho v) (rho w, lap T) (dT/dx, dT/dy) (dT/dz, T)
-// Output pairs: (u, v) (w, rho uu) (rho vv, rho ww) (rho uv, rho uw)
-//               (rho vw, drho) (DT, 0)
+// Output pairs, first round: (u, v) (w, rho uu) (rho vv, rho ww) (rho uv, rho uw)
+// second round (kept in registers meanwhile): (rho vw, drho) (DT, 0)
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_xphys(Dev d, int rk, int do_cfl, int do_diag) {
+__device__ __forceinline__ void x_extract(const Dev &d, const double2 *sm, int p, int fa, int fb, int y, int z0,
+                                          int nzb) {
   using F = Four<N1, N2>;
   using G = Geo<N1, N2>;
-  constexpr int N = F::N, ZB = G::ZB, LD = G::LD;
+  constexpr int N = F::N;
+  const double dn = 1.0 / (double)N, hdn = 0.5 * dn;
+  double2 *A = d.zb[fa];
+  double2 *B = fb >= 0 ? d.zb[fb] : nullptr;
+  for (int l = 0; l < nzb; l++) {
+    const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * d.nkx;
+    const double2 *line = sm + (size_t)(p * G::ZB + l) * G::LD;
+    for (int k = threadIdx.x; k < d.nkx; k += blockDim.x) {
+      const double2 c = line[F::sk(k)];
+      double2 a, b;
+      if (k == 0) {
+        a = make_double2(c.x * dn, 0.0);
+        b = make_double2(c.y * dn, 0.0);
+      } else {
+        const double2 q = line[F::sk(N - k)];
+        a = make_double2((c.x + q.x) * hdn, (c.y - q.y) * hdn);
+        b = make_double2((c.y + q.y) * hdn, (q.x - c.x) * hdn);
+      }
+      A[g0 + k] = a;
+      if (B) B[g0 + k] = b;
+    }
+  }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do_cfl, int do_diag) {
+  using F = Four<N1, N2>;
+  using G = Geo<N1, N2>;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
   extern __shared__ double2 sm[];
   __shared__ unsigned long long s_tmax[ZB];
   __shared__ double s_red[4][8];
@@ -141,69 +176,63 @@ __global__ void __launch_bounds__(256) k_xphys(Dev d, int rk, int do_cfl, int do
   const double dtxi = dt * d.xi[rk], dtg = dt * d.gama[rk], dtb = dt * d.beta[rk];
   const double ab = d.alpha[rk] / d.beta[rk], ipe = 1.0 / d.peclet;
   double mu = 0.0, mv = 0.0, mw = 0.0, rs = 0.0;
-  for (int l = 0; l < nzb; l++) {
-    double *rhl = d.rhst + ((size_t)y * d.mgalz + z0 + l) * N;
-    double tmax = 0.0;
-    for (int pos = threadIdx.x; pos < N; pos += blockDim.x) {
-      const int sp = F::sk(pos);
-      double2 *c0 = sm + (size_t)l * LD + sp;
+  double r0[PT], r1[PT], r2[PT];
+#pragma unroll
+  for (int j = 0; j < PT; j++) {
+    const int q = threadIdx.x + j * blockDim.x;
+    r0[j] = r1[j] = r2[j] = 0.0;
+    if (q < nzb * N) {
+      const int l = q / N, pos = q - l * N;
+      double2 *c0 = sm + (size_t)l * LD + F::sk(pos);
       double2 *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
-      double2 *c4 = c3 + (size_t)ZB * LD, *c5 = c4 + (size_t)ZB * LD;
       const double2 p0 = *c0, p1 = *c1, p2 = *c2, p3 = *c3;
       const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
-      const double rhp = rhl[pos];
+      double *rh = d.rhst + ((size_t)y * d.mgalz + z0 + l) * N + pos;
+      const double rhp = *rh;
       const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
       double tn = T + dtxi * rhp;                                      // cross.f:1626
       double d8 = dtxi * rhp;                                          // cross.f:1627
       const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
-      rhl[pos] = rhs;
+      *rh = rhs;
       tn = tn + dtg * rhs;                                             // cross.f:1641
       d8 = d8 + dtg * rhs;                                             // cross.f:1642
-      const double drho = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);  // cross.f:1670-1671
       *c0 = make_double2(u, v);
-      *c1 = make_double2(w, ru * u);
+      *c1 = make_double2(w, ru * u);                                   // cross.f:1655-1666
       *c2 = make_double2(rv * v, rw * w);
       *c3 = make_double2(ru * v, ru * w);
-      *c4 = make_double2(rv * w, drho);
-      *c5 = make_double2(d8, 0.0);
+      r0[j] = rv * w;
+      r1[j] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);              // cross.f:1670-1671
+      r2[j] = d8;                                                      // cross.f:1645-1647
       if (do_cfl) {
         mu = fmax(mu, fabs(u));
         mv = fmax(mv, fabs(v));
         mw = fmax(mw, fabs(w));
-        tmax = fmax(tmax, T);
+        atomic_max_pos(&s_tmax[l], fmax(T, 0.0));
       }
       if (do_diag) rs += 1.0 / T;
     }
-    if (do_cfl) {
-      tmax = warp_max(tmax);
-      if ((threadIdx.x & 31) == 0) atomic_max_pos(&s_tmax[l], tmax);
+  }
+  __syncthreads();
+  F::template perm2nat<-1>(sm, 4 * ZB, LD, d.twx);
+  x_extract<N1, N2>(d, sm, 0, OU, OV, y, z0, nzb);
+  x_extract<N1, N2>(d, sm, 1, OW, ORUU, y, z0, nzb);
+  x_extract<N1, N2>(d, sm, 2, ORVV, ORWW, y, z0, nzb);
+  x_extract<N1, N2>(d, sm, 3, ORUV, ORUW, y, z0, nzb);
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < PT; j++) {
+    const int q = threadIdx.x + j * blockDim.x;
+    if (q < ZB * N) {
+      const int l = q / N, pos = q - l * N;
+      double2 *c0 = sm + (size_t)l * LD + F::sk(pos);
+      c0[0] = make_double2(r0[j], r1[j]);
+      c0[(size_t)ZB * LD] = make_double2(r2[j], 0.0);
     }
   }
   __syncthreads();
-  F::template perm2nat<-1>(sm, 6 * ZB, LD, d.twx);
-  const double dn = 1.0 / (double)N, hdn = 0.5 * dn;
-  for (int p = 0; p < 6; p++) {
-    double2 *A = d.zb[2 * p];
-    double2 *B = (2 * p + 1 < 11) ? d.zb[2 * p + 1] : nullptr;
-    for (int l = 0; l < nzb; l++) {
-      const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
-      const double2 *line = sm + (size_t)(p * ZB + l) * LD;
-      for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
-        const double2 c = line[F::sk(k)];
-        double2 a, b;
-        if (k == 0) {
-          a = make_double2(c.x * dn, 0.0);
-          b = make_double2(c.y * dn, 0.0);
-        } else {
-          const double2 q = line[F::sk(N - k)];
-          a = make_double2((c.x + q.x) * hdn, (c.y - q.y) * hdn);
-          b = make_double2((c.y + q.y) * hdn, (q.x - c.x) * hdn);
-        }
-        A[g0 + k] = a;
-        if (B) B[g0 + k] = b;
-      }
-    }
-  }
+  F::template perm2nat<-1>(sm, 2 * ZB, LD, d.twx);
+  x_extract<N1, N2>(d, sm, 0, ORVW, ODRHO, y, z0, nzb);
+  x_extract<N1, N2>(d, sm, 1, ODT, -1, y, z0, nzb);
   if (do_cfl || do_diag) {
     mu = warp_max(mu); mv = warp_max(mv); mw = warp_max(mw); rs = warp_sum(rs);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,14 +265,14 @@ template <int N1, int N2>
 struct Launch {
   using G = Geo<N1, N2>;
   static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(double2); }
-  static size_t xsm() { return (size_t)6 * G::ZB * G::LD * sizeof(double2); }
+  static size_t xsm() { return (size_t)4 * G::ZB * G::LD * sizeof(double2); }
   static void zinv(const Dev &d, cudaStream_t s) {
     dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 8);
-    k_zinv<N1, N2><<<g, 256, zsm(), s>>>(d);
+    k_zinv<N1, N2><<<g, G::ZT, zsm(), s>>>(d);
   }
   static void zfwd(const Dev &d, cudaStream_t s) {
     dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 11);
-    k_zfwd<N1, N2><<<g, 256, zsm(), s>>>(d);
+    k_zfwd<N1, N2><<<g, G::ZT, zsm(), s>>>(d);
   }
   static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     dim3 g((d.mgalz + G::ZB - 1) / G::ZB, d.my);
