@@ -150,6 +150,19 @@ int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_params *ic,
  * Used by the parity tests of the y-kernels. */
 int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev,
              double *out2_dev);
+/* Compact first y-derivative (the operator of op 1 above) for callers that
+ * may not allocate device memory: drivers with a fixed device-memory
+ * budget, or time loops that cannot afford the device-wide synchronisation
+ * of cudaFree.  It has no counterpart in the reference.  It takes npencil
+ * complex pencils of my points each (y fastest, re/im interleaved) at
+ * in_dev and writes d/dy to out_dev on `stream` (a cudaStream_t; NULL for
+ * the default stream).  Its operator tables live in one fixed 256 KiB
+ * device array per device (no cudaMalloc/cudaFree): my <= 544, larger
+ * returns LMC_EINVAL.  The array is shared by all calls and overwritten by
+ * each; calls that overlap on the GPU race on it.  The first call on a
+ * device takes the array's address and should precede any stream capture. */
+int lmc_deryr2_noalloc(int my, const double *y, int npencil,
+                       const double *in_dev, double *out_dev, void *stream);
 #ifdef __cplusplus
 }
 #endif

@@ -30,7 +30,7 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read",
+    "lmc_profile_read", "lmc_deryr2_noalloc",
 )
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset")
@@ -99,6 +99,7 @@ def _lib():
         L.lmc_op_y.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         L.lmc_profile_start.argtypes = [vp]
         L.lmc_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
+        L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
         _LIB = L
     return _LIB
 
@@ -187,6 +188,14 @@ def make_ic(p: Params, y: np.ndarray, ic: ICParams):
                             *[_ptr(a.view(np.float64)) for a in f], *[_ptr(a) for a in r])
     _check(rc, "lmc_make_ic")
     return dict(vor=f[0], phi=f[1], psi=f[2], scal=f[3], u00=r[0], v00=r[1], w00=r[2], time=0.0)
+
+
+def deryr2_noalloc(y: np.ndarray, npencil: int, in_ptr: int, out_ptr: int, stream: int = 0) -> int:
+    """d/dy of npencil device pencils without any device allocation (see
+    lmc_deryr2_noalloc in include/lomacte_b200.h).  Returns the status."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return _lib().lmc_deryr2_noalloc(len(y), _ptr(y), int(npencil), ctypes.c_void_p(in_ptr),
+                                     ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream))
 
 
 class Lomacte:
