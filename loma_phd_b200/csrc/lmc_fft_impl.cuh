@@ -18,6 +18,7 @@
 #include <cmath>
 #include <vector>
 
+#include "lmc_async.cuh"
 #include "lmc_kernels.cuh"
 
 using namespace lmcd;
@@ -42,43 +43,77 @@ struct Geo {
 
 __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ? k : k + (d.mgalz - d.mz); }
 
+// Persistent: each block walks tiles (field, y, kx block) with stride
+// gridDim.x; the next tile's kz rows (one contiguous run of nb*mz complex
+// values in the [y][kx][kz] layout) arrive by a TMA bulk copy while the
+// current tile is transformed.
 template <int N1, int N2>
-__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d) {
+__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
   using F = Four<N1, N2>;
   using G = Geo<N1, N2>;
+  constexpr int KB = G::KB, LD = G::LD;
   extern __shared__ double2 sm[];
-  const int f = blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
-  const int nb = min(G::KB, d.nkx - i0);
-  const double2 *src;
-  int mult = 0;  // 0: as is, 1: * i kx, 2: * i kz
-  switch (f) {
-    case 0: src = d.sb[SB_RU]; break;
-    case 1: src = d.sb[SB_RV]; break;
-    case 2: src = d.sb[SB_RW]; break;
-    case 3: src = d.sb[SB_LAPT]; break;
-    case 4: src = d.scal; mult = 1; break;
-    case 5: src = d.sb[SB_DTDY]; break;
-    case 6: src = d.scal; mult = 2; break;
-    default: src = d.scal; break;
-  }
-  for (int idx = threadIdx.x; idx < G::KB * G::LD; idx += blockDim.x) sm[idx] = czero();
-  __syncthreads();
-  for (int il = 0; il < nb; il++) {
-    const double kx = __ldg(d.kx + i0 + il);
-    const double2 *row = src + ((size_t)y * d.nkx + i0 + il) * d.mz;
-    for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
-      double2 v = __ldg(row + k);
-      if (mult == 1) v = cik(kx, v);
-      else if (mult == 2) v = cik(__ldg(d.kz + k), v);
-      sm[il * G::LD + F::sk(kz_pad(d, k))] = v;
+  double2 *W = sm, *St = sm + KB * LD;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb;
+  auto src_of = [&](int f) -> const double2 * {
+    switch (f) {
+      case 0: return d.sb[SB_RU];
+      case 1: return d.sb[SB_RV];
+      case 2: return d.sb[SB_RW];
+      case 3: return d.sb[SB_LAPT];
+      case 5: return d.sb[SB_DTDY];
+      default: return d.scal;
     }
-  }
+  };
+  auto issue = [&](int t) {
+    const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
+    const int nb = min(KB, d.nkx - kb * KB);
+    const uint32_t bytes = (uint32_t)nb * d.mz * sizeof(double2);
+    mbar_expect_tx(&bar, bytes);
+    bulk_g2s(St, src_of(f) + ((size_t)y * d.nkx + kb * KB) * d.mz, bytes, &bar);
+  };
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
-  F::template nat2perm<+1>(sm, nb, G::LD, d.twz);
-  double2 *dst = d.zb[f] + (size_t)y * N1 * N2 * d.nkx + i0;
-  for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
-    const int z = idx / G::KB, il = idx - z * G::KB;
-    if (il < nb) dst[(size_t)z * d.nkx + il] = sm[il * G::LD + F::sk(z)];
+  int t = blockIdx.x;
+  if (threadIdx.x == 0 && t < ntiles) issue(t);
+  uint32_t ph = 0;
+  const int gap = d.mgalz - d.mz;  // zero-padded kz positions nz1+1 .. nz1+gap
+  for (; t < ntiles; t += gridDim.x) {
+    if (threadIdx.x == 0) s_ok = mbar_wait(&bar, ph, d.status);
+    __syncthreads();
+    if (!s_ok) return;
+    ph ^= 1;
+    const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
+    const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
+    const int mult = (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
+    for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
+      const int il = idx / gap, g = idx - il * gap;
+      W[il * LD + F::sk(d.nz1 + 1 + g)] = czero();
+    }
+    for (int il = 0; il < nb; il++) {
+      const double kx = __ldg(d.kx + i0 + il);
+      const double2 *row = St + il * d.mz;
+      for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
+        double2 v = row[k];
+        if (mult == 1) v = cik(kx, v);
+        else if (mult == 2) v = cik(__ldg(d.kz + k), v);
+        W[il * LD + F::sk(kz_pad(d, k))] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
+      fence_proxy_async();
+      issue(t + gridDim.x);
+    }
+    F::template nat2perm<+1>(W, nb, LD, d.twz);
+    double2 *dst = d.zb[f] + (size_t)y * F::N * d.nkx + i0;
+    for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
+      const int z = idx / KB, il = idx - z * KB;
+      if (il < nb) dst[(size_t)z * d.nkx + il] = W[il * LD + F::sk(z)];
+    }
+    __syncthreads();
   }
 }
 
@@ -140,123 +175,176 @@ __device__ __forceinline__ void x_extract(const Dev &d, const double2 *sm, int p
   }
 }
 
+// Persistent: each block walks tiles (y, z block of ZB lines).  The next
+// tile's eight input rows (each ZB*nkx contiguous complex values in the
+// [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
+// current tile is transformed.
 template <int N1, int N2>
-__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do_cfl, int do_diag) {
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
   using F = Four<N1, N2>;
   using G = Geo<N1, N2>;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
   extern __shared__ double2 sm[];
-  __shared__ unsigned long long s_tmax[ZB];
-  __shared__ double s_red[4][8];
-  const int y = blockIdx.y, z0 = blockIdx.x * ZB;
-  const int nzb = min(ZB, d.mgalz - z0), nkx = d.nkx;
-  for (int idx = threadIdx.x; idx < 4 * ZB * LD; idx += blockDim.x) sm[idx] = czero();
-  for (int idx = threadIdx.x; idx < ZB; idx += blockDim.x) s_tmax[idx] = 0ull;
-  __syncthreads();
-  for (int p = 0; p < 4; p++) {
-    const double2 *A = d.zb[2 * p], *B = d.zb[2 * p + 1];
-    for (int l = 0; l < nzb; l++) {
-      const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
-      double2 *line = sm + (size_t)(p * ZB + l) * LD;
-      for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
-        const double2 a = __ldg(A + g0 + k), b = __ldg(B + g0 + k);
-        if (k == 0) {
-          line[F::sk(0)] = make_double2(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
-        } else {
-          line[F::sk(k)] = make_double2(a.x - b.y, a.y + b.x);
-          line[F::sk(N - k)] = make_double2(a.x + b.y, b.x - a.y);
-        }
-      }
-    }
+  const int nkx = d.nkx;
+  double2 *W = sm;                         // 4 buffers x ZB lines x LD
+  double2 *St = sm + 4 * ZB * LD;          // 8 rows of ZB*nkx inputs
+  double *Sr = (double *)(St + 8 * ZB * nkx);  // ZB*N RHS(T)
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ok;
+  __shared__ unsigned long long s_tmax[ZB], s_vmax;
+  __shared__ double s_red[3][8];
+  const int nzk = (d.mgalz + ZB - 1) / ZB;
+  auto issue = [&](int t) {
+    const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
+    const uint32_t rb = (uint32_t)nzb * nkx * sizeof(double2), hb = (uint32_t)nzb * N * sizeof(double);
+    mbar_expect_tx(&bar, 8 * rb + hb);
+    const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
+    for (int f = 0; f < 8; f++) bulk_g2s(St + f * ZB * nkx, d.zb[f] + g0, rb, &bar);
+    bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    s_vmax = 0ull;
   }
+  for (int l = threadIdx.x; l < ZB; l += blockDim.x) s_tmax[l] = 0ull;
   __syncthreads();
-  F::template nat2perm<+1>(sm, 4 * ZB, LD, d.twx);
-
+  int t = blockIdx.x;
+  if (threadIdx.x == 0 && t < ntiles) issue(t);
+  uint32_t ph = 0;
+  const double ipe = 1.0 / d.peclet;
   const double dt = d.scal_d[0];
   const double dtxi = dt * d.xi[rk], dtg = dt * d.gama[rk], dtb = dt * d.beta[rk];
-  const double ab = d.alpha[rk] / d.beta[rk], ipe = 1.0 / d.peclet;
-  double mu = 0.0, mv = 0.0, mw = 0.0, rs = 0.0;
-  double r0[PT], r1[PT], r2[PT];
-#pragma unroll
-  for (int j = 0; j < PT; j++) {
-    const int q = threadIdx.x + j * blockDim.x;
-    r0[j] = r1[j] = r2[j] = 0.0;
-    if (q < nzb * N) {
-      const int l = q / N, pos = q - l * N;
-      double2 *c0 = sm + (size_t)l * LD + F::sk(pos);
-      double2 *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
-      const double2 p0 = *c0, p1 = *c1, p2 = *c2, p3 = *c3;
-      const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
-      double *rh = d.rhst + ((size_t)y * d.mgalz + z0 + l) * N + pos;
-      const double rhp = *rh;
-      const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
-      double tn = T + dtxi * rhp;                                      // cross.f:1626
-      double d8 = dtxi * rhp;                                          // cross.f:1627
-      const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
-      *rh = rhs;
-      tn = tn + dtg * rhs;                                             // cross.f:1641
-      d8 = d8 + dtg * rhs;                                             // cross.f:1642
-      *c0 = make_double2(u, v);
-      *c1 = make_double2(w, ru * u);                                   // cross.f:1655-1666
-      *c2 = make_double2(rv * v, rw * w);
-      *c3 = make_double2(ru * v, ru * w);
-      r0[j] = rv * w;
-      r1[j] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);              // cross.f:1670-1671
-      r2[j] = d8;                                                      // cross.f:1645-1647
-      if (do_cfl) {
-        mu = fmax(mu, fabs(u));
-        mv = fmax(mv, fabs(v));
-        mw = fmax(mw, fabs(w));
-        atomic_max_pos(&s_tmax[l], fmax(T, 0.0));
+  const double ab = d.alpha[rk] / d.beta[rk];
+  double mu = 0.0, mw = 0.0, cfy = 0.0, cft = 0.0;  // running maxima (cfy, cft: thread 0)
+  for (; t < ntiles; t += gridDim.x) {
+    if (threadIdx.x == 0) s_ok = mbar_wait(&bar, ph, d.status);
+    __syncthreads();
+    if (!s_ok) return;
+    ph ^= 1;
+    const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
+    // zero the dealiased gap kx = nkx .. N-nkx of the 4 input lines
+    const int gap = N - 2 * nkx + 1;
+    for (int idx = threadIdx.x; idx < 4 * ZB * gap; idx += blockDim.x) {
+      const int ln = idx / gap, g = idx - ln * gap;
+      W[ln * LD + F::sk(nkx + g)] = czero();
+    }
+    for (int p = 0; p < 4; p++)
+      for (int l = 0; l < ZB; l++) {
+        double2 *line = W + (p * ZB + l) * LD;
+        const double2 *A = St + (2 * p) * ZB * nkx + l * nkx, *B = St + (2 * p + 1) * ZB * nkx + l * nkx;
+        for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
+          double2 a = czero(), b = czero();
+          if (l < nzb) { a = A[k]; b = B[k]; }
+          if (k == 0) {
+            line[F::sk(0)] = make_double2(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
+          } else {
+            line[F::sk(k)] = make_double2(a.x - b.y, a.y + b.x);
+            line[F::sk(N - k)] = make_double2(a.x + b.y, b.x - a.y);
+          }
+        }
       }
-      if (do_diag) rs += 1.0 / T;
-    }
-  }
-  __syncthreads();
-  F::template perm2nat<-1>(sm, 4 * ZB, LD, d.twx);
-  x_extract<N1, N2>(d, sm, 0, OU, OV, y, z0, nzb);
-  x_extract<N1, N2>(d, sm, 1, OW, ORUU, y, z0, nzb);
-  x_extract<N1, N2>(d, sm, 2, ORVV, ORWW, y, z0, nzb);
-  x_extract<N1, N2>(d, sm, 3, ORUV, ORUW, y, z0, nzb);
-  __syncthreads();
+    double rh[PT];
 #pragma unroll
-  for (int j = 0; j < PT; j++) {
-    const int q = threadIdx.x + j * blockDim.x;
-    if (q < ZB * N) {
-      const int l = q / N, pos = q - l * N;
-      double2 *c0 = sm + (size_t)l * LD + F::sk(pos);
-      c0[0] = make_double2(r0[j], r1[j]);
-      c0[(size_t)ZB * LD] = make_double2(r2[j], 0.0);
+    for (int j = 0; j < PT; j++) {
+      const int q = threadIdx.x + j * blockDim.x;
+      rh[j] = (q < nzb * N) ? Sr[q] : 0.0;
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
+      fence_proxy_async();
+      issue(t + gridDim.x);
+    }
+    F::template nat2perm<+1>(W, 4 * ZB, LD, d.twx);
+
+    double r0[PT], r1[PT], r2[PT], rs = 0.0, mv = 0.0;
+#pragma unroll
+    for (int j = 0; j < PT; j++) {
+      const int q = threadIdx.x + j * blockDim.x;
+      r0[j] = r1[j] = r2[j] = 0.0;
+      if (q < nzb * N) {
+        const int l = q / N, pos = q - l * N;
+        double2 *c0 = W + (size_t)l * LD + F::sk(pos);
+        double2 *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
+        const double2 p0 = *c0, p1 = *c1, p2 = *c2, p3 = *c3;
+        const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
+        const double rhp = rh[j];
+        const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
+        double tn = T + dtxi * rhp;                                      // cross.f:1626
+        double d8 = dtxi * rhp;                                          // cross.f:1627
+        const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
+        d.rhst[((size_t)y * d.mgalz + z0 + l) * N + pos] = rhs;
+        tn = tn + dtg * rhs;                                             // cross.f:1641
+        d8 = d8 + dtg * rhs;                                             // cross.f:1642
+        *c0 = make_double2(u, v);
+        *c1 = make_double2(w, ru * u);                                   // cross.f:1655-1666
+        *c2 = make_double2(rv * v, rw * w);
+        *c3 = make_double2(ru * v, ru * w);
+        r0[j] = rv * w;
+        r1[j] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);              // cross.f:1670-1671
+        r2[j] = d8;                                                      // cross.f:1645-1647
+        if (do_cfl) {
+          mu = fmax(mu, fabs(u));
+          mv = fmax(mv, fabs(v));
+          mw = fmax(mw, fabs(w));
+          atomic_max_pos(&s_tmax[l], fmax(T, 0.0));
+        }
+        if (do_diag) rs += 1.0 / T;
+      }
+    }
+    if (do_diag) {
+      rs = warp_sum(rs);
+      if ((threadIdx.x & 31) == 0) atomicAdd(d.rhom + y, rs);
+    }
+    if (do_cfl) {
+      mv = warp_max(mv);
+      if ((threadIdx.x & 31) == 0) atomic_max_pos(&s_vmax, mv);
+    }
+    __syncthreads();
+    if (do_cfl && threadIdx.x == 0) {  // cross.f:1690-1708 for the lines of this tile
+      const double hy = d.hy[y];
+      cfy = fmax(cfy, __longlong_as_double((long long)s_vmax) / hy);
+      for (int l = 0; l < nzb; l++) {
+        const double DD = ipe * __longlong_as_double((long long)s_tmax[l]);  // cross.f:1704
+        cft = fmax(cft, 2.0 * DD * ((d.hxalp / 2) * (d.hxalp / 2) + (d.hzbet / 2) * (d.hzbet / 2) + (1.0 / hy) * (1.0 / hy)));
+        s_tmax[l] = 0ull;
+      }
+      s_vmax = 0ull;
+    }
+    F::template perm2nat<-1>(W, 4 * ZB, LD, d.twx);
+    x_extract<N1, N2>(d, W, 0, OU, OV, y, z0, nzb);
+    x_extract<N1, N2>(d, W, 1, OW, ORUU, y, z0, nzb);
+    x_extract<N1, N2>(d, W, 2, ORVV, ORWW, y, z0, nzb);
+    x_extract<N1, N2>(d, W, 3, ORUV, ORUW, y, z0, nzb);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PT; j++) {
+      const int q = threadIdx.x + j * blockDim.x;
+      if (q < ZB * N) {
+        const int l = q / N, pos = q - l * N;
+        double2 *c0 = W + (size_t)l * LD + F::sk(pos);
+        c0[0] = make_double2(r0[j], r1[j]);
+        c0[(size_t)ZB * LD] = make_double2(r2[j], 0.0);
+      }
+    }
+    __syncthreads();
+    F::template perm2nat<-1>(W, 2 * ZB, LD, d.twx);
+    x_extract<N1, N2>(d, W, 0, ORVW, ODRHO, y, z0, nzb);
+    x_extract<N1, N2>(d, W, 1, ODT, -1, y, z0, nzb);
+    __syncthreads();
   }
-  __syncthreads();
-  F::template perm2nat<-1>(sm, 2 * ZB, LD, d.twx);
-  x_extract<N1, N2>(d, sm, 0, ORVW, ODRHO, y, z0, nzb);
-  x_extract<N1, N2>(d, sm, 1, ODT, -1, y, z0, nzb);
-  if (do_cfl || do_diag) {
-    mu = warp_max(mu); mv = warp_max(mv); mw = warp_max(mw); rs = warp_sum(rs);
+  if (do_cfl) {
+    mu = warp_max(mu);
+    mw = warp_max(mw);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) { s_red[0][wid] = mu; s_red[1][wid] = mv; s_red[2][wid] = mw; s_red[3][wid] = rs; }
+    if (lane == 0) { s_red[0][wid] = mu; s_red[1][wid] = mw; }
     __syncthreads();
     if (threadIdx.x == 0) {
-      const int nw = blockDim.x >> 5;
-      double a = 0, b = 0, c = 0, r = 0;
-      for (int q = 0; q < nw; q++) {
-        a = fmax(a, s_red[0][q]); b = fmax(b, s_red[1][q]); c = fmax(c, s_red[2][q]); r += s_red[3][q];
-      }
-      if (do_cfl) {
-        const double hy = d.hy[y];
-        double ct = 0.0;
-        for (int l = 0; l < nzb; l++) {
-          const double DD = ipe * __longlong_as_double((long long)s_tmax[l]);  // cross.f:1704
-          ct = fmax(ct, 2.0 * DD * ((d.hxalp / 2) * (d.hxalp / 2) + (d.hzbet / 2) * (d.hzbet / 2) + (1.0 / hy) * (1.0 / hy)));
-        }
-        atomic_max_pos(d.cflmax + 0, a);
-        atomic_max_pos(d.cflmax + 1, b / hy);
-        atomic_max_pos(d.cflmax + 2, c);
-        atomic_max_pos(d.cflmax + 3, ct);
-      }
-      if (do_diag) atomicAdd(d.rhom + y, r);
+      double a = 0, c = 0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a = fmax(a, s_red[0][q]); c = fmax(c, s_red[1][q]); }
+      atomic_max_pos(d.cflmax + 0, a);
+      atomic_max_pos(d.cflmax + 1, cfy);
+      atomic_max_pos(d.cflmax + 2, c);
+      atomic_max_pos(d.cflmax + 3, cft);
     }
   }
 }
@@ -265,18 +353,36 @@ template <int N1, int N2>
 struct Launch {
   using G = Geo<N1, N2>;
   static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(double2); }
+  static size_t zinv_sm(int mz) { return zsm() + (size_t)G::KB * mz * sizeof(double2); }
   static size_t xsm() { return (size_t)4 * G::ZB * G::LD * sizeof(double2); }
+  static size_t xphys_sm(int nkx) {
+    return xsm() + (size_t)8 * G::ZB * nkx * sizeof(double2) + (size_t)G::ZB * G::N * sizeof(double);
+  }
+  // resident blocks per SM x SMs, for the persistent kernels
+  static int grid_for(const void *fn, int threads, size_t smem, int ntiles) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+    if (per < 1) per = 1;
+    const int g = sms * per;
+    return g < ntiles ? g : ntiles;
+  }
   static void zinv(const Dev &d, cudaStream_t s) {
-    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 8);
-    k_zinv<N1, N2><<<g, G::ZT, zsm(), s>>>(d);
+    const int ntiles = 8 * d.my * ((d.nkx + G::KB - 1) / G::KB);
+    const size_t sm = zinv_sm(d.mz);
+    const int g = grid_for((const void *)k_zinv<N1, N2>, G::ZT, sm, ntiles);
+    k_zinv<N1, N2><<<g, G::ZT, sm, s>>>(d, ntiles);
   }
   static void zfwd(const Dev &d, cudaStream_t s) {
     dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 11);
     k_zfwd<N1, N2><<<g, G::ZT, zsm(), s>>>(d);
   }
   static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
-    dim3 g((d.mgalz + G::ZB - 1) / G::ZB, d.my);
-    k_xphys<N1, N2><<<g, G::XT, xsm(), s>>>(d, rk, do_cfl, do_diag);
+    const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
+    const size_t sm = xphys_sm(d.nkx);
+    const int g = grid_for((const void *)k_xphys<N1, N2>, G::XT, sm, ntiles);
+    k_xphys<N1, N2><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
   }
   static cudaError_t optin(int limit) {
     cudaError_t e;
@@ -315,8 +421,8 @@ inline cudaError_t upload_twiddles() {
   case N: Launch<N1, N2>::xphys(d, rk, do_cfl, do_diag, s); return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
-#define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2>::zsm();
-#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2>::xsm();
+#define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2>::zinv_sm(2 * (N / 3));
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2>::xphys_sm(N / 3);
 #define LMC_FFT_CASE_OPT(N, N1, N2) \
   if ((e = Launch<N1, N2>::optin(limit)) != cudaSuccess) return e;
 #define LMC_FFT_CASE_HAS(N, N1, N2) case N: return true;
