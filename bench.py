@@ -43,6 +43,7 @@ sys.path.insert(0, ROOT)
 #   tder : T read; T, dT/dy, lap T written
 #   post1: T, DT, rho vv, rho uv, rho vw, rho uu, rho uw, rho ww read; T, N_x, N_y, N_z written
 #   post2: u, v, w, N_x, N_y, N_z, vor, phi read; R_om, R_phi, vor, phi written
+#          (two launches, post2a and post2b, counted together as one stage)
 #   psi  : drho read, psi written (+ 7 doubles/point mode tables read)
 ALGO = {
     "zinv": lambda S, Z, P, w: 6 * S * w + 8 * Z * w,
@@ -55,8 +56,18 @@ ALGO = {
     "post2": lambda S, Z, P, w: 12 * S * w,
     "psi": lambda S, Z, P, w: 2 * S * w + S * 7 * 8 // 2,
 }
-# Kernel launches per RK3 step (3 substeps x 9 kernels).
-LAUNCHES_PER_STEP = 27
+# DRAM bytes (read + write) per launch measured by ncu on the 256x65x256 case
+# of this workload (profiles/kernels_lomacte_fp64_256x65x256.md).  Traffic
+# grows in proportion to ny at fixed x/z sizes, so for nx = nz = 256 it is
+# scaled by ny/65; other sizes report null.
+NCU_TRAFFIC_256x65 = {
+    "lapv": 226.3e6, "assemble": 368.4e6, "tder": 79.9e6, "zinv": 603.6e6, "xphys": 1064.6e6,
+    "zfwd": 900.8e6, "post1": 368.6e6, "post2": 469.6e6, "psi": 265.6e6,
+}
+
+# Kernel launches per RK3 step: 3 substeps x 10 kernels (lapv, assemble,
+# tder, zinv, xphys, zfwd, post1, post2a, post2b, psi).
+LAUNCHES_PER_STEP = 30
 
 
 def parse():
@@ -301,8 +312,13 @@ def main():
     peak, kind = peaks()
     achieved = algo / avg_s / 1e9
     share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES}
+    traffic = None
+    if a.nx == 256 and a.nz == 256 and top in NCU_TRAFFIC_256x65:
+        traffic = NCU_TRAFFIC_256x65[top] * a.ny / 65.0
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at "
+                                  "256x65x256, scaled by ny/65" if traffic else None,
                 "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
