@@ -2,12 +2,15 @@
 """Benchmark of the lomacte RK3 step on B200 (Mpts.RK3-steps/s).
 
 Workload (default): nx = nz = 256 Fourier modes (3/2 dealiased: mgalx =
-mgalz = 384), ny = 257 on y = 12 sinh(2 eta)/sinh(2), FP64 plain path,
-seeded initial condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed
-Deltat = 0.01.  One "step" = one full RK3 step (3 substeps).  The metric is
-(nx*ny*nz/1e6) * steps / seconds.
+mgalz = 384), ny = 257 on y = 12 sinh(2 eta)/sinh(2), seeded initial
+condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed Deltat = 0.01.
+One "step" = one full RK3 step (3 substeps).  The metric is
+(nx*ny*nz/1e6) * steps / seconds, measured for the mixed-precision form
+(the headline value) and the FP64 plain path (reported beside it, with the
+ratio and the relative L2 difference of the two final states).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision both|mixed|fp64]
 
 N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
 time is the max over ranks and the value the aggregate over ranks.
@@ -33,14 +36,16 @@ sys.path.insert(0, ROOT)
 
 # Algorithmic HBM bytes per launch, in units of the spectral (S = nplanes *
 # mz * ny complex), z-padded (Z = nplanes * mgalz * ny complex) and physical
-# (P = mgalx * mgalz * ny real) counts; w = bytes per complex value (16 in
-# FP64).  Compulsory reads + writes of each kernel:
-#   zinv : 6 spectral fields read (rho u, rho v, rho w, lap T, dT/dy, T), 8 Z written
-#   xphys: 8 Z read, 11 Z written, RHS(T) physical accumulator read + written
+# (P = mgalx * mgalz * ny real) counts.  State fields (Omega_y, phi, psi, T,
+# R_Omega, R_phi) are FP64 complex (16 B) in both forms; transform work
+# buffers take w bytes per complex value (16 in the FP64 form, 8 in the mixed
+# form).  Compulsory reads + writes of each kernel:
+#   zinv : 6 spectral inputs read (rho u, rho v, rho w, lap T, dT/dy, T), 8 Z written
+#   xphys: 8 Z read, 11 Z written, RHS(T) physical accumulator (FP64) read + written
 #   zfwd : 11 Z read, 11 S written
 #   lapv : phi read, m_y and dm_y/dy written (+ 7 doubles/point mode tables read)
-#   assemble: vor, dm_y, psi, m_y, R_om, phi, R_phi read; rho u, rho v, rho w, vor, phi written
-#   tder : T read; T, dT/dy, lap T written
+#   assemble: vor, psi, R_om, phi, R_phi, m_y, dm_y read; rho u, rho v, rho w, vor, phi written
+#   tder : T read and written; dT/dy, lap T written
 #   post1: T, DT, rho vv, rho uv, rho vw, rho uu, rho uw, rho ww read; T, N_x, N_y, N_z written
 #   post2: u, v, w, N_x, N_y, N_z, vor, phi read; R_om, R_phi, vor, phi written
 #          (two launches, post2a and post2b, counted together as one stage)
@@ -49,13 +54,14 @@ ALGO = {
     "zinv": lambda S, Z, P, w: 6 * S * w + 8 * Z * w,
     "xphys": lambda S, Z, P, w: 19 * Z * w + 2 * P * 8,
     "zfwd": lambda S, Z, P, w: 11 * Z * w + 11 * S * w,
-    "lapv": lambda S, Z, P, w: 3 * S * w + S * 7 * 8 // 2,
-    "assemble": lambda S, Z, P, w: 12 * S * w,
-    "tder": lambda S, Z, P, w: 4 * S * w,
-    "post1": lambda S, Z, P, w: 12 * S * w,
-    "post2": lambda S, Z, P, w: 12 * S * w,
-    "psi": lambda S, Z, P, w: 2 * S * w + S * 7 * 8 // 2,
+    "lapv": lambda S, Z, P, w: S * 16 + 2 * S * w + S * 7 * 8 // 2,
+    "assemble": lambda S, Z, P, w: 7 * S * 16 + 5 * S * w,
+    "tder": lambda S, Z, P, w: 2 * S * 16 + 2 * S * w,
+    "post1": lambda S, Z, P, w: 2 * S * 16 + 10 * S * w,
+    "post2": lambda S, Z, P, w: 6 * S * 16 + 6 * S * w,
+    "psi": lambda S, Z, P, w: S * 16 + S * w + S * 7 * 8 // 2,
 }
+
 # DRAM bytes (read + write) per launch measured by ncu on the 256x65x256 case
 # of this workload (profiles/kernels_lomacte_fp64_256x65x256.md).  Traffic
 # grows in proportion to ny at fixed x/z sizes, so for nx = nz = 256 it is
@@ -64,6 +70,12 @@ NCU_TRAFFIC_256x65 = {
     "lapv": 226.3e6, "assemble": 368.4e6, "tder": 79.9e6, "zinv": 603.6e6, "xphys": 1064.6e6,
     "zfwd": 900.8e6, "post1": 368.6e6, "post2": 469.6e6, "psi": 265.6e6,
 }
+
+# The same for the mixed form (not captured yet: null).
+NCU_TRAFFIC_MIXED_256x65 = {}
+
+MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
+               2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
 
 # Kernel launches per RK3 step: 3 substeps x 10 kernels (lapv, assemble,
 # tder, zinv, xphys, zfwd, post1, post2a, post2b, psi).
@@ -79,6 +91,10 @@ def parse():
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--nz", type=int, default=256)
     ap.add_argument("--ny", type=int, default=257)
+    ap.add_argument("--precision", default="both", choices=("both", "mixed", "fp64"),
+                    help="both: time the FP64 and the mixed form; the headline value is the mixed form")
+    ap.add_argument("--mixed-form", type=int, default=1, choices=(1, 2),
+                    help="1: FP32 FFT arithmetic; 2: FP64 FFT arithmetic on FP32 storage")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
@@ -211,28 +227,14 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    a = parse()
-    if a.impl == "reference":
-        run_reference(a)
-        return
+def run_arm(a, prec, dev, rank, world, dist, want_e2e):
+    """Warm up, time K steps of one form (prec 0: FP64, 1: mixed) with CUDA
+    events, then optionally the end-to-end loop through the public API."""
     import torch
     from loma_phd_b200 import ICParams, Lomacte, Params, make_ic, stretched_mesh
     from loma_phd_b200.lomacte import KERNEL_NAMES
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = local if world > 1 else 0
-    torch.cuda.set_device(dev)
-
-    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev)
+    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec)
     y = stretched_mesh(p.my)
     st = make_ic(p, y, ICParams(s=4.0, seed=rank))
     g = Lomacte(p, y)
@@ -265,18 +267,18 @@ def main():
         t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    secs = ms / 1e3
-    value = mpts(a) * a.steps * world / secs
+    value = mpts(a) * a.steps * world / (ms / 1e3)
     diag = g.diag()
     if not np.isfinite(diag["dm"]):
         raise RuntimeError("non-finite diagnostics after the timed steps")
+    state = g.get_state()
 
     # end-to-end through the public API with host buffers: every step loads
     # the state from pinned host memory, advances one RK3 step and reads the
     # state back.
     e2e = None
-    if not a.no_e2e:
-        S, Z, P = sizes(p)
+    S, Z, P = sizes(p)
+    if want_e2e:
         host = {k: torch.from_numpy(np.ascontiguousarray(st[k]).view(np.float64).copy()).pin_memory()
                 for k in ("vor", "phi", "psi", "scal")}
         h00 = {k: torch.from_numpy(np.ascontiguousarray(st[k], dtype=np.float64).copy()).pin_memory()
@@ -302,42 +304,93 @@ def main():
         nbytes = 4 * S * 16 + 3 * p.my * 8
         e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
+    g.close()
 
     # roofline of the dominant kernel, live CUDA-event times of the timed region
-    S, Z, P = sizes(p)
+    w = 16 if prec == 0 else 8
     top = max((k for k in KERNEL_NAMES if k in ALGO), key=lambda k: prof[k][0])
     tot_ms, cnt = prof[top]
     avg_s = tot_ms / max(cnt, 1) / 1e3
-    algo = ALGO[top](S, Z, P, 16)
+    algo = ALGO[top](S, Z, P, w)
     peak, kind = peaks()
     achieved = algo / avg_s / 1e9
     share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES}
     traffic = None
-    if a.nx == 256 and a.nz == 256 and top in NCU_TRAFFIC_256x65:
-        traffic = NCU_TRAFFIC_256x65[top] * a.ny / 65.0
+    table = NCU_TRAFFIC_256x65 if prec == 0 else NCU_TRAFFIC_MIXED_256x65
+    if a.nx == 256 and a.nz == 256 and top in table:
+        traffic = table[top] * a.ny / 65.0
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at "
                                   "256x65x256, scaled by ny/65" if traffic else None,
                 "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
+    step_bytes = 3 * sum(f(S, Z, P, w) for f in ALGO.values())
+    return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
+            "kernel_share": share, "e2e": e2e, "state": state, "diag": diag, "step_bytes": step_bytes,
+            "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    forms = {"mixed": [1], "fp64": [0], "both": [0, 1]}[a.precision]
+    arms = {prec: run_arm(a, a.mixed_form if prec else 0, dev, rank, world, dist, not a.no_e2e) for prec in forms}
+    head = arms[1] if 1 in arms else arms[0]
+    errs = None
+    if 0 in arms and 1 in arms:
+        # same seeded state advanced warmup + steps + e2e steps by both forms
+        errs = {}
+        ref = arms[0]["state"]
+        for k in ("vor", "phi", "psi", "scal", "u00", "v00", "w00"):
+            den = np.linalg.norm(ref[k])
+            if k in ("v00", "w00"):  # measured against the size of u00
+                den = max(den, np.linalg.norm(ref["u00"]))
+            errs[k] = float(np.linalg.norm(np.asarray(arms[1]["state"][k]) - np.asarray(ref[k])) / den)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a, p, y, st)
-    g.close()
+        cpu = cpu_baseline(a, head["p"], head["y"], head["st"])
     if rank == 0:
+        p = head["p"]
+        mixed = 1 in arms
         line = {
-            "metric": "Mpts*RK3-steps/s", "value": value, "unit": "Mpts*RK3-steps/s",
-            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "metric": "Mpts*RK3-steps/s", "value": head["value"], "unit": "Mpts*RK3-steps/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["ms"] / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed f32/f64" if mixed else "f64",
+            "precision_form": a.mixed_form if mixed else 0,
             "data": "synthetic (seeded initial condition)",
-            "config": {"workload": f"lomacte FP64 plain path {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), "
-                                   f"s=4, Re=160, dt=0.01", "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (
-                           3 * sum(f(S, Z, P, 16) for f in ALGO.values()) / 1e9)},
+            "config": {"workload": f"lomacte {MIXED_NAMES[a.mixed_form] if mixed else 'FP64 plain path'} "
+                                   f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},
             "gpu_launches": LAUNCHES_PER_STEP * a.steps,
-            "clocks": ck, "roofline": roofline, "kernel_share": share,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
+            "step_roofline_frac": head["step_roofline_frac"],
+            "e2e": head["e2e"], "cpu_baseline": cpu,
         }
+        if mixed and 0 in arms:
+            f64 = arms[0]
+            line["fp64"] = {"value": f64["value"], "ms_per_step": f64["ms"] / a.steps, "roofline": f64["roofline"],
+                            "kernel_share": f64["kernel_share"], "e2e": f64["e2e"], "clocks": f64["clocks"]}
+            line["mixed_over_fp64"] = head["value"] / f64["value"]
+            line["error_vs_fp64"] = {"rel_l2": errs, "steps": a.warmup + a.steps,
+                                     "note": "mixed vs FP64 GPU path from the same seeded state"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

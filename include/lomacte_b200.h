@@ -44,7 +44,11 @@ typedef struct lmc_params {
   int ncfl;             /* steps between CFL updates (main.f:564) */
   int dt_mode;          /* 0: reference CFL mode, 1: fixed Deltat */
   double dt;            /* initial Deltat (reference: 1e-4, main.f:559) or the fixed Deltat */
-  int precision;        /* 0: FP64 (the plain path) */
+  int precision;        /* 0: FP64 (the plain path)
+                           1: mixed: FP32 work buffers and FP32 FFTs; FP64
+                              state, RK3 accumulators, y solves, 00 modes
+                              and pointwise EOS / d(rho)/dt math
+                           2: as 1 with FP64 FFT arithmetic (FP32 storage) */
   int device;           /* CUDA device ordinal */
 } lmc_params;
 

@@ -26,6 +26,9 @@ struct lmc_handle {
   std::vector<void *> allocs;
   int steps = 0;
   int err = 0;
+  // mixed form: the two FP64 plane-sum arrays alternate between substeps
+  double *mo[2] = {nullptr, nullptr};
+  int mo_flip = 0;
   // per-kernel CUDA-event profiling (lmc_profile_start / lmc_profile_read)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -68,6 +71,15 @@ std::vector<double2> twiddles(int n) {
   for (int k = 0; k < n; k++) {
     const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
     t[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+  }
+  return t;
+}
+
+std::vector<float2> twiddles_f32(int n) {
+  std::vector<float2> t(n);
+  for (int k = 0; k < n; k++) {
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+    t[k] = make_float2((float)cosl(a), (float)(-sinl(a)));
   }
   return t;
 }
@@ -121,9 +133,10 @@ int do_load(lmc_handle *h, const double *vor, const double *phi, const double *p
   // reference layout [kx][kz][y] -> device layout [y][kx][kz]
   const double *src[4] = {vor, phi, psi, scal};
   double2 *dst[4] = {d.vor, d.phi, d.psi, d.scal};
-  for (int f = 0; f < 4; f++) {
-    LMC_CK(cudaMemcpyAsync(d.sb[f], src[f], ns, cudaMemcpyHostToDevice, h->s));
-    lmc::launch_ref2dev(d, d.sb[f], dst[f], h->s);
+  for (int f = 0; f < 4; f++) {  // staged through the FP64 buffers 7..9
+    double2 *stage = d.sb[7 + f % 3];
+    LMC_CK(cudaMemcpyAsync(stage, src[f], ns, cudaMemcpyHostToDevice, h->s));
+    lmc::launch_ref2dev(d, stage, dst[f], h->s);
   }
   LMC_CK(cudaMemsetAsync(d.Rom, 0, ns, h->s));
   LMC_CK(cudaMemsetAsync(d.Rphi, 0, ns, h->s));
@@ -145,6 +158,7 @@ int do_load(lmc_handle *h, const double *vor, const double *phi, const double *p
   LMC_CK(cudaStreamSynchronize(h->s));
   h->steps = 0;
   h->err = 0;
+  h->d.mean_ok = 0;  // no plane sums of a previous substep yet
   return LMC_OK;
 }
 
@@ -174,13 +188,14 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     return LMC_ENODEV;
   }
   if (p->device < 0 || p->device >= ndev) return LMC_EINVAL;
-  if (p->precision != 0) return LMC_EINVAL;
+  if (p->precision < 0 || p->precision > 2) return LMC_EINVAL;
   lmc_handle *h = new (std::nothrow) lmc_handle();
   if (!h) return LMC_ENOMEM;
   h->p = *p;
   h->g.set(p->mgalx, p->mgalz, p->my);
   lmc::Dev &d = h->d;
   std::memset(&d, 0, sizeof(d));
+  d.prec = p->precision;
   const lmc::Grid &g = h->g;
   int rc = LMC_OK;
   if (g.nkx < 1 || g.mz < 1 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) rc = LMC_EINVAL;
@@ -250,13 +265,38 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     }
     d.twx = tx;
     d.twz = tz;
+    if (d.prec == 1) {
+      const float2 *fx = nullptr, *fz = nullptr;
+      if ((rc = dupload(h, &fx, twiddles_f32(g.mgalx))) || (rc = dupload(h, &fz, twiddles_f32(g.mgalz)))) {
+        lmc_destroy(h);
+        return rc;
+      }
+      d.twxf = fx;
+      d.twzf = fz;
+    }
   }
   const size_t ns = (size_t)g.nmode * g.my, nzp = (size_t)g.nkx * g.my * g.mgalz;
   double2 **spec[] = {&d.vor, &d.phi, &d.psi, &d.scal, &d.Rom, &d.Rphi};
   for (auto q : spec)
     if ((rc = dalloc(h, q, ns))) { lmc_destroy(h); return rc; }
-  for (int f = 0; f < 11; f++)
-    if ((rc = dalloc(h, &d.sb[f], ns)) || (rc = dalloc(h, &d.zb[f], nzp))) { lmc_destroy(h); return rc; }
+  // work buffers: FP64 in the plain form; FP32 in the mixed form, which
+  // keeps three FP64 spectral buffers for the ABI transposes and lmc_op_y
+  for (int f = 0; f < 11; f++) {
+    if (!d.prec || (f >= 7 && f <= 9))
+      if ((rc = dalloc(h, &d.sb[f], ns))) { lmc_destroy(h); return rc; }
+    if (!d.prec) {
+      if ((rc = dalloc(h, &d.zb[f], nzp))) { lmc_destroy(h); return rc; }
+    } else {
+      if ((rc = dalloc(h, &d.sbf[f], ns)) || (rc = dalloc(h, &d.zbf[f], nzp))) { lmc_destroy(h); return rc; }
+    }
+  }
+  if (d.prec) {
+    if ((rc = dalloc(h, &d.mi, (size_t)6 * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)11 * g.my)) ||
+        (rc = dalloc(h, &h->mo[1], (size_t)11 * g.my))) {
+      lmc_destroy(h);
+      return rc;
+    }
+  }
   double **vec[] = {&d.u00, &d.v00, &d.w00, &d.rf0u, &d.rf0w, &d.rf0v, &d.rhom};
   for (auto q : vec)
     if ((rc = dalloc(h, q, (size_t)g.my))) { lmc_destroy(h); return rc; }
@@ -321,8 +361,9 @@ int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi, doub
   const double2 *srcd[4] = {d.vor, d.phi, d.psi, d.scal};
   for (int f = 0; f < 4; f++)
     if (dsth[f]) {
-      lmc::launch_dev2ref(d, srcd[f], d.sb[f], h->s);
-      LMC_CK(cudaMemcpyAsync(dsth[f], d.sb[f], ns, cudaMemcpyDeviceToHost, h->s));
+      double2 *stage = d.sb[7 + f % 3];
+      lmc::launch_dev2ref(d, srcd[f], stage, h->s);
+      LMC_CK(cudaMemcpyAsync(dsth[f], stage, ns, cudaMemcpyDeviceToHost, h->s));
     }
   if (u00) LMC_CK(cudaMemcpyAsync(u00, d.u00, ny, cudaMemcpyDeviceToHost, h->s));
   if (v00) LMC_CK(cudaMemcpyAsync(v00, d.v00, ny, cudaMemcpyDeviceToHost, h->s));
@@ -355,12 +396,18 @@ int lmc_step(lmc_handle *h, int nsteps) {
   if (!h || nsteps < 0) return LMC_EINVAL;
   if (h->err) return h->err;
   LMC_CK(cudaSetDevice(h->p.device));
-  const lmc::Dev &d = h->d;
+  lmc::Dev &d = h->d;
   cudaStream_t s = h->s;
   const int ncfl = h->p.ncfl > 0 ? h->p.ncfl : 1;
   for (int n = 0; n < nsteps; n++) {
     const int cfl_step = (h->p.dt_mode == 0) && (h->steps % ncfl == 0);  // cross.f:240
     for (int rk = 0; rk < 3; rk++) {
+      if (d.prec) {  // this substep's plane sums, and the previous ones
+        d.mo_cur = h->mo[h->mo_flip];
+        d.mo_prev = h->mo[1 - h->mo_flip];
+        prof_mark(h, 9);
+        LMC_CK(cudaMemsetAsync(d.mo_cur, 0, (size_t)11 * d.my * sizeof(double), s));
+      }
       prof_mark(h, 0);
       lmc::launch_lapv(d, s);
       prof_mark(h, 1);
@@ -386,6 +433,10 @@ int lmc_step(lmc_handle *h, int nsteps) {
       prof_mark(h, 8);
       lmc::launch_psi(d, rk, cfl_step, 1, s);
       prof_mark(h, -1);
+      if (d.prec) {
+        d.mean_ok = 1;
+        h->mo_flip = 1 - h->mo_flip;
+      }
     }
     h->steps++;
     if (check_launch(h)) return LMC_ECUDA;

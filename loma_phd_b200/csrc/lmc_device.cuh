@@ -35,6 +35,39 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 czero() { return make_double2(0.0, 0.0); }
 
+// The same operations on single-precision complex values (the transform
+// work buffers of the mixed-precision form).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__device__ __forceinline__ float2 cik(float k, float2 a) { return make_float2(-k * a.y, k * a.x); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// real type and constructors of a complex type
+template <typename CT>
+struct CReal;
+template <>
+struct CReal<double2> { using R = double; };
+template <>
+struct CReal<float2> { using R = float; };
+template <typename CT>
+__device__ __forceinline__ CT cmk(typename CReal<CT>::R a, typename CReal<CT>::R b) {
+  CT c;
+  c.x = a;
+  c.y = b;
+  return c;
+}
+template <typename CT>
+__device__ __forceinline__ CT cz() { return cmk<CT>(0, 0); }
+// FP64 value of a stored work-buffer element and back
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2(a.x, a.y); }
+template <typename CT>
+__device__ __forceinline__ CT from_d2(double2 a) { return cmk<CT>((typename CReal<CT>::R)a.x, (typename CReal<CT>::R)a.y); }
+
 __device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
   return make_double2(__shfl_up_sync(LMC_FULL, v.x, d), __shfl_up_sync(LMC_FULL, v.y, d));
 }
@@ -401,43 +434,47 @@ __host__ __device__ constexpr int tw_off(int R) {
 constexpr int TW_TOTAL = 4 + 6 + 8 + 9 + 12 + 16 + 18 + 24 + 32 + 36;
 
 static __constant__ double2 c_tw[TW_TOTAL];  // one copy per translation unit
+static __constant__ float2 c_twf[TW_TOTAL];  // the same, rounded to FP32
 
-template <int R, int SIGN>
-__device__ __forceinline__ double2 ctw(int e) {
+template <int R, int SIGN, typename CT>
+__device__ __forceinline__ CT ctw(int e) {
   constexpr int o = tw_off(R);
   static_assert(o >= 0, "register DFT size without twiddles");
-  const double2 w = c_tw[o + e];
+  CT w;
+  if constexpr (sizeof(CT) == sizeof(double2)) w = c_tw[o + e];
+  else w = c_twf[o + e];
   return SIGN > 0 ? cconj(w) : w;
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void bfly(double2 (&x)[R]) {
+template <int R, int SIGN, typename CT>
+__device__ __forceinline__ void bfly(CT (&x)[R]) {
+  using Re = typename CReal<CT>::R;
   if constexpr (R == 2) {
-    const double2 a = x[0], b = x[1];
+    const CT a = x[0], b = x[1];
     x[0] = cadd(a, b);
     x[1] = csub(a, b);
   } else if constexpr (R == 4) {
-    const double2 t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
-    const double2 d = csub(x[1], x[3]);
-    const double2 t3 = (SIGN > 0) ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);  // d * (SIGN i)
+    const CT t0 = cadd(x[0], x[2]), t1 = csub(x[0], x[2]), t2 = cadd(x[1], x[3]);
+    const CT d = csub(x[1], x[3]);
+    const CT t3 = (SIGN > 0) ? cmk<CT>(-d.y, d.x) : cmk<CT>(d.y, -d.x);  // d * (SIGN i)
     x[0] = cadd(t0, t2);
     x[2] = csub(t0, t2);
     x[1] = cadd(t1, t3);
     x[3] = csub(t1, t3);
   } else if constexpr (R == 3) {
-    const double s3 = 0.86602540378443864676;  // sqrt(3)/2
-    const double2 t = cadd(x[1], x[2]);
-    const double2 d = csub(x[1], x[2]);
-    const double2 u = (SIGN > 0) ? make_double2(-s3 * d.y, s3 * d.x) : make_double2(s3 * d.y, -s3 * d.x);
-    const double2 a = make_double2(fma(-0.5, t.x, x[0].x), fma(-0.5, t.y, x[0].y));
+    const Re s3 = (Re)0.86602540378443864676;  // sqrt(3)/2
+    const CT t = cadd(x[1], x[2]);
+    const CT d = csub(x[1], x[2]);
+    const CT u = (SIGN > 0) ? cmk<CT>(-s3 * d.y, s3 * d.x) : cmk<CT>(s3 * d.y, -s3 * d.x);
+    const CT a = cmk<CT>(x[0].x - (Re)0.5 * t.x, x[0].y - (Re)0.5 * t.y);
     x[0] = cadd(x[0], t);
     x[1] = cadd(a, u);
     x[2] = csub(a, u);
   }
 }
 
-template <int R, int SIGN>
-__device__ __forceinline__ void rdft(double2 (&x)[R]) {
+template <int R, int SIGN, typename CT>
+__device__ __forceinline__ void rdft(CT (&x)[R]) {
   if constexpr (R == 1) {
     return;
   } else if constexpr (R == 2 || R == 3 || R == 4) {
@@ -445,7 +482,7 @@ __device__ __forceinline__ void rdft(double2 (&x)[R]) {
   } else {
     constexpr int p = (R % 4 == 0) ? 4 : ((R % 2 == 0) ? 2 : 3);
     constexpr int m = R / p;
-    double2 sub[p][m];
+    CT sub[p][m];
 #pragma unroll
     for (int r = 0; r < p; r++)
 #pragma unroll
@@ -454,9 +491,9 @@ __device__ __forceinline__ void rdft(double2 (&x)[R]) {
     for (int r = 0; r < p; r++) rdft<m, SIGN>(sub[r]);
 #pragma unroll
     for (int k = 0; k < m; k++) {
-      double2 t[p];
+      CT t[p];
 #pragma unroll
-      for (int r = 0; r < p; r++) t[r] = (r == 0 || k == 0) ? sub[r][k] : cmul(sub[r][k], ctw<R, SIGN>(r * k));
+      for (int r = 0; r < p; r++) t[r] = (r == 0 || k == 0) ? sub[r][k] : cmul(sub[r][k], ctw<R, SIGN, CT>(r * k));
       bfly<p, SIGN>(t);
 #pragma unroll
       for (int q = 0; q < p; q++) x[k + m * q] = t[q];
@@ -466,8 +503,9 @@ __device__ __forceinline__ void rdft(double2 (&x)[R]) {
 
 // Four-step transform of nb lines of length N = N1*N2 in shared memory.
 // Line b starts at sm + b*ld; natural index n is stored at skew(n) =
-// n + n/N1.  twN[e] = exp(-2 pi i e/N).
-template <int N1, int N2>
+// n + n/N1.  twN[e] = exp(-2 pi i e/N).  CT is the complex type of the
+// samples and of the arithmetic (double2, or float2 in the mixed form).
+template <int N1, int N2, typename CT = double2>
 struct Four {
   static constexpr int N = N1 * N2;
   static constexpr int LD = N2 * (N1 + 1);  // skewed line length
@@ -475,19 +513,19 @@ struct Four {
 
   // natural -> permuted: X[k2 + N2 k1] lands at skew position k1 + N1 k2
   template <int SIGN>
-  __device__ static void nat2perm(double2 *sm, int nb, int ld, const double2 *__restrict__ twN) {
+  __device__ static void nat2perm(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
     for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
       const int b = idx / N1, n1 = idx - b * N1;
-      double2 *p = sm + (size_t)b * ld + n1;
-      double2 x[N2];
+      CT *p = sm + (size_t)b * ld + n1;
+      CT x[N2];
 #pragma unroll
       for (int j = 0; j < N2; j++) x[j] = p[j * (N1 + 1)];
       rdft<N2, SIGN>(x);
 #pragma unroll
       for (int k = 0; k < N2; k++) {
-        double2 v = x[k];
+        CT v = x[k];
         if (k > 0 && n1 > 0) {
-          double2 w = __ldg(twN + n1 * k);
+          CT w = __ldg(twN + n1 * k);
           if (SIGN > 0) w = cconj(w);
           v = cmul(v, w);
         }
@@ -497,8 +535,8 @@ struct Four {
     __syncthreads();
     for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
       const int b = idx / N2, k2 = idx - b * N2;
-      double2 *p = sm + (size_t)b * ld + k2 * (N1 + 1);
-      double2 x[N1];
+      CT *p = sm + (size_t)b * ld + k2 * (N1 + 1);
+      CT x[N1];
 #pragma unroll
       for (int j = 0; j < N1; j++) x[j] = p[j];
       rdft<N1, SIGN>(x);
@@ -510,19 +548,19 @@ struct Four {
 
   // permuted -> natural (transpose of nat2perm)
   template <int SIGN>
-  __device__ static void perm2nat(double2 *sm, int nb, int ld, const double2 *__restrict__ twN) {
+  __device__ static void perm2nat(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
     for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
       const int b = idx / N2, k2 = idx - b * N2;
-      double2 *p = sm + (size_t)b * ld + k2 * (N1 + 1);
-      double2 x[N1];
+      CT *p = sm + (size_t)b * ld + k2 * (N1 + 1);
+      CT x[N1];
 #pragma unroll
       for (int j = 0; j < N1; j++) x[j] = p[j];
       rdft<N1, SIGN>(x);
 #pragma unroll
       for (int j = 0; j < N1; j++) {
-        double2 v = x[j];
+        CT v = x[j];
         if (j > 0 && k2 > 0) {
-          double2 w = __ldg(twN + j * k2);
+          CT w = __ldg(twN + j * k2);
           if (SIGN > 0) w = cconj(w);
           v = cmul(v, w);
         }
@@ -532,8 +570,8 @@ struct Four {
     __syncthreads();
     for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
       const int b = idx / N1, n1 = idx - b * N1;
-      double2 *p = sm + (size_t)b * ld + n1;
-      double2 x[N2];
+      CT *p = sm + (size_t)b * ld + n1;
+      CT x[N2];
 #pragma unroll
       for (int j = 0; j < N2; j++) x[j] = p[j * (N1 + 1)];
       rdft<N2, SIGN>(x);

@@ -1,6 +1,12 @@
-// lmc_fft_impl.cuh -- transform kernels of one lomacte RK3 substep (FP64),
+// lmc_fft_impl.cuh -- transform kernels of one lomacte RK3 substep,
 // templated on the four-step factorisation N = N1*N2 of the transform
-// length.  Included by the lmc_fft_*.cu translation units, each of which
+// length, on the complex type CT of the butterflies (and of the lines in
+// shared memory) and on the complex type ST of the work buffers in HBM:
+//   <double2, double2>  FP64 plain form
+//   <float2,  float2>   mixed form (FP32 transforms)
+//   <double2, float2>   mixed form with FP64 transform arithmetic
+// The pointwise products, the T update and the d(rho)/dt source are FP64
+// in every form.  Included by the lmc_fft_*.cu translation units, each of which
 // instantiates a group of lengths (they compile in parallel).
 //
 //   zinv : localyz2zy + fourz(+1) (fou3D.f:80-145): spectral [y][kx][kz]
@@ -41,38 +47,58 @@ struct Geo {
   static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
 };
 
+__host__ __device__ constexpr size_t round16(size_t b) { return (b + 15) / 16 * 16; }
+template <typename TO, typename FROM>
+__device__ __forceinline__ TO ccvt(FROM a) {
+  return cmk<TO>((typename CReal<TO>::R)a.x, (typename CReal<TO>::R)a.y);
+}
+
 __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ? k : k + (d.mgalz - d.mz); }
 
 // Persistent: each block walks tiles (field, y, kx block) with stride
 // gridDim.x; the next tile's kz rows (one contiguous run of nb*mz complex
 // values in the [y][kx][kz] layout) arrive by a TMA bulk copy while the
-// current tile is transformed.
-template <int N1, int N2>
+// current tile is transformed.  A bulk copy moves whole 16-byte units, so
+// for FP32 values the run is widened to an even start and length and the
+// tile is read from offset `lead` in the staging buffer.
+template <int N1, int N2, typename CT, typename ST>
 __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
-  using F = Four<N1, N2>;
+  using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
+  using Re = typename CReal<CT>::R;
   constexpr int KB = G::KB, LD = G::LD;
-  extern __shared__ double2 sm[];
-  double2 *W = sm, *St = sm + KB * LD;
+  constexpr int E = 16 / (int)sizeof(ST);  // stored values per 16-byte unit
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CT *W = (CT *)smraw;
+  ST *St = (ST *)(smraw + round16(sizeof(CT) * KB * LD));
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
   const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb;
-  auto src_of = [&](int f) -> const double2 * {
+  auto src_of = [&](int f) -> const ST * {
     switch (f) {
-      case 0: return d.sb[SB_RU];
-      case 1: return d.sb[SB_RV];
-      case 2: return d.sb[SB_RW];
-      case 3: return d.sb[SB_LAPT];
-      case 5: return d.sb[SB_DTDY];
-      default: return d.scal;
+      case 0: return wsb<ST>(d, SB_RU);
+      case 1: return wsb<ST>(d, SB_RV);
+      case 2: return wsb<ST>(d, SB_RW);
+      case 3: return wsb<ST>(d, SB_LAPT);
+      case 5: return wsb<ST>(d, SB_DTDY);
+      default:
+        if constexpr (sizeof(ST) == sizeof(double2)) return d.scal;
+        else return wsb<ST>(d, SB_T32);
     }
+  };
+  auto lead_of = [&](int t) {
+    const int r = t % per_f, y = r / nkb, kb = r - y * nkb;
+    return (int)((((size_t)y * d.nkx + kb * KB) * d.mz) % E);
   };
   auto issue = [&](int t) {
     const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
     const int nb = min(KB, d.nkx - kb * KB);
-    const uint32_t bytes = (uint32_t)nb * d.mz * sizeof(double2);
+    const size_t start = ((size_t)y * d.nkx + kb * KB) * d.mz;
+    const int lead = (int)(start % E);
+    const uint32_t cnt = (uint32_t)(((nb * d.mz + lead + E - 1) / E) * E);
+    const uint32_t bytes = cnt * (uint32_t)sizeof(ST);
     mbar_expect_tx(&bar, bytes);
-    bulk_g2s(St, src_of(f) + ((size_t)y * d.nkx + kb * KB) * d.mz, bytes, &bar);
+    bulk_g2s(St, src_of(f) + (start - lead), bytes, &bar);
   };
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
@@ -87,18 +113,21 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
     ph ^= 1;
     const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
     const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
+    const int lead = lead_of(t);
     const int mult = (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
     for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
       const int il = idx / gap, g = idx - il * gap;
-      W[il * LD + F::sk(d.nz1 + 1 + g)] = czero();
+      W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
     }
     for (int il = 0; il < nb; il++) {
-      const double kx = __ldg(d.kx + i0 + il);
-      const double2 *row = St + il * d.mz;
+      const Re kx = (Re)__ldg(d.kx + i0 + il);
+      const ST *row = St + lead + il * d.mz;
       for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
-        double2 v = row[k];
+        CT v = ccvt<CT>(row[k]);
         if (mult == 1) v = cik(kx, v);
-        else if (mult == 2) v = cik(__ldg(d.kz + k), v);
+        else if (mult == 2) v = cik((Re)__ldg(d.kz + k), v);
+        if constexpr (sizeof(ST) == sizeof(float2))
+          if (i0 + il == 0 && k == 0) v = cz<CT>();  // 00 mode: added back in FP64 by xphys
         W[il * LD + F::sk(kz_pad(d, k))] = v;
       }
     }
@@ -107,34 +136,37 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
       fence_proxy_async();
       issue(t + gridDim.x);
     }
-    F::template nat2perm<+1>(W, nb, LD, d.twz);
-    double2 *dst = d.zb[f] + (size_t)y * F::N * d.nkx + i0;
+    F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
+    ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.nkx + i0;
     for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
       const int z = idx / KB, il = idx - z * KB;
-      if (il < nb) dst[(size_t)z * d.nkx + il] = W[il * LD + F::sk(z)];
+      if (il < nb) dst[(size_t)z * d.nkx + il] = ccvt<ST>(W[il * LD + F::sk(z)]);
     }
     __syncthreads();
   }
 }
 
-template <int N1, int N2>
+template <int N1, int N2, typename CT, typename ST>
 __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zfwd(Dev d) {
-  using F = Four<N1, N2>;
+  using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
-  extern __shared__ double2 sm[];
+  using Re = typename CReal<CT>::R;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CT *sm = (CT *)smraw;
   const int f = blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
   const int nb = min(G::KB, d.nkx - i0);
-  const double2 *src = d.zb[f] + (size_t)y * N1 * N2 * d.nkx + i0;
+  const ST *src = wzb<ST>(d, f) + (size_t)y * N1 * N2 * d.nkx + i0;
   for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
     const int z = idx / G::KB, il = idx - z * G::KB;
-    if (il < nb) sm[il * G::LD + F::sk(z)] = __ldg(src + (size_t)z * d.nkx + il);
+    if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.nkx + il));
   }
   __syncthreads();
-  F::template perm2nat<-1>(sm, nb, G::LD, d.twz);
-  const double dn = 1.0 / (double)F::N;
+  F::template perm2nat<-1>(sm, nb, G::LD, wtwz<CT>(d));
+  const Re dn = (Re)(1.0 / (double)F::N);
   for (int il = 0; il < nb; il++) {
-    double2 *row = d.sb[f] + ((size_t)y * d.nkx + i0 + il) * d.mz;
-    for (int k = threadIdx.x; k < d.mz; k += blockDim.x) row[k] = cscale(dn, sm[il * G::LD + F::sk(kz_pad(d, k))]);
+    ST *row = wsb<ST>(d, f) + ((size_t)y * d.nkx + i0 + il) * d.mz;
+    for (int k = threadIdx.x; k < d.mz; k += blockDim.x)
+      row[k] = ccvt<ST>(cscale(dn, sm[il * G::LD + F::sk(kz_pad(d, k))]));
   }
 }
 
@@ -146,31 +178,32 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) 
 //   (rho u, rho v) (rho w, lap T) (dT/dx, dT/dy) (dT/dz, T)
 // Output pairs, first round: (u, v) (w, rho uu) (rho vv, rho ww) (rho uv, rho uw)
 // second round (kept in registers meanwhile): (rho vw, drho) (DT, 0)
-template <int N1, int N2>
-__device__ __forceinline__ void x_extract(const Dev &d, const double2 *sm, int p, int fa, int fb, int y, int z0,
+template <int N1, int N2, typename CT, typename ST>
+__device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int fa, int fb, int y, int z0,
                                           int nzb) {
-  using F = Four<N1, N2>;
+  using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
+  using Re = typename CReal<CT>::R;
   constexpr int N = F::N;
-  const double dn = 1.0 / (double)N, hdn = 0.5 * dn;
-  double2 *A = d.zb[fa];
-  double2 *B = fb >= 0 ? d.zb[fb] : nullptr;
+  const Re dn = (Re)(1.0 / (double)N), hdn = (Re)(0.5 / (double)N);
+  ST *A = wzb<ST>(d, fa);
+  ST *B = fb >= 0 ? wzb<ST>(d, fb) : nullptr;
   for (int l = 0; l < nzb; l++) {
     const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * d.nkx;
-    const double2 *line = sm + (size_t)(p * G::ZB + l) * G::LD;
+    const CT *line = sm + (size_t)(p * G::ZB + l) * G::LD;
     for (int k = threadIdx.x; k < d.nkx; k += blockDim.x) {
-      const double2 c = line[F::sk(k)];
-      double2 a, b;
+      const CT c = line[F::sk(k)];
+      CT a, b;
       if (k == 0) {
-        a = make_double2(c.x * dn, 0.0);
-        b = make_double2(c.y * dn, 0.0);
+        a = cmk<CT>(c.x * dn, 0);
+        b = cmk<CT>(c.y * dn, 0);
       } else {
-        const double2 q = line[F::sk(N - k)];
-        a = make_double2((c.x + q.x) * hdn, (c.y - q.y) * hdn);
-        b = make_double2((c.y + q.y) * hdn, (q.x - c.x) * hdn);
+        const CT q = line[F::sk(N - k)];
+        a = cmk<CT>((c.x + q.x) * hdn, (c.y - q.y) * hdn);
+        b = cmk<CT>((c.y + q.y) * hdn, (q.x - c.x) * hdn);
       }
-      A[g0 + k] = a;
-      if (B) B[g0 + k] = b;
+      A[g0 + k] = ccvt<ST>(a);
+      if (B) B[g0 + k] = ccvt<ST>(b);
     }
   }
 }
@@ -179,15 +212,16 @@ __device__ __forceinline__ void x_extract(const Dev &d, const double2 *sm, int p
 // tile's eight input rows (each ZB*nkx contiguous complex values in the
 // [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
 // current tile is transformed.
-template <int N1, int N2>
+template <int N1, int N2, typename CT, typename ST>
 __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
-  using F = Four<N1, N2>;
+  using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
+  using Re = typename CReal<CT>::R;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
-  extern __shared__ double2 sm[];
-  const int nkx = d.nkx;
-  double2 *W = sm;                         // 4 buffers x ZB lines x LD
-  double2 *St = sm + 4 * ZB * LD;          // 8 rows of ZB*nkx inputs
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nkx = d.nkx;  // a multiple of 8 for every supported length
+  CT *W = (CT *)smraw;                                       // 4 buffers x ZB lines x LD
+  ST *St = (ST *)(smraw + round16(sizeof(CT) * 4 * ZB * LD));  // 8 rows of ZB*nkx inputs
   double *Sr = (double *)(St + 8 * ZB * nkx);  // ZB*N RHS(T)
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
@@ -196,10 +230,10 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   const int nzk = (d.mgalz + ZB - 1) / ZB;
   auto issue = [&](int t) {
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
-    const uint32_t rb = (uint32_t)nzb * nkx * sizeof(double2), hb = (uint32_t)nzb * N * sizeof(double);
+    const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = (uint32_t)nzb * N * sizeof(double);
     mbar_expect_tx(&bar, 8 * rb + hb);
     const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
-    for (int f = 0; f < 8; f++) bulk_g2s(St + f * ZB * nkx, d.zb[f] + g0, rb, &bar);
+    for (int f = 0; f < 8; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
     bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
   };
   if (threadIdx.x == 0) {
@@ -226,20 +260,20 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
     const int gap = N - 2 * nkx + 1;
     for (int idx = threadIdx.x; idx < 4 * ZB * gap; idx += blockDim.x) {
       const int ln = idx / gap, g = idx - ln * gap;
-      W[ln * LD + F::sk(nkx + g)] = czero();
+      W[ln * LD + F::sk(nkx + g)] = cz<CT>();
     }
     for (int p = 0; p < 4; p++)
       for (int l = 0; l < ZB; l++) {
-        double2 *line = W + (p * ZB + l) * LD;
-        const double2 *A = St + (2 * p) * ZB * nkx + l * nkx, *B = St + (2 * p + 1) * ZB * nkx + l * nkx;
+        CT *line = W + (p * ZB + l) * LD;
+        const ST *A = St + (2 * p) * ZB * nkx + l * nkx, *B = St + (2 * p + 1) * ZB * nkx + l * nkx;
         for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
-          double2 a = czero(), b = czero();
-          if (l < nzb) { a = A[k]; b = B[k]; }
+          CT a = cz<CT>(), b = cz<CT>();
+          if (l < nzb) { a = ccvt<CT>(A[k]); b = ccvt<CT>(B[k]); }
           if (k == 0) {
-            line[F::sk(0)] = make_double2(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
+            line[F::sk(0)] = cmk<CT>(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
           } else {
-            line[F::sk(k)] = make_double2(a.x - b.y, a.y + b.x);
-            line[F::sk(N - k)] = make_double2(a.x + b.y, b.x - a.y);
+            line[F::sk(k)] = cmk<CT>(a.x - b.y, a.y + b.x);
+            line[F::sk(N - k)] = cmk<CT>(a.x + b.y, b.x - a.y);
           }
         }
       }
@@ -254,18 +288,44 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
       fence_proxy_async();
       issue(t + gridDim.x);
     }
-    F::template nat2perm<+1>(W, 4 * ZB, LD, d.twx);
+    F::template nat2perm<+1>(W, 4 * ZB, LD, wtwx<CT>(d));
 
-    double r0[PT], r1[PT], r2[PT], rs = 0.0, mv = 0.0;
+    // mixed form: FP64 00 profiles of the inputs at this y, and the values
+    // subtracted from the outputs before they are rounded to FP32
+    constexpr bool MX = sizeof(ST) == sizeof(float2);
+    double m_in[6], est[11], acc[11];
+    if constexpr (MX) {
+#pragma unroll
+      for (int q = 0; q < 6; q++) m_in[q] = d.mi[(size_t)q * d.my + y];
+      if (d.mean_ok) {
+        const double inn = 1.0 / ((double)d.mgalx * (double)d.mgalz);
+#pragma unroll
+        for (int o = 0; o < 11; o++) est[o] = d.mo_prev[(size_t)o * d.my + y] * inn;
+      } else {  // products of the input means
+        const double eu = m_in[0] * m_in[5], ev = m_in[1] * m_in[5], ew = m_in[2] * m_in[5];
+        est[OU] = eu; est[OV] = ev; est[OW] = ew;
+        est[ORUU] = m_in[0] * eu; est[ORVV] = m_in[1] * ev; est[ORWW] = m_in[2] * ew;
+        est[ORUV] = m_in[0] * ev; est[ORUW] = m_in[0] * ew; est[ORVW] = m_in[1] * ew;
+        est[ODRHO] = 0.0; est[ODT] = 0.0;
+      }
+#pragma unroll
+      for (int o = 0; o < 11; o++) acc[o] = 0.0;
+    }
+
+    Re r0[PT], r1[PT], r2[PT];
+    double rs = 0.0, mv = 0.0;
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
       r0[j] = r1[j] = r2[j] = 0.0;
       if (q < nzb * N) {
         const int l = q / N, pos = q - l * N;
-        double2 *c0 = W + (size_t)l * LD + F::sk(pos);
-        double2 *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
-        const double2 p0 = *c0, p1 = *c1, p2 = *c2, p3 = *c3;
+        CT *c0 = W + (size_t)l * LD + F::sk(pos);
+        CT *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
+        double2 p0 = to_d2(*c0), p1 = to_d2(*c1), p2 = to_d2(*c2), p3 = to_d2(*c3);
+        if constexpr (MX) {
+          p0.x += m_in[0]; p0.y += m_in[1]; p1.x += m_in[2]; p1.y += m_in[3]; p2.y += m_in[4]; p3.y += m_in[5];
+        }
         const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
         const double rhp = rh[j];
         const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
@@ -275,13 +335,26 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
         d.rhst[((size_t)y * d.mgalz + z0 + l) * N + pos] = rhs;
         tn = tn + dtg * rhs;                                             // cross.f:1641
         d8 = d8 + dtg * rhs;                                             // cross.f:1642
-        *c0 = make_double2(u, v);
-        *c1 = make_double2(w, ru * u);                                   // cross.f:1655-1666
-        *c2 = make_double2(rv * v, rw * w);
-        *c3 = make_double2(ru * v, ru * w);
-        r0[j] = rv * w;
-        r1[j] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);              // cross.f:1670-1671
-        r2[j] = d8;                                                      // cross.f:1645-1647
+        double o[11];
+        o[OU] = u; o[OV] = v; o[OW] = w;
+        o[ORUU] = ru * u; o[ORVV] = rv * v; o[ORWW] = rw * w;              // cross.f:1655-1666
+        o[ORUV] = ru * v; o[ORUW] = ru * w; o[ORVW] = rv * w;
+        o[ODRHO] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);          // cross.f:1670-1671
+        o[ODT] = d8;                                                     // cross.f:1645-1647
+        if constexpr (MX) {
+#pragma unroll
+          for (int q = 0; q < 11; q++) {
+            acc[q] += o[q];
+            o[q] -= est[q];
+          }
+        }
+        *c0 = from_d2<CT>(make_double2(o[OU], o[OV]));
+        *c1 = from_d2<CT>(make_double2(o[OW], o[ORUU]));
+        *c2 = from_d2<CT>(make_double2(o[ORVV], o[ORWW]));
+        *c3 = from_d2<CT>(make_double2(o[ORUV], o[ORUW]));
+        r0[j] = (Re)o[ORVW];
+        r1[j] = (Re)o[ODRHO];
+        r2[j] = (Re)o[ODT];
         if (do_cfl) {
           mu = fmax(mu, fabs(u));
           mv = fmax(mv, fabs(v));
@@ -294,6 +367,13 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
     if (do_diag) {
       rs = warp_sum(rs);
       if ((threadIdx.x & 31) == 0) atomicAdd(d.rhom + y, rs);
+    }
+    if constexpr (MX) {  // FP64 plane sums: the exact 00 modes of the outputs
+#pragma unroll
+      for (int q = 0; q < 11; q++) {
+        const double v = warp_sum(acc[q]);
+        if ((threadIdx.x & 31) == 0) atomicAdd(d.mo_cur + (size_t)q * d.my + y, v);
+      }
     }
     if (do_cfl) {
       mv = warp_max(mv);
@@ -310,26 +390,26 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
       }
       s_vmax = 0ull;
     }
-    F::template perm2nat<-1>(W, 4 * ZB, LD, d.twx);
-    x_extract<N1, N2>(d, W, 0, OU, OV, y, z0, nzb);
-    x_extract<N1, N2>(d, W, 1, OW, ORUU, y, z0, nzb);
-    x_extract<N1, N2>(d, W, 2, ORVV, ORWW, y, z0, nzb);
-    x_extract<N1, N2>(d, W, 3, ORUV, ORUW, y, z0, nzb);
+    F::template perm2nat<-1>(W, 4 * ZB, LD, wtwx<CT>(d));
+    x_extract<N1, N2, CT, ST>(d, W, 0, OU, OV, y, z0, nzb);
+    x_extract<N1, N2, CT, ST>(d, W, 1, OW, ORUU, y, z0, nzb);
+    x_extract<N1, N2, CT, ST>(d, W, 2, ORVV, ORWW, y, z0, nzb);
+    x_extract<N1, N2, CT, ST>(d, W, 3, ORUV, ORUW, y, z0, nzb);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
       if (q < ZB * N) {
         const int l = q / N, pos = q - l * N;
-        double2 *c0 = W + (size_t)l * LD + F::sk(pos);
-        c0[0] = make_double2(r0[j], r1[j]);
-        c0[(size_t)ZB * LD] = make_double2(r2[j], 0.0);
+        CT *c0 = W + (size_t)l * LD + F::sk(pos);
+        c0[0] = cmk<CT>(r0[j], r1[j]);
+        c0[(size_t)ZB * LD] = cmk<CT>(r2[j], 0);
       }
     }
     __syncthreads();
-    F::template perm2nat<-1>(W, 2 * ZB, LD, d.twx);
-    x_extract<N1, N2>(d, W, 0, ORVW, ODRHO, y, z0, nzb);
-    x_extract<N1, N2>(d, W, 1, ODT, -1, y, z0, nzb);
+    F::template perm2nat<-1>(W, 2 * ZB, LD, wtwx<CT>(d));
+    x_extract<N1, N2, CT, ST>(d, W, 0, ORVW, ODRHO, y, z0, nzb);
+    x_extract<N1, N2, CT, ST>(d, W, 1, ODT, -1, y, z0, nzb);
     __syncthreads();
   }
   if (do_cfl) {
@@ -349,14 +429,17 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   }
 }
 
-template <int N1, int N2>
+template <int N1, int N2, typename CT, typename ST>
 struct Launch {
   using G = Geo<N1, N2>;
-  static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(double2); }
-  static size_t zinv_sm(int mz) { return zsm() + (size_t)G::KB * mz * sizeof(double2); }
-  static size_t xsm() { return (size_t)4 * G::ZB * G::LD * sizeof(double2); }
+  static constexpr int E = 16 / (int)sizeof(ST);
+  static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(CT); }
+  static size_t zinv_sm(int mz) {
+    return round16(sizeof(CT) * G::KB * G::LD) + ((size_t)G::KB * mz + 2 * E) * sizeof(ST);
+  }
+  static size_t xsm() { return round16(sizeof(CT) * 4 * G::ZB * G::LD); }
   static size_t xphys_sm(int nkx) {
-    return xsm() + (size_t)8 * G::ZB * nkx * sizeof(double2) + (size_t)G::ZB * G::N * sizeof(double);
+    return xsm() + (size_t)8 * G::ZB * nkx * sizeof(ST) + (size_t)G::ZB * G::N * sizeof(double);
   }
   // resident blocks per SM x SMs, for the persistent kernels
   static int grid_for(const void *fn, int threads, size_t smem, int ntiles) {
@@ -371,43 +454,46 @@ struct Launch {
   static void zinv(const Dev &d, cudaStream_t s) {
     const int ntiles = 8 * d.my * ((d.nkx + G::KB - 1) / G::KB);
     const size_t sm = zinv_sm(d.mz);
-    const int g = grid_for((const void *)k_zinv<N1, N2>, G::ZT, sm, ntiles);
-    k_zinv<N1, N2><<<g, G::ZT, sm, s>>>(d, ntiles);
+    const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, G::ZT, sm, ntiles);
+    k_zinv<N1, N2, CT, ST><<<g, G::ZT, sm, s>>>(d, ntiles);
   }
   static void zfwd(const Dev &d, cudaStream_t s) {
     dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 11);
-    k_zfwd<N1, N2><<<g, G::ZT, zsm(), s>>>(d);
+    k_zfwd<N1, N2, CT, ST><<<g, G::ZT, zsm(), s>>>(d);
   }
   static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
     const size_t sm = xphys_sm(d.nkx);
-    const int g = grid_for((const void *)k_xphys<N1, N2>, G::XT, sm, ntiles);
-    k_xphys<N1, N2><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST>, G::XT, sm, ntiles);
+    k_xphys<N1, N2, CT, ST><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+  }
+  static cudaError_t optin1(const void *fn, int limit) {
+    cudaError_t e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, fn)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, limit - (int)fa.sharedSizeBytes);
   }
   static cudaError_t optin(int limit) {
     cudaError_t e;
-    cudaFuncAttributes fa;
-    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_zinv<N1, N2>)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute((const void *)k_zinv<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  limit - (int)fa.sharedSizeBytes)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_zfwd<N1, N2>)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute((const void *)k_zfwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  limit - (int)fa.sharedSizeBytes)) != cudaSuccess) return e;
-    if ((e = cudaFuncGetAttributes(&fa, (const void *)k_xphys<N1, N2>)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute((const void *)k_xphys<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                limit - (int)fa.sharedSizeBytes);
+    if ((e = optin1((const void *)k_zinv<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
+    if ((e = optin1((const void *)k_zfwd<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
+    return optin1((const void *)k_xphys<N1, N2, CT, ST>, limit);
   }
 };
 
 // register-DFT twiddles exp(-2 pi i e / R) of every block size
 inline cudaError_t upload_twiddles() {
   std::vector<double2> t;
+  std::vector<float2> tf;
   for (int R : TW_SIZES)
     for (int e = 0; e < R; e++) {
       const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)R;
       t.push_back(make_double2((double)cosl(a), (double)(-sinl(a))));
+      tf.push_back(make_float2((float)cosl(a), (float)(-sinl(a))));
     }
-  return cudaMemcpyToSymbol(c_tw, t.data(), t.size() * sizeof(double2));
+  cudaError_t e = cudaMemcpyToSymbol(c_tw, t.data(), t.size() * sizeof(double2));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(c_twf, tf.data(), tf.size() * sizeof(float2));
 }
 
 }  // namespace LMC_FFT_NS
@@ -415,16 +501,24 @@ inline cudaError_t upload_twiddles() {
 
 // Each translation unit defines LMC_FFT_SIZES(X) as X(N, N1, N2) entries and
 // then expands LMC_FFT_TU_BODY(suffix) to get its dispatch functions.
+#define LMC_FFT_FORMS(N1, N2, CALL)                                   \
+  switch (d.prec) {                                                   \
+    case 1: Launch<N1, N2, float2, float2>::CALL; break;              \
+    case 2: Launch<N1, N2, double2, float2>::CALL; break;             \
+    default: Launch<N1, N2, double2, double2>::CALL; break;           \
+  }
 #define LMC_FFT_CASE_Z(N, N1, N2, WHAT) \
-  case N: Launch<N1, N2>::WHAT(d, s); return true;
+  case N: LMC_FFT_FORMS(N1, N2, WHAT(d, s)) return true;
 #define LMC_FFT_CASE_X(N, N1, N2) \
-  case N: Launch<N1, N2>::xphys(d, rk, do_cfl, do_diag, s); return true;
+  case N: LMC_FFT_FORMS(N1, N2, xphys(d, rk, do_cfl, do_diag, s)) return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
-#define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2>::zinv_sm(2 * (N / 3));
-#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2>::xphys_sm(N / 3);
-#define LMC_FFT_CASE_OPT(N, N1, N2) \
-  if ((e = Launch<N1, N2>::optin(limit)) != cudaSuccess) return e;
+#define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3);
+#define LMC_FFT_CASE_OPT(N, N1, N2)                                                         \
+  if ((e = Launch<N1, N2, double2, double2>::optin(limit)) != cudaSuccess) return e;        \
+  if ((e = Launch<N1, N2, float2, float2>::optin(limit)) != cudaSuccess) return e;          \
+  if ((e = Launch<N1, N2, double2, float2>::optin(limit)) != cudaSuccess) return e;
 #define LMC_FFT_CASE_HAS(N, N1, N2) case N: return true;
 
 #define LMC_FFT_TU_BODY(SUF)                                                                      \

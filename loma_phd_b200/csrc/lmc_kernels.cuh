@@ -13,6 +13,8 @@ namespace lmc {
 // The reference layout [kx][kz][y] is used only at the C ABI and converted
 // by the transpose kernels.
 struct Dev {
+  int prec;  // 0: FP64; 1: mixed (FP32 work buffers and transforms);
+             // 2: mixed with FP64 transform arithmetic (FP32 work buffers)
   int my, mgalx, mgalz, nkx, mz, nz1, nmode;
   int lpm, base, extra, C;  // y-chunking of a pencil over the lanes of a warp
   int ldy;                  // staging stride of a pencil (odd, >= my)
@@ -27,23 +29,61 @@ struct Dev {
   const double *PL, *PU, *V12, *AAinv, *k2;
   const double *kx, *kz;  // wavenumber per kx plane / kz index
   const double2 *twx, *twz;  // exp(-2 pi i e / N) for the x / z transform lengths
+  const float2 *twxf, *twzf;  // the same in FP32 (mixed form)
   // state
   double2 *vor, *phi, *psi, *scal, *Rom, *Rphi;
   double *u00, *v00, *w00, *rf0u, *rf0w, *rf0v;
-  double2 *sb[11];  // spectral work buffers
-  double2 *zb[11];  // z-physical work buffers
+  double2 *sb[11];  // spectral work buffers (FP64 form; [7..9] also staging)
+  double2 *zb[11];  // z-physical work buffers (FP64 form)
+  float2 *sbf[11];  // spectral work buffers (mixed form)
+  float2 *zbf[11];  // z-physical work buffers (mixed form)
   double *rhst;
   // device scalars: [0] Deltat, [1] dtr, [2] time, [3] rhobot, [4] rhotop
   double *scal_d;
   unsigned long long *cflmax;  // [4] max|u|, max|v|/hy, max|w|, max cflT (ordered bits)
   double *rhom;                // [my] plane sums of 1/T
+  // Mixed form: the kx = kz = 0 (00) modes bypass the FP32 transforms.
+  //   mi     [6][my]  00 profiles of the transform inputs rho u, rho v,
+  //                   rho w, lap T, dT/dy, T (FP64); zinv drops the 00
+  //                   coefficient and xphys adds the profile back per point
+  //   mo_cur [11][my] FP64 plane sums of the 11 transform outputs (their
+  //                   exact 00 modes times mgalx*mgalz), read by post1/psi
+  //   mo_prev[11][my] the sums of the previous substep: xphys subtracts
+  //                   prev/(mgalx*mgalz) before rounding an output to FP32,
+  //                   so the FP32 transforms carry fluctuations only
+  //   mean_ok         0 until mo_prev holds a substep's sums
+  double *mi, *mo_cur, *mo_prev;
+  int mean_ok;
   double *diag;                // [16]
   int *status;
 };
 
 // Spectral work-buffer roles before / after the transforms.
-enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY };
+// SB_T32 holds an FP32 copy of T for the z transforms of the mixed form.
+enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32 };
 enum { OU = 0, OV, OW, ORUU, ORVV, ORWW, ORUV, ORUW, ORVW, ODRHO, ODT };
+
+// work-buffer views of the two precisions
+template <typename CT>
+__device__ __forceinline__ CT *wsb(const Dev &d, int i) {
+  if constexpr (sizeof(CT) == sizeof(double2)) return d.sb[i];
+  else return d.sbf[i];
+}
+template <typename CT>
+__device__ __forceinline__ CT *wzb(const Dev &d, int i) {
+  if constexpr (sizeof(CT) == sizeof(double2)) return d.zb[i];
+  else return d.zbf[i];
+}
+template <typename CT>
+__device__ __forceinline__ const CT *wtwx(const Dev &d) {
+  if constexpr (sizeof(CT) == sizeof(double2)) return d.twx;
+  else return d.twxf;
+}
+template <typename CT>
+__device__ __forceinline__ const CT *wtwz(const Dev &d) {
+  if constexpr (sizeof(CT) == sizeof(double2)) return d.twz;
+  else return d.twzf;
+}
 
 bool fft_supported(int n);
 void launch_lapv(const Dev &d, cudaStream_t s);

@@ -1,0 +1,31 @@
+// lmc_ylaunch.h -- launchers of the y-direction kernels for one chunk size
+// C and one work-buffer type CT (double2: FP64 form, float2: mixed form).
+// The definitions are in lmc_ykernels.cuh; each lmc_y_*.cu translation unit
+// instantiates its chunk sizes so that they compile in parallel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lmc_kernels.cuh"
+
+namespace lmc {
+
+template <int C, typename CT>
+struct YL {
+  static void lapv(const Dev &d, cudaStream_t s);
+  static void assemble(const Dev &d, int rk, cudaStream_t s);
+  static void tder(const Dev &d, cudaStream_t s);
+  static void post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
+  static void post2(const Dev &d, int rk, cudaStream_t s);
+  static void psi(const Dev &d, int rk, int cfl_step, int do_diag, cudaStream_t s);
+  static void op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s);
+  static cudaError_t optin(int limit);
+};
+
+#define LMC_Y_CHUNKS(X) X(4) X(5) X(7) X(9) X(13) X(17)
+#define LMC_Y_EXTERN(C)                   \
+  extern template struct YL<C, double2>; \
+  extern template struct YL<C, float2>;
+LMC_Y_CHUNKS(LMC_Y_EXTERN)
+#undef LMC_Y_EXTERN
+
+}  // namespace lmc
