@@ -167,6 +167,13 @@ int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev,
  * device takes the array's address and should precede any stream capture. */
 int lmc_deryr2_noalloc(int my, const double *y, int npencil,
                        const double *in_dev, double *out_dev, void *stream);
+
+/* y-metrics of a mesh, host only (no device needed): fmap = 1/(dy/deta)
+ * by the compact first-derivative scheme (cfdiff.f:912-937, the fmap the
+ * reference writes into restart record 1, escru.f:130-132), and the mesh
+ * weights hy and trp of main.f:689-696.  Any output pointer may be NULL.
+ * Returns LMC_EINVAL for my < 9. */
+int lmc_y_metrics(int my, const double *y, double *fmap, double *hy, double *trp);
 #ifdef __cplusplus
 }
 #endif

@@ -521,3 +521,19 @@ extern "C" int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_pa
   }
   return LMC_OK;
 }
+
+extern "C" int lmc_y_metrics(int my, const double *y, double *fmap, double *hy, double *trp) {
+  if (!y || my < 9) return LMC_EINVAL;
+  lmc::YOps o;
+  try {
+    lmc::build_yops(my, y, o);
+  } catch (...) {
+    return LMC_EINVAL;
+  }
+  for (int j = 0; j < my; j++) {
+    if (fmap) fmap[j] = o.fmap[j];
+    if (hy) hy[j] = o.hy[j];
+    if (trp) trp[j] = o.trp[j];
+  }
+  return LMC_OK;
+}

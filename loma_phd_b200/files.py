@@ -1,0 +1,238 @@
+"""The reference's file formats, read and written by the host side.
+
+* Restart / image files (Fortran unformatted sequential, little endian,
+  4-byte record markers), written by escru (trunk/lomacte3/src/escru.f:
+  121-139) and read by getfil (trunk/lomacte3/src/main.f:361-406):
+    record 1: time, Re, alp, bet, a0 (real*4), mx, my, mz (integer*4),
+              (y_j, fmap_j) real*8 pairs for j = 1..my,
+              (u00_j, v00_j, w00_j) real*4 triples for j = 1..my
+    then one record per kx plane i = 0..mx/2-1:
+              ((vor, phi, psi, scal)(j, k), j = 0..2my-1, k = 0..mz-1) real*4,
+              the four fields interleaved per real scalar, j running over
+              the (re, im) pairs of the y pencil.
+  Reading into a grid with another mz keeps the kz = 0..klen-1 and the last
+  klen-1 (negative) modes, as assign does (main.f:841-882).
+* hre.dat (main.f:502-545): lines that start with "CC" are comments; then
+  Re alp bet a0 / nstep nimag nhist / CFL ncfl / id22 nstart ntimes /
+  output, input and statistics file names.
+* The .cf history line (cross.f:1172-1176): 21 values in format 21(d22.14):
+  time, dm, dw, Re*dw, trapz, masst, enerdis, energy(1..9), massu, massv,
+  massw, wall time, communication time.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import struct
+from typing import Dict, Iterable, List, Optional
+
+import numpy as np
+
+_FIELDS = ("vor", "phi", "psi", "scal")
+
+
+# --------------------------------------------------------------------------
+# Fortran sequential records
+# --------------------------------------------------------------------------
+def _write_record(f, payload: bytes) -> None:
+    n = struct.pack("<i", len(payload))
+    f.write(n)
+    f.write(payload)
+    f.write(n)
+
+
+def _read_record(f) -> Optional[bytes]:
+    head = f.read(4)
+    if not head:
+        return None
+    if len(head) != 4:
+        raise ValueError("truncated record marker")
+    (n,) = struct.unpack("<i", head)
+    if n < 0:
+        raise ValueError("negative record length (not a little-endian sequential file?)")
+    payload = f.read(n)
+    tail = f.read(4)
+    if len(payload) != n or len(tail) != 4 or struct.unpack("<i", tail)[0] != n:
+        raise ValueError("record markers do not match")
+    return payload
+
+
+# --------------------------------------------------------------------------
+# restart / image files
+# --------------------------------------------------------------------------
+@dataclasses.dataclass
+class RestartHeader:
+    time: float
+    Re: float
+    alp: float
+    bet: float
+    a0: float
+    mx: int
+    my: int
+    mz: int
+    y: np.ndarray
+    fmap: np.ndarray
+
+
+def write_restart(path: str, state: Dict[str, np.ndarray], y: np.ndarray, fmap: np.ndarray, *, time: float,
+                  Re: float, alp: float, bet: float, a0: float = 0.0) -> None:
+    """Write a state dict (vor, phi, psi, scal complex [nkx][mz][my]; u00,
+    v00, w00 [my]) as the reference writes its images (escru.f:121-139).
+    Values are stored in real*4 like the reference; y and fmap in real*8."""
+    vor = np.asarray(state["vor"])
+    nkx, mz, my = vor.shape
+    y = np.asarray(y, dtype=np.float64)
+    fmap = np.asarray(fmap, dtype=np.float64)
+    if y.shape != (my,) or fmap.shape != (my,):
+        raise ValueError("y and fmap must have my entries")
+    head = struct.pack("<5f3i", time, Re, alp, bet, a0, 2 * nkx, my, mz)
+    yf = np.empty((my, 2), dtype="<f8")
+    yf[:, 0] = y
+    yf[:, 1] = fmap
+    w00 = np.empty((my, 3), dtype="<f4")
+    w00[:, 0] = state["u00"]
+    w00[:, 1] = state["v00"]
+    w00[:, 2] = state["w00"]
+    with open(path, "wb") as f:
+        _write_record(f, head + yf.tobytes() + w00.tobytes())
+        plane = np.empty((mz, 2 * my, 4), dtype="<f4")
+        for i in range(nkx):
+            for q, name in enumerate(_FIELDS):
+                a = np.ascontiguousarray(state[name][i], dtype=np.complex64)  # [mz][my]
+                plane[:, :, q] = a.view(np.float32).reshape(mz, 2 * my)
+            _write_record(f, plane.tobytes())
+
+
+def _assign_kz(a: np.ndarray, mz: int) -> np.ndarray:
+    """kz re-mapping of a [..][mze][..] array to mz modes (main.f:857-882)."""
+    mze = a.shape[-2]
+    if mze == mz:
+        return a
+    out = np.zeros(a.shape[:-2] + (mz, a.shape[-1]), dtype=a.dtype)
+    klen = (min(mz, mze) + 1) // 2
+    out[..., :klen, :] = a[..., :klen, :]
+    if klen > 1:
+        out[..., mz - klen + 1:, :] = a[..., mze - klen + 1:, :]
+    return out
+
+
+def read_restart(path: str, mz: Optional[int] = None) -> Dict[str, object]:
+    """Read a restart / image file.  Returns a dict with the header
+    (RestartHeader under "header") and the state: vor, phi, psi, scal as
+    complex128 [nplanes][mz][my] (real*4 values widened), u00, v00, w00.
+    With mz given, the kz modes are re-mapped as the reference does."""
+    with open(path, "rb") as f:
+        r1 = _read_record(f)
+        if r1 is None or len(r1) < 32:
+            raise ValueError("missing header record")
+        time, Re, alp, bet, a0, mx, my, mze = struct.unpack("<5f3i", r1[:32])
+        need = 32 + 16 * my + 12 * my
+        if len(r1) != need:
+            raise ValueError(f"header record has {len(r1)} bytes, expected {need} for my={my}")
+        yf = np.frombuffer(r1, dtype="<f8", count=2 * my, offset=32).reshape(my, 2)
+        w00 = np.frombuffer(r1, dtype="<f4", count=3 * my, offset=32 + 16 * my).reshape(my, 3)
+        planes: List[np.ndarray] = []
+        while True:
+            rec = _read_record(f)
+            if rec is None:
+                break
+            if len(rec) != 4 * 8 * my * mze:
+                raise ValueError("plane record of unexpected length")
+            planes.append(np.frombuffer(rec, dtype="<f4").reshape(mze, 2 * my, 4))
+    data = np.stack(planes) if planes else np.zeros((0, mze, 2 * my, 4), dtype=np.float32)
+    out: Dict[str, object] = {
+        "header": RestartHeader(time, Re, alp, bet, a0, mx, my, mze, yf[:, 0].copy(), yf[:, 1].copy()),
+        "u00": w00[:, 0].astype(np.float64), "v00": w00[:, 1].astype(np.float64),
+        "w00": w00[:, 2].astype(np.float64), "time": float(time),
+    }
+    for q, name in enumerate(_FIELDS):
+        re_im = np.ascontiguousarray(data[:, :, :, q]).reshape(data.shape[0], mze, my, 2)
+        c = (re_im[..., 0].astype(np.float64) + 1j * re_im[..., 1].astype(np.float64))
+        out[name] = _assign_kz(c, mz) if mz is not None else c
+    return out
+
+
+# --------------------------------------------------------------------------
+# hre.dat
+# --------------------------------------------------------------------------
+@dataclasses.dataclass
+class HreData:
+    Re: float
+    alp: float
+    bet: float
+    a0: float
+    nstep: int
+    nimag: int
+    nhist: int
+    cfl: float
+    ncfl: int
+    id22: int
+    nstart: int
+    ntimes: int
+    filout: str
+    filinp: str
+    filstt: str
+
+
+def _fortran_values(text: str) -> List[str]:
+    return [t for t in text.replace(",", " ").split() if t]
+
+
+def _ffloat(t: str) -> float:
+    return float(t.replace("D", "E").replace("d", "e"))
+
+
+def read_hre(path: str) -> HreData:
+    """Parse hre.dat as initcr does (main.f:502-545)."""
+    with open(path) as f:
+        lines = [ln.rstrip("\n") for ln in f]
+    data = [ln for ln in lines if not ln[:2] == "CC"]
+    if len(data) < 7:
+        raise ValueError("hre.dat needs 4 parameter lines and 3 file names")
+    v = _fortran_values(data[0])
+    Re, alp, bet, a0 = (_ffloat(t) for t in v[:4])
+    nstep, nimag, nhist = (int(_ffloat(t)) for t in _fortran_values(data[1])[:3])
+    v = _fortran_values(data[2])
+    cfl, ncfl = _ffloat(v[0]), int(_ffloat(v[1]))
+    id22, nstart, ntimes = (int(_ffloat(t)) for t in _fortran_values(data[3])[:3])
+    # a70 read, then the name up to the first blank (filout(1:index(filout,' ')-1))
+    names = [data[4 + q][:70].split(" ")[0] for q in range(3)]
+    return HreData(Re, alp, bet, a0, nstep, nimag, nhist, cfl, ncfl, id22, nstart, ntimes, *names)
+
+
+# --------------------------------------------------------------------------
+# .cf history
+# --------------------------------------------------------------------------
+def fortran_d(x: float, w: int = 22, d: int = 14) -> str:
+    """Fortran Dw.d edit of one value (0.ddd...D+ee, right-justified)."""
+    x = float(x)
+    if not math.isfinite(x):
+        return ("NaN" if math.isnan(x) else ("-Infinity" if x < 0 else "Infinity")).rjust(w)
+    sign = "-" if (x < 0 or (x == 0 and math.copysign(1.0, x) < 0)) else ""
+    a = abs(x)
+    if a == 0.0:
+        mant, e = "0" * d, 0
+    else:
+        s = f"{a:.{d - 1}e}"  # d significant digits: m.mmm e+XX
+        digits, exp = s.split("e")
+        mant = digits.replace(".", "")
+        e = int(exp) + 1
+    if abs(e) <= 99:
+        ex = f"D{'+' if e >= 0 else '-'}{abs(e):02d}"
+    else:
+        ex = f"{'+' if e >= 0 else '-'}{abs(e):03d}"
+    s = f"{sign}0.{mant}{ex}"
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def cf_line(diag: Dict[str, float], energies: Optional[Iterable[float]] = None, enerdis: float = 0.0,
+            wall: float = 0.0, comm: float = 0.0) -> str:
+    """One .cf record (cross.f:1172-1176) from a diag dict of Lomacte.diag().
+    energy(1..9) and enerdis come from the statistics module of the
+    reference; without them they are written as zeros."""
+    en = list(energies) if energies is not None else [0.0] * 9
+    if len(en) != 9:
+        raise ValueError("energy has 9 entries")
+    vals = [diag["time"], diag["dm"], diag["dw"], diag["Redw"], diag["trapz"], diag["masst"], enerdis] + en + \
+        [diag["massu"], diag["massv"], diag["massw"], wall, comm]
+    return "".join(fortran_d(v) for v in vals)

@@ -30,7 +30,7 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read", "lmc_deryr2_noalloc",
+    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics",
 )
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset")
@@ -100,6 +100,7 @@ def _lib():
         L.lmc_profile_start.argtypes = [vp]
         L.lmc_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
+        L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         _LIB = L
     return _LIB
 
@@ -190,6 +191,14 @@ def make_ic(p: Params, y: np.ndarray, ic: ICParams):
     return dict(vor=f[0], phi=f[1], psi=f[2], scal=f[3], u00=r[0], v00=r[1], w00=r[2], time=0.0)
 
 
+def y_metrics(y: np.ndarray):
+    """fmap = 1/(dy/deta), hy and trp of a mesh (host only; lmc_y_metrics)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    out = [np.zeros(len(y)) for _ in range(3)]
+    _check(_lib().lmc_y_metrics(len(y), _ptr(y), *[_ptr(a) for a in out]), "lmc_y_metrics")
+    return dict(fmap=out[0], hy=out[1], trp=out[2])
+
+
 def deryr2_noalloc(y: np.ndarray, npencil: int, in_ptr: int, out_ptr: int, stream: int = 0) -> int:
     """d/dy of npencil device pencils without any device allocation (see
     lmc_deryr2_noalloc in include/lomacte_b200.h).  Returns the status."""
@@ -233,6 +242,17 @@ class Lomacte:
         r = [np.ascontiguousarray(st[k], dtype=np.float64) for k in ("u00", "v00", "w00")]
         _check(_lib().lmc_load_state_f64(self._h, *[_ptr(a) for a in f], *[_ptr(a) for a in r],
                                          float(st.get("time", 0.0))), "lmc_load_state_f64")
+
+    def load_state_f32(self, fields: dict, u00, v00, w00, time: float = 0.0):
+        """Load complex*8 fields (the reference's storage type, e.g. from
+        files.read_restart) through lmc_load_state_f32."""
+        f = [np.ascontiguousarray(fields[k], dtype=np.complex64).view(np.float32) for k in ("vor", "phi", "psi", "scal")]
+        for a in f:
+            if a.size != 2 * int(np.prod(self.shape)):
+                raise ValueError("field size does not match the grid")
+        r = [np.ascontiguousarray(v, dtype=np.float64) for v in (u00, v00, w00)]
+        _check(_lib().lmc_load_state_f32(self._h, *[_ptr(a, _fp) for a in f], *[_ptr(a) for a in r], float(time)),
+               "lmc_load_state_f32")
 
     def get_state(self) -> dict:
         f = [np.zeros(self.shape, dtype=np.complex128) for _ in range(4)]
