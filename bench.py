@@ -95,6 +95,10 @@ def parse():
                     help="both: time the FP64 and the mixed form; the headline value is the mixed form")
     ap.add_argument("--mixed-form", type=int, default=1, choices=(1, 2),
                     help="1: FP32 FFT arithmetic; 2: FP64 FFT arithmetic on FP32 storage")
+    ap.add_argument("--serve-requests", type=int, default=16,
+                    help="requests of the synthetic serving stream (0: skip)")
+    ap.add_argument("--serve-scale", type=float, default=0.05,
+                    help="factor on the stream's step counts (log-uniform in [200, 2000])")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
@@ -330,6 +334,25 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
             "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
 
 
+def run_serving(a, dev):
+    """The synthetic serving stream (Poisson arrivals of 3-D runs of uneven
+    sizes) served by continuous batching, once in the mixed form and once in
+    FP64; p50/p99 completion latency and aggregate throughput of each."""
+    import torch
+    from loma_phd_b200.serve import Server, synthetic_stream
+    free, _ = torch.cuda.mem_get_info(dev)
+    cap = int(min(150e9, 0.8 * free))
+    out = {"stream": f"{a.serve_requests} requests, Poisson arrivals at 4/s, nx=nz in {{64..256}}, "
+                     f"ny in {{129,193,257}}, Re~U[100,1000], s~U[1,8], steps log-uniform [200,2000] x "
+                     f"{a.serve_scale:g}, HBM cap {cap / 1e9:.0f} GB, 16 slots",
+           "unit": "s (latency), Mpts*RK3-steps/s (aggregate)"}
+    for name, prec in (("mixed", a.mixed_form), ("fp64", 0)):
+        reqs = synthetic_stream(a.serve_requests, seed=7, rate=4.0, steps_scale=a.serve_scale,
+                                nx_range=(64, 256), precision=prec)
+        out[name] = Server(cap, max_active=16, chunk=8, device=dev).run(reqs)["stats"]
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -362,6 +385,9 @@ def main():
             if k in ("v00", "w00"):  # measured against the size of u00
                 den = max(den, np.linalg.norm(ref["u00"]))
             errs[k] = float(np.linalg.norm(np.asarray(arms[1]["state"][k]) - np.asarray(ref[k])) / den)
+    serving = None
+    if world == 1 and a.serve_requests > 0:
+        serving = run_serving(a, dev)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, head["p"], head["y"], head["st"])
@@ -382,7 +408,7 @@ def main():
             "gpu_launches": LAUNCHES_PER_STEP * a.steps,
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "step_roofline_frac": head["step_roofline_frac"],
-            "e2e": head["e2e"], "cpu_baseline": cpu,
+            "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving,
         }
         if mixed and 0 in arms:
             f64 = arms[0]

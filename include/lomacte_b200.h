@@ -125,6 +125,21 @@ int lmc_state_device_ptrs(lmc_handle *h, double **vor, double **phi,
 int lmc_profile_start(lmc_handle *h);
 int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count);
 
+/* Serving helpers (no counterpart in the reference, which runs one case per
+ * MPI job).
+ * lmc_use_graphs: lmc_step replays one CUDA graph per RK3 step (the default,
+ *   on) or enqueues the kernels one by one (off).  The first step after a
+ *   load and steps run while profiling always enqueue directly.
+ * lmc_query: 1 when all work enqueued on the handle's stream has finished,
+ *   0 while it runs, < 0 on error (never blocks).
+ * lmc_device_bytes: device memory held by the handle.
+ * lmc_footprint: device bytes lmc_create would allocate for p (0 for an
+ *   unsupported grid), for admission control before creating a case. */
+int lmc_use_graphs(lmc_handle *h, int on);
+int lmc_query(lmc_handle *h);
+size_t lmc_device_bytes(lmc_handle *h);
+size_t lmc_footprint(const lmc_params *p);
+
 /* Seeded initial condition (host only, no GPU): the structure of the
  * reference generator trunk/initloma3/src/main.f:95-609 with a
  * counter-based PRNG keyed by seed.  Mean profiles rho00 = 1 +

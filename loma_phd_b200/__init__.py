@@ -4,4 +4,4 @@ The compute lives in liblomacte_b200.so (sm_100a CUDA + C++ host set-up);
 ``lomacte.Lomacte`` is the host-side mirror of the reference cross1 loop.
 """
 from .lomacte import (ICParams, Lomacte, LomacteError, Params, lib, make_ic,  # noqa: F401
-                      stretched_mesh, y_metrics)
+                      footprint, stretched_mesh, y_metrics)

@@ -30,7 +30,8 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics",
+    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
+    "lmc_device_bytes", "lmc_footprint",
 )
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset")
@@ -101,6 +102,12 @@ def _lib():
         L.lmc_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
         L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.lmc_use_graphs.argtypes = [vp, ctypes.c_int]
+        L.lmc_query.argtypes = [vp]
+        L.lmc_device_bytes.argtypes = [vp]
+        L.lmc_device_bytes.restype = ctypes.c_size_t
+        L.lmc_footprint.argtypes = [ctypes.POINTER(lmc_params)]
+        L.lmc_footprint.restype = ctypes.c_size_t
         _LIB = L
     return _LIB
 
@@ -199,6 +206,12 @@ def y_metrics(y: np.ndarray):
     return dict(fmap=out[0], hy=out[1], trp=out[2])
 
 
+def footprint(p: "Params") -> int:
+    """Device bytes a case with these parameters holds (lmc_footprint)."""
+    pc = p.c()
+    return int(_lib().lmc_footprint(ctypes.byref(pc)))
+
+
 def deryr2_noalloc(y: np.ndarray, npencil: int, in_ptr: int, out_ptr: int, stream: int = 0) -> int:
     """d/dy of npencil device pencils without any device allocation (see
     lmc_deryr2_noalloc in include/lomacte_b200.h).  Returns the status."""
@@ -253,6 +266,20 @@ class Lomacte:
         r = [np.ascontiguousarray(v, dtype=np.float64) for v in (u00, v00, w00)]
         _check(_lib().lmc_load_state_f32(self._h, *[_ptr(a, _fp) for a in f], *[_ptr(a) for a in r], float(time)),
                "lmc_load_state_f32")
+
+    def use_graphs(self, on: bool):
+        _check(_lib().lmc_use_graphs(self._h, int(bool(on))), "lmc_use_graphs")
+
+    def done(self) -> bool:
+        """True when the enqueued steps have finished (never blocks)."""
+        rc = _lib().lmc_query(self._h)
+        if rc < 0:
+            raise LomacteError(rc, "lmc_query")
+        return rc == 1
+
+    @property
+    def device_bytes(self) -> int:
+        return int(_lib().lmc_device_bytes(self._h))
 
     def get_state(self) -> dict:
         f = [np.zeros(self.shape, dtype=np.complex128) for _ in range(4)]
