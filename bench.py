@@ -78,7 +78,8 @@ MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
                2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
 
 # Kernel launches per RK3 step: 3 substeps x 10 kernels (lapv, assemble,
-# tder, zinv, xphys, zfwd, post1, post2a, post2b, psi).
+# tder, zinv, xphys, zfwd, post1, post2a, post2b, psi); the mixed form adds
+# the plane-sum reduction (msum) after xphys in every substep.
 LAUNCHES_PER_STEP = 30
 
 
@@ -405,7 +406,7 @@ def main():
                                    f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
                        "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},
-            "gpu_launches": LAUNCHES_PER_STEP * a.steps,
+            "gpu_launches": (LAUNCHES_PER_STEP + (3 if mixed else 0)) * a.steps,
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving,

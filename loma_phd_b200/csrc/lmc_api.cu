@@ -301,8 +301,11 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     }
   }
   if (d.prec) {
+    // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
+    d.mpart_ld = 4 * g.mgalz;
     if ((rc = dalloc(h, &d.mi, (size_t)6 * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)11 * g.my)) ||
-        (rc = dalloc(h, &h->mo[1], (size_t)11 * g.my))) {
+        (rc = dalloc(h, &h->mo[1], (size_t)11 * g.my)) ||
+        (rc = dalloc(h, &d.mpart, (size_t)11 * g.my * d.mpart_ld))) {
       lmc_destroy(h);
       return rc;
     }
@@ -417,8 +420,6 @@ int enqueue_step(lmc_handle *h, int cfl_step) {
       if (d.prec) {  // this substep's plane sums, and the previous ones
         d.mo_cur = h->mo[h->mo_flip];
         d.mo_prev = h->mo[1 - h->mo_flip];
-        prof_mark(h, 9);
-        LMC_CK(cudaMemsetAsync(d.mo_cur, 0, (size_t)11 * d.my * sizeof(double), s));
       }
       prof_mark(h, 0);
       lmc::launch_lapv(d, s);
@@ -560,7 +561,7 @@ size_t lmc_footprint(const lmc_params *p) {
   size_t b = 6 * S * 16 + P * 8;                                  // state, R_om, R_phi, RHS(T)
   b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8;  // per-mode Poisson tables
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
-  else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8;
+  else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;
   b += (size_t)C * 32 * 64 * 8 + 6 * 5 * 32 * 16 * 8 + (size_t)(g.mgalx + g.mgalz) * 24;  // y tables, twiddles
   b += 64 * 16 * 64;                                              // allocation padding and scalars
   return b;

@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
+  static_assert(G::XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nkx = d.nkx;  // a multiple of 8 for every supported length
   CT *W = (CT *)smraw;                                       // 4 buffers x ZB lines x LD
@@ -368,11 +369,12 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
       rs = warp_sum(rs);
       if ((threadIdx.x & 31) == 0) atomicAdd(d.rhom + y, rs);
     }
-    if constexpr (MX) {  // FP64 plane sums: the exact 00 modes of the outputs
+    if constexpr (MX) {  // FP64 partial plane sums, one slot per (tile, warp)
+      const int slot = (z0 / ZB) * (G::XT / 32) + (threadIdx.x >> 5);
 #pragma unroll
       for (int q = 0; q < 11; q++) {
         const double v = warp_sum(acc[q]);
-        if ((threadIdx.x & 31) == 0) atomicAdd(d.mo_cur + (size_t)q * d.my + y, v);
+        if ((threadIdx.x & 31) == 0) d.mpart[((size_t)q * d.my + y) * d.mpart_ld + slot] = v;
       }
     }
     if (do_cfl) {
@@ -429,6 +431,24 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   }
 }
 
+// Plane sums of the mixed form's outputs from the partial sums of k_xphys,
+// added in a fixed order so that a run is reproducible bit for bit.
+template <int N1, int N2>
+__global__ void __launch_bounds__(128) k_msum(Dev d, int nslot) {
+  __shared__ double red[128];
+  const int y = blockIdx.x, q = blockIdx.y;
+  const double *src = d.mpart + ((size_t)q * d.my + y) * d.mpart_ld;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nslot; i += blockDim.x) s += src[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = 64; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) d.mo_cur[(size_t)q * d.my + y] = red[0];
+}
+
 template <int N1, int N2, typename CT, typename ST>
 struct Launch {
   using G = Geo<N1, N2>;
@@ -466,6 +486,10 @@ struct Launch {
     const size_t sm = xphys_sm(d.nkx);
     const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST>, G::XT, sm, ntiles);
     k_xphys<N1, N2, CT, ST><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    if constexpr (sizeof(ST) == sizeof(float2)) {
+      const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (G::XT / 32);
+      k_msum<N1, N2><<<dim3(d.my, 11), 128, 0, s>>>(d, nslot);
+    }
   }
   static cudaError_t optin1(const void *fn, int limit) {
     cudaError_t e;

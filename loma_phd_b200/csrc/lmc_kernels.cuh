@@ -52,8 +52,10 @@ struct Dev {
   //                   prev/(mgalx*mgalz) before rounding an output to FP32,
   //                   so the FP32 transforms carry fluctuations only
   //   mean_ok         0 until mo_prev holds a substep's sums
-  double *mi, *mo_cur, *mo_prev;
-  int mean_ok;
+  //   mpart  [11][my][mpart_ld] per-(tile, warp) partial sums of xphys,
+  //          added in a fixed order into mo_cur by k_msum
+  double *mi, *mo_cur, *mo_prev, *mpart;
+  int mean_ok, mpart_ld;
   double *diag;                // [16]
   int *status;
 };
