@@ -77,11 +77,6 @@ NCU_TRAFFIC_MIXED_256x65 = {}
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
                2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
 
-# Kernel launches per RK3 step: 3 substeps x 10 kernels (lapv, assemble,
-# tder, zinv, xphys, zfwd, post1, post2a, post2b, psi); the mixed form adds
-# the plane-sum reduction (msum) after xphys in every substep.
-LAUNCHES_PER_STEP = 30
-
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -244,6 +239,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     st = make_ic(p, y, ICParams(s=4.0, seed=rank))
     g = Lomacte(p, y)
     g.load_state(st)
+    g_launches = g.launches_per_step
+    y_family = g.y_family
     stream = torch.cuda.ExternalStream(g.stream, device=dev)
 
     def barrier():
@@ -329,9 +326,11 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at "
                                   "256x65x256, scaled by ny/65" if traffic else None,
                 "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
+    launches = g_launches
     step_bytes = 3 * sum(f(S, Z, P, w) for f in ALGO.values())
     return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
             "kernel_share": share, "e2e": e2e, "state": state, "diag": diag, "step_bytes": step_bytes,
+            "launches_per_step": launches, "y_family": y_family,
             "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
 
 
@@ -406,7 +405,8 @@ def main():
                                    f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
                        "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},
-            "gpu_launches": (LAUNCHES_PER_STEP + (3 if mixed else 0)) * a.steps,
+            "gpu_launches": head["launches_per_step"] * a.steps,
+            "y_kernels": head["y_family"],
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving,

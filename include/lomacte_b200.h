@@ -135,6 +135,13 @@ int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count);
  * lmc_device_bytes: device memory held by the handle.
  * lmc_footprint: device bytes lmc_create would allocate for p (0 for an
  *   unsupported grid), for admission control before creating a case. */
+/* lmc_launches_per_step: kernels one RK3 step launches on this handle.
+ * lmc_y_family: 1 when the handle runs the mode-parallel y kernels (one
+ *   thread per (kx,kz) mode; chosen for grids with >= 16384 modes, or by
+ *   LMC_YPATH=mode|warp in the environment at lmc_create), 0 for the
+ *   warp-per-mode kernels. */
+int lmc_launches_per_step(lmc_handle *h);
+int lmc_y_family(lmc_handle *h);
 int lmc_use_graphs(lmc_handle *h, int on);
 int lmc_query(lmc_handle *h);
 size_t lmc_device_bytes(lmc_handle *h);

@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -107,6 +108,16 @@ int pick_chunks(int my, int &C, int &lpm, int &base, int &extra) {
   if (lpm > 32 || base < 3) return LMC_EINVAL;
   if (!(base == C - 1 || (base == C && extra == 0))) return LMC_EINVAL;
   return LMC_OK;
+}
+
+// y kernels: mode-parallel (one thread per mode) once there are enough
+// modes to fill the GPU, warp-per-mode below that.  LMC_YPATH=mode|warp
+// forces one family (tests compare them).
+bool mode_parallel(int nmode) {
+  const char *e = std::getenv("LMC_YPATH");
+  if (e && std::strcmp(e, "mode") == 0) return true;
+  if (e && std::strcmp(e, "warp") == 0) return false;
+  return nmode >= 16384;
 }
 
 // Record a profiling boundary: the work enqueued after it (until the next
@@ -238,10 +249,26 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   // y-operator tables go to the device chunk-major (see lmcd::tab)
   const int C = d.C, lpm = d.lpm, base = d.base, extra = d.extra, my = g.my;
   auto cm = [&](const std::vector<double> &T, int W) { return lmc::chunk_major(T, my, W, C, lpm, base, extra); };
+  d.tpm = mode_parallel(g.nmode);
   const size_t pm2 = (size_t)C * 2 * 32, pm3 = (size_t)C * 3 * 32;
-  std::vector<double> PLc((size_t)g.nmode * pm2), PUc((size_t)g.nmode * pm3), V12c((size_t)g.nmode * pm2);
+  const size_t nm = d.tpm ? 0 : (size_t)g.nmode;  // chunk-major per-mode tables: warp kernels only
+  std::vector<double> PLc(nm * pm2), PUc(nm * pm3), V12c(nm * pm2);
+  // mode-fastest per-mode tables [my][band][nmode]: mode-parallel kernels only
+  const size_t nt = d.tpm ? (size_t)g.nmode * my : 0;
+  std::vector<double> PLt(nt * 2), PUt(nt * 3), V12t(nt * 2);
+  if (d.tpm) {
+    const size_t n = (size_t)g.nmode;
 #pragma omp parallel for schedule(static)
-  for (int m = 0; m < g.nmode; m++) {
+    for (int j = 0; j < my; j++)
+      for (size_t m = 0; m < n; m++) {
+        const size_t src = m * my + j;
+        for (int c = 0; c < 2; c++) PLt[((size_t)j * 2 + c) * n + m] = h->pt.L[src * 2 + c];
+        for (int c = 0; c < 3; c++) PUt[((size_t)j * 3 + c) * n + m] = h->pt.U[src * 3 + c];
+        for (int c = 0; c < 2; c++) V12t[((size_t)j * 2 + c) * n + m] = h->pt.V12[src * 2 + c];
+      }
+  }
+#pragma omp parallel for schedule(static)
+  for (int m = 0; m < (int)nm; m++) {
     std::vector<double> a(h->pt.L.begin() + (size_t)m * my * 2, h->pt.L.begin() + (size_t)(m + 1) * my * 2);
     std::vector<double> b(h->pt.U.begin() + (size_t)m * my * 3, h->pt.U.begin() + (size_t)(m + 1) * my * 3);
     std::vector<double> v(h->pt.V12.begin() + (size_t)m * my * 2, h->pt.V12.begin() + (size_t)(m + 1) * my * 2);
@@ -262,6 +289,17 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
       (rc = dupload(h, &d.PL, PLc)) || (rc = dupload(h, &d.PU, PUc)) || (rc = dupload(h, &d.V12, V12c)) ||
       (rc = dupload(h, &d.AAinv, h->pt.AAinv)) || (rc = dupload(h, &d.k2, h->pt.k2)) || (rc = dupload(h, &d.kx, kx)) ||
       (rc = dupload(h, &d.kz, kz))) {
+    lmc_destroy(h);
+    return rc;
+  }
+  if (d.tpm &&
+      ((rc = dupload(h, &d.r_dt12, o.dt12)) || (rc = dupload(h, &d.r_dt11, o.dt11)) ||
+       (rc = dupload(h, &d.r_dt22, o.dt22)) || (rc = dupload(h, &d.r_dt21, o.dt21)) ||
+       (rc = dupload(h, &d.r_p1L, o.p1L)) || (rc = dupload(h, &d.r_p1U, o.p1U)) ||
+       (rc = dupload(h, &d.r_p3L, o.p3L)) || (rc = dupload(h, &d.r_p3U, o.p3U)) ||
+       (rc = dupload(h, &d.r_fmap, o.fmap)) || (rc = dupload(h, &d.r_ebot, o.ebot)) ||
+       (rc = dupload(h, &d.r_etop, o.etop)) || (rc = dupload(h, &d.PLt, PLt)) || (rc = dupload(h, &d.PUt, PUt)) ||
+       (rc = dupload(h, &d.V12t, V12t)))) {
     lmc_destroy(h);
     return rc;
   }
@@ -310,6 +348,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
       return rc;
     }
   }
+  if (d.tpm)
+    for (int q = 0; q < 4; q++)
+      if ((rc = dalloc(h, &d.ws[q], ns))) { lmc_destroy(h); return rc; }
   double **vec[] = {&d.u00, &d.v00, &d.w00, &d.rf0u, &d.rf0w, &d.rf0v, &d.rhom};
   for (auto q : vec)
     if ((rc = dalloc(h, q, (size_t)g.my))) { lmc_destroy(h); return rc; }
@@ -549,6 +590,18 @@ int lmc_query(lmc_handle *h) {
 
 size_t lmc_device_bytes(lmc_handle *h) { return h ? h->bytes : 0; }
 
+int lmc_launches_per_step(lmc_handle *h) {
+  if (!h) return LMC_EINVAL;
+  // per substep: lapv, assemble, tder, zinv, xphys, zfwd, post1, post2
+  // (two kernels in the warp family), psi; the mode-parallel family adds
+  // the 00 tails of post1 and psi and runs post2 as one kernel; the mixed
+  // forms add the plane-sum reduction after xphys
+  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0);
+  return 3 * per;
+}
+
+int lmc_y_family(lmc_handle *h) { return h ? h->d.tpm : LMC_EINVAL; }
+
 size_t lmc_footprint(const lmc_params *p) {
   if (!p || p->precision < 0 || p->precision > 2) return 0;
   lmc::Grid g;
@@ -558,8 +611,11 @@ size_t lmc_footprint(const lmc_params *p) {
   if (!lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) return 0;
   const size_t S = (size_t)g.nmode * g.my, Z = (size_t)g.nkx * g.my * g.mgalz;
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
-  size_t b = 6 * S * 16 + P * 8;                                  // state, R_om, R_phi, RHS(T)
-  b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8;  // per-mode Poisson tables
+  size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)
+  if (mode_parallel(g.nmode))
+    b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 4 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
+  else
+    b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8;  // per-mode Poisson tables
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
   else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;
   b += (size_t)C * 32 * 64 * 8 + 6 * 5 * 32 * 16 * 8 + (size_t)(g.mgalx + g.mgalz) * 24;  // y tables, twiddles

@@ -27,6 +27,14 @@ struct Dev {
   const double *fmap, *hy, *trp, *y, *ebot, *etop;
   // per-mode Poisson data
   const double *PL, *PU, *V12, *AAinv, *k2;
+  // Mode-parallel y kernels (tpm = 1, lmc_ytpm.cuh): the same operators in
+  // row form ([my][band], one row read by all threads of a warp), per-mode
+  // Poisson tables mode-fastest ([my][band][nmode]), and four FP64
+  // spectral scratch fields for the forward halves of the banded solves.
+  int tpm;
+  const double *r_dt12, *r_dt11, *r_dt22, *r_dt21, *r_p1L, *r_p1U, *r_p3L, *r_p3U, *r_fmap, *r_ebot, *r_etop;
+  const double *PLt, *PUt, *V12t;
+  double2 *ws[4];
   const double *kx, *kz;  // wavenumber per kx plane / kz index
   const double2 *twx, *twz;  // exp(-2 pi i e / N) for the x / z transform lengths
   const float2 *twxf, *twzf;  // the same in FP32 (mixed form)

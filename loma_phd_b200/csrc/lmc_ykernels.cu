@@ -54,17 +54,45 @@ __global__ void __launch_bounds__(256) k_dev2ref(int my, int nkx, int mz, const 
     LMC_YCASE(13, CALL) default : LMC_YCASE(17, CALL)                                         \
   }
 
-void launch_lapv(const Dev &d, cudaStream_t s) { LMC_YDISPATCH(lapv(d, s)) }
-void launch_assemble(const Dev &d, int rk, cudaStream_t s) { LMC_YDISPATCH(assemble(d, rk, s)) }
-void launch_tder(const Dev &d, cudaStream_t s) { LMC_YDISPATCH(tder(d, s)) }
-void launch_post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
-  LMC_YDISPATCH(post1(d, rk, do_cfl, do_diag, s))
+// d.tpm selects the mode-parallel kernels (lmc_ytpm.cu) over the
+// warp-per-mode ones; the 00-mode tails always run the warp code.
+void launch_lapv(const Dev &d, cudaStream_t s) {
+  if (d.tpm) tpm_lapv(d, s);
+  else LMC_YDISPATCH(lapv(d, s))
 }
-void launch_post2(const Dev &d, int rk, cudaStream_t s) { LMC_YDISPATCH(post2(d, rk, s)) }
+void launch_assemble(const Dev &d, int rk, cudaStream_t s) {
+  if (d.tpm) tpm_assemble(d, rk, s);
+  else LMC_YDISPATCH(assemble(d, rk, s))
+}
+void launch_tder(const Dev &d, cudaStream_t s) {
+  if (d.tpm) tpm_tder(d, s);
+  else LMC_YDISPATCH(tder(d, s))
+}
+void launch_post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+  if (d.tpm) {
+    tpm_post1(d, s);
+    LMC_YDISPATCH(post1_00(d, rk, do_cfl, do_diag, s))
+  } else {
+    LMC_YDISPATCH(post1(d, rk, do_cfl, do_diag, s))
+  }
+}
+void launch_post2(const Dev &d, int rk, cudaStream_t s) {
+  if (d.tpm) tpm_post2(d, rk, s);
+  else LMC_YDISPATCH(post2(d, rk, s))
+}
 void launch_psi(const Dev &d, int rk, int cfl_step, int do_diag, cudaStream_t s) {
-  LMC_YDISPATCH(psi(d, rk, cfl_step, do_diag, s))
+  if (d.tpm) {
+    tpm_psi(d, s);
+    LMC_YDISPATCH(psi_00(d, rk, cfl_step, s))
+  } else {
+    LMC_YDISPATCH(psi(d, rk, cfl_step, do_diag, s))
+  }
 }
 void launch_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s) {
+  if (d.tpm) {
+    tpm_op_y(d, op, in, out, out2, s);
+    return;
+  }
   switch (d.C) {
     case 4: YL<4, double2>::op_y(d, op, in, out, out2, s); break;
     case 5: YL<5, double2>::op_y(d, op, in, out, out2, s); break;

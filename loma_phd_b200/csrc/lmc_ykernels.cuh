@@ -337,67 +337,14 @@ __global__ void __launch_bounds__(TM * 32, 2) k_tder(Dev d) {
 // The 00 pencils of d(rho uv)/dy and d(rho vw)/dy are parked in rf0u and
 // rf0w until the 00 RHS replaces them at the end of the kernel.
 // ----------------------------------------------------------------------
+// 00 mode of post1 (block (0,0); warp 0 computes): dw, dm, masst, the
+// viscous 00 RHS of rho u00 / rho w00 (its d(rho uv)/dy, d(rho vw)/dy parts
+// parked in rf0u / rf0w), H00 and the CFL Deltat: cross.f:686-722,
+// 1416-1429, 1778-1826.  All threads of the block take part in the staging.
 template <int C, typename CT>
-__global__ void __launch_bounds__(TM * 32, 2) k_post1(Dev d, int rk, int do_cfl, int do_diag) {
-  YKERNEL_PROLOGUE
-  const double kx = __ldg(d.kx + T.i), kz = __ldg(d.kz + T.k);
-  const bool m00 = T.act && T.m == 0;
+__device__ __forceinline__ void post1_00(const Dev &d, const Tile &T, const Lane &L, double2 *S, int rk, int do_cfl,
+                                         int do_diag) {
   double2 a[C], b[C];
-  tload<C>(d, T, d.scal, S, L, a);
-  tstage(d, T, wsb<CT>(d, ODT), S);
-#pragma unroll
-  for (int t = 0; t < C; t++) {
-    double2 dT = sv(d, T, S, L, t);
-    if constexpr (is_mixed<CT>())
-      if (m00) dT = mo00(d, ODT, L, t);
-    a[t] = cadd(a[t], dT);  // cross.f:619-627
-  }
-  tstore<C>(d, T, d.scal, S, L, a);
-  // N_y = -ikx rho uv - d(rho vv)/dy - ikz rho vw
-  tload<C>(d, T, wsb<CT>(d, ORVV), S, L, a);
-  d1<C>(d, L, a);
-  tstage(d, T, wsb<CT>(d, ORUV), S);
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, sv(d, T, S, L, t))));
-  tstage(d, T, wsb<CT>(d, ORVW), S);
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, sv(d, T, S, L, t)));
-  tstore<C>(d, T, wsb<CT>(d, ORVV), S, L, a);
-  // N_x = -ikx rho uu - d(rho uv)/dy - ikz rho uw
-  tload<C>(d, T, wsb<CT>(d, ORUV), S, L, a);
-  if constexpr (is_mixed<CT>())
-    if (m00) load_mo00<C>(d, ORUV, L, a);
-  d1<C>(d, L, a);
-  if (m00) {
-#pragma unroll
-    for (int t = 0; t < C; t++)
-      if (t < L.n) d.rf0u[L.s + t] = a[t].x;
-  }
-  tstage(d, T, wsb<CT>(d, ORUU), S);
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, sv(d, T, S, L, t))));
-  tload<C>(d, T, wsb<CT>(d, ORUW), S, L, b);  // kept for N_z
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, b[t]));
-  tstore<C>(d, T, wsb<CT>(d, ORUU), S, L, a);
-  // N_z = -ikx rho uw - d(rho vw)/dy - ikz rho ww
-  tload<C>(d, T, wsb<CT>(d, ORVW), S, L, a);
-  if constexpr (is_mixed<CT>())
-    if (m00) load_mo00<C>(d, ORVW, L, a);
-  d1<C>(d, L, a);
-  if (m00) {
-#pragma unroll
-    for (int t = 0; t < C; t++)
-      if (t < L.n) d.rf0w[L.s + t] = a[t].x;
-  }
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, b[t])));
-  tstage(d, T, wsb<CT>(d, ORWW), S);
-#pragma unroll
-  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, sv(d, T, S, L, t)));
-  tstore<C>(d, T, wsb<CT>(d, ORWW), S, L, a);
-  if (!(blockIdx.x == 0 && blockIdx.y == 0)) return;
-  // ---- 00 mode: block (0,0), warp 0 ----
   tload<C>(d, T, wsb<CT>(d, OU), S, L, a);
   if (T.w != 0) return;
   if constexpr (is_mixed<CT>()) {  // the u pencil (and its staged copy) in FP64
@@ -477,6 +424,69 @@ __global__ void __launch_bounds__(TM * 32, 2) k_post1(Dev d, int rk, int do_cfl,
       d.scal_d[1] = (double)(float)(d.cfl / (cx + cy + cz + ct));  // dtr is real*4
     }
   }
+}
+
+template <int C, typename CT>
+__global__ void __launch_bounds__(TM * 32, 2) k_post1(Dev d, int rk, int do_cfl, int do_diag) {
+  YKERNEL_PROLOGUE
+  const double kx = __ldg(d.kx + T.i), kz = __ldg(d.kz + T.k);
+  const bool m00 = T.act && T.m == 0;
+  double2 a[C], b[C];
+  tload<C>(d, T, d.scal, S, L, a);
+  tstage(d, T, wsb<CT>(d, ODT), S);
+#pragma unroll
+  for (int t = 0; t < C; t++) {
+    double2 dT = sv(d, T, S, L, t);
+    if constexpr (is_mixed<CT>())
+      if (m00) dT = mo00(d, ODT, L, t);
+    a[t] = cadd(a[t], dT);  // cross.f:619-627
+  }
+  tstore<C>(d, T, d.scal, S, L, a);
+  // N_y = -ikx rho uv - d(rho vv)/dy - ikz rho vw
+  tload<C>(d, T, wsb<CT>(d, ORVV), S, L, a);
+  d1<C>(d, L, a);
+  tstage(d, T, wsb<CT>(d, ORUV), S);
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, sv(d, T, S, L, t))));
+  tstage(d, T, wsb<CT>(d, ORVW), S);
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, sv(d, T, S, L, t)));
+  tstore<C>(d, T, wsb<CT>(d, ORVV), S, L, a);
+  // N_x = -ikx rho uu - d(rho uv)/dy - ikz rho uw
+  tload<C>(d, T, wsb<CT>(d, ORUV), S, L, a);
+  if constexpr (is_mixed<CT>())
+    if (m00) load_mo00<C>(d, ORUV, L, a);
+  d1<C>(d, L, a);
+  if (m00) {
+#pragma unroll
+    for (int t = 0; t < C; t++)
+      if (t < L.n) d.rf0u[L.s + t] = a[t].x;
+  }
+  tstage(d, T, wsb<CT>(d, ORUU), S);
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, sv(d, T, S, L, t))));
+  tload<C>(d, T, wsb<CT>(d, ORUW), S, L, b);  // kept for N_z
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, b[t]));
+  tstore<C>(d, T, wsb<CT>(d, ORUU), S, L, a);
+  // N_z = -ikx rho uw - d(rho vw)/dy - ikz rho ww
+  tload<C>(d, T, wsb<CT>(d, ORVW), S, L, a);
+  if constexpr (is_mixed<CT>())
+    if (m00) load_mo00<C>(d, ORVW, L, a);
+  d1<C>(d, L, a);
+  if (m00) {
+#pragma unroll
+    for (int t = 0; t < C; t++)
+      if (t < L.n) d.rf0w[L.s + t] = a[t].x;
+  }
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(czero(), cadd(a[t], cik(kx, b[t])));
+  tstage(d, T, wsb<CT>(d, ORWW), S);
+#pragma unroll
+  for (int t = 0; t < C; t++) a[t] = csub(a[t], cik(kz, sv(d, T, S, L, t)));
+  tstore<C>(d, T, wsb<CT>(d, ORWW), S, L, a);
+  if (!(blockIdx.x == 0 && blockIdx.y == 0)) return;
+  post1_00<C, CT>(d, T, L, S, rk, do_cfl, do_diag);
 }
 
 // ----------------------------------------------------------------------
@@ -563,23 +573,16 @@ __global__ void __launch_bounds__(TM * 32, 2) k_post2b(Dev d, int rk) {
 // then advances the 00 modes and integrates d(rho)/dt for rho v00
 // (cross.f:1006-1074).
 // ----------------------------------------------------------------------
+// 00 mode of the psi stage (block (0,0); warp 0 computes): rho u00 / rho
+// w00 RK3 update, masses, inty8 of d(rho)/dt00 for rho v00 with the
+// acoustic wall correction, end-of-step time and Deltat: cross.f:1006-1074,
+// 1196-1204.  All threads of the block take part in the staging.
 template <int C, typename CT>
-__global__ void __launch_bounds__(TM * 32, 2) k_psi(Dev d, int rk, int cfl_step, int do_diag) {
-  YKERNEL_PROLOGUE
+__device__ __forceinline__ void psi_00(const Dev &d, const Tile &T, const Lane &L, double2 *S, int rk, int cfl_step) {
   double2 a[C];
-  tload<C>(d, T, wsb<CT>(d, ODRHO), S, L, a);
-  const bool zero = (__ldg(d.k2 + T.m) == 0.0);
-  neumann<C>(d, L, T.m, a);
-  if (zero) {
-#pragma unroll
-    for (int t = 0; t < C; t++) a[t] = czero();
-  }
-  tstore<C>(d, T, d.psi, S, L, a);
-  if (!(blockIdx.x == 0 && blockIdx.y == 0)) return;
   tload<C>(d, T, wsb<CT>(d, ODRHO), S, L, a);
   if (T.w != 0) return;
   if constexpr (is_mixed<CT>()) load_mo00<C>(d, ODRHO, L, a);
-  (void)do_diag;
   const double dt = d.scal_d[0], dtg = dt * d.gama[rk];
   double mu = 0.0, mv = 0.0, mw = 0.0;
 #pragma unroll
@@ -623,6 +626,35 @@ __global__ void __launch_bounds__(TM * 32, 2) k_psi(Dev d, int rk, int cfl_step,
       d.diag[12] = d.scal_d[0];
     }
   }
+}
+
+template <int C, typename CT>
+__global__ void __launch_bounds__(TM * 32, 2) k_psi(Dev d, int rk, int cfl_step, int do_diag) {
+  YKERNEL_PROLOGUE
+  double2 a[C];
+  tload<C>(d, T, wsb<CT>(d, ODRHO), S, L, a);
+  const bool zero = (__ldg(d.k2 + T.m) == 0.0);
+  neumann<C>(d, L, T.m, a);
+  if (zero) {
+#pragma unroll
+    for (int t = 0; t < C; t++) a[t] = czero();
+  }
+  tstore<C>(d, T, d.psi, S, L, a);
+  if (!(blockIdx.x == 0 && blockIdx.y == 0)) return;
+  psi_00<C, CT>(d, T, L, S, rk, cfl_step);
+}
+
+// the 00-mode tails alone (one block), after the mode-parallel kernels of
+// lmc_ytpm.cuh
+template <int C, typename CT>
+__global__ void __launch_bounds__(TM * 32, 1) k_post1_00(Dev d, int rk, int do_cfl, int do_diag) {
+  YKERNEL_PROLOGUE
+  post1_00<C, CT>(d, T, L, S, rk, do_cfl, do_diag);
+}
+template <int C, typename CT>
+__global__ void __launch_bounds__(TM * 32, 1) k_psi_00(Dev d, int rk, int cfl_step) {
+  YKERNEL_PROLOGUE
+  psi_00<C, CT>(d, T, L, S, rk, cfl_step);
 }
 
 // single-operator kernel (tests), device layout
@@ -689,6 +721,14 @@ void YL<C, CT>::psi(const Dev &d, int rk, int cfl_step, int do_diag, cudaStream_
   LMC_YL((k_psi<C, CT>), d, rk, cfl_step, do_diag);
 }
 template <int C, typename CT>
+void YL<C, CT>::post1_00(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+  k_post1_00<C, CT><<<dim3(1, 1), TM * 32, ysmem(d), s>>>(d, rk, do_cfl, do_diag);
+}
+template <int C, typename CT>
+void YL<C, CT>::psi_00(const Dev &d, int rk, int cfl_step, cudaStream_t s) {
+  k_psi_00<C, CT><<<dim3(1, 1), TM * 32, ysmem(d), s>>>(d, rk, cfl_step);
+}
+template <int C, typename CT>
 void YL<C, CT>::op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s) {
   LMC_YL(k_op_y<C>, d, op, in, out, out2);
 }
@@ -696,7 +736,8 @@ template <int C, typename CT>
 cudaError_t YL<C, CT>::optin(int limit) {
   const void *fns[] = {(const void *)k_lapv<C, CT>, (const void *)k_assemble<C, CT>, (const void *)k_tder<C, CT>,
                        (const void *)k_post1<C, CT>, (const void *)k_post2a<C, CT>, (const void *)k_post2b<C, CT>,
-                       (const void *)k_psi<C, CT>, (const void *)k_op_y<C>};
+                       (const void *)k_psi<C, CT>, (const void *)k_op_y<C>, (const void *)k_post1_00<C, CT>,
+                       (const void *)k_psi_00<C, CT>};
   for (const void *fn : fns) {
     const cudaError_t e = yoptin(fn, limit);
     if (e != cudaSuccess) return e;

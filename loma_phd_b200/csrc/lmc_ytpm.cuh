@@ -1,0 +1,744 @@
+// lmc_ytpm.cuh -- mode-parallel y kernels: one thread per (kx,kz) mode.
+//
+// In the spectral layout [y][kx][kz] the value of mode m at row j sits at
+// f[j*nmode + m], so the threads of a warp (32 consecutive modes) read and
+// write every row of their pencils as one coalesced 32-value run, and the
+// coefficients of a row are the same for the whole warp (one broadcast
+// load).  Each banded solve A x = b with A = L U (the LU of cfdiff.f /
+// laps.f in row form) runs as two sweeps along y: the forward sweep forms
+// the band product of the right-hand side and applies L^-1, writing the
+// intermediate pencil to an FP64 scratch field; the backward sweep reads it
+// in reverse and applies U^-1.  Fields are streamed through a small queue
+// of registers that is refilled K rows ahead of use, so every thread keeps
+// several loads in flight.  Kernels follow the same statements of
+// trunk/lomacte3/src/cross.f:307-1141 as the warp-per-mode kernels of
+// lmc_ykernels.cuh (which keep serving small grids and the 00-mode tails).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lmc_kernels.cuh"
+
+namespace lmc {
+namespace tpm {
+
+using namespace lmcd;
+
+constexpr int TB = 128;  // modes per block
+
+template <typename CT>
+__host__ __device__ constexpr bool mixed() { return sizeof(CT) == sizeof(float2); }
+
+// Prefetching reader of one pencil, walking rows first, first+dir, ...
+// Loads go through L2 (ld.global.cg), never the non-coherent read-only
+// path: a kernel reads back scratch pencils and fields it wrote itself.
+template <typename PT, int K>
+struct Rd {
+  const PT *p;
+  size_t ld;
+  int my, dir, nxt;
+  PT q[K];
+  __device__ __forceinline__ PT fetch(int r) const {
+    PT z;
+    z.x = 0;
+    z.y = 0;
+    return (r >= 0 && r < my) ? __ldcg(p + (size_t)r * ld) : z;
+  }
+  __device__ __forceinline__ void start(const PT *base, size_t ld_, int my_, int dir_, int first) {
+    p = base;
+    ld = ld_;
+    my = my_;
+    dir = dir_;
+    nxt = first;
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+      q[t] = fetch(nxt);
+      nxt += dir;
+    }
+  }
+  __device__ __forceinline__ double2 pop() {
+    const double2 v = to_d2(q[0]);
+#pragma unroll
+    for (int t = 0; t < K - 1; t++) q[t] = q[t + 1];
+    q[K - 1] = fetch(nxt);
+    nxt += dir;
+    return v;
+  }
+};
+
+template <typename PT>
+__device__ __forceinline__ void put(PT *base, size_t ld, int j, double2 v) {
+  base[(size_t)j * ld] = from_d2<PT>(v);
+}
+
+// u_{j-3} .. u_{j+3} around the current row j
+struct Win {
+  double2 u[7];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int t = 0; t < 7; t++) u[t] = czero();
+  }
+  __device__ __forceinline__ void push(double2 v) {
+#pragma unroll
+    for (int t = 0; t < 6; t++) u[t] = u[t + 1];
+    u[6] = v;
+  }
+  __device__ __forceinline__ double2 c() const { return u[3]; }
+};
+
+// the last three results of a sweep (x_{j-+1}, x_{j-+2}, x_{j-+3})
+struct Hist {
+  double2 a, b, c;
+  __device__ __forceinline__ void clear() { a = b = c = czero(); }
+  __device__ __forceinline__ void push(double2 v) {
+    c = b;
+    b = a;
+    a = v;
+  }
+};
+
+__device__ __forceinline__ double2 fms(double2 s, double k, double2 v) {  // s - k v
+  return make_double2(fma(-k, v.x, s.x), fma(-k, v.y, s.y));
+}
+
+// forward half of d/dy (deryr2, cfdiff.f:518-601): w_j = (L1^-1 dt12 u)_j
+__device__ __forceinline__ double2 d1f(const Dev &d, int j, const Win &u, Hist &h) {
+  const double *c = d.r_dt12 + 7 * j;
+  double2 r = czero();
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    const double k = __ldg(c + t);
+    r.x = fma(k, u.u[t].x, r.x);
+    r.y = fma(k, u.u[t].y, r.y);
+  }
+  const double *l = d.r_p1L + 3 * j;
+  r = fms(fms(fms(r, __ldg(l + 2), h.c), __ldg(l + 1), h.b), __ldg(l), h.a);
+  h.push(r);
+  return r;
+}
+// backward half of d/dy: x_j = (U1^-1 w)_j times fmap_j
+__device__ __forceinline__ double2 d1b(const Dev &d, int j, double2 w, Hist &h) {
+  const double *u = d.r_p1U + 4 * j;
+  double2 x = fms(fms(fms(w, __ldg(u + 3), h.c), __ldg(u + 2), h.b), __ldg(u + 1), h.a);
+  x = cscale(__ldg(u), x);
+  h.push(x);
+  return cscale(__ldg(d.r_fmap + j), x);
+}
+// forward half of d2/dy2 (deryyr2, cfdiff.f:735-797)
+__device__ __forceinline__ double2 d2f(const Dev &d, int j, const Win &u, Hist &h) {
+  const double *c = d.r_dt22 + 5 * j;
+  double2 r = czero();
+#pragma unroll
+  for (int t = 0; t < 5; t++) {
+    const double k = __ldg(c + t);
+    r.x = fma(k, u.u[t + 1].x, r.x);
+    r.y = fma(k, u.u[t + 1].y, r.y);
+  }
+  const double *l = d.r_p3L + 2 * j;
+  r = fms(fms(r, __ldg(l + 1), h.b), __ldg(l), h.a);
+  h.push(r);
+  return r;
+}
+__device__ __forceinline__ double2 d2b(const Dev &d, int j, double2 w, Hist &h) {
+  const double *u = d.r_p3U + 3 * j;
+  double2 x = fms(fms(w, __ldg(u + 2), h.b), __ldg(u + 1), h.a);
+  x = cscale(__ldg(u), x);
+  h.push(x);
+  return x;
+}
+// Dirichlet Poisson of mode m (laps.f:375-401): right-hand side dt21 f with
+// zero wall rows, then the mode's LU (dt22 - k^2 dt21 with identity rows)
+__device__ __forceinline__ double2 pf(const Dev &d, int j, const Win &u, Hist &h, int m) {
+  double2 r = czero();
+  if (j > 0 && j < d.my - 1) {
+    const double *c = d.r_dt21 + 5 * j;
+#pragma unroll
+    for (int t = 0; t < 5; t++) {
+      const double k = __ldg(c + t);
+      r.x = fma(k, u.u[t + 1].x, r.x);
+      r.y = fma(k, u.u[t + 1].y, r.y);
+    }
+  }
+  const size_t n = (size_t)d.nmode, b = (size_t)j * 2 * n + m;
+  r = fms(fms(r, __ldg(d.PLt + b + n), h.b), __ldg(d.PLt + b), h.a);
+  h.push(r);
+  return r;
+}
+__device__ __forceinline__ double2 pb(const Dev &d, int j, double2 w, Hist &h, int m) {
+  const size_t n = (size_t)d.nmode, b = (size_t)j * 3 * n + m;
+  double2 x = fms(fms(w, __ldg(d.PUt + b + 2 * n), h.b), __ldg(d.PUt + b + n), h.a);
+  x = cscale(__ldg(d.PUt + b), x);
+  h.push(x);
+  return x;
+}
+
+struct Mode {
+  int m;
+  double kx, kz, k2;
+};
+__device__ __forceinline__ bool mode_of(const Dev &d, Mode &M) {
+  M.m = blockIdx.x * TB + threadIdx.x;
+  if (M.m >= d.nmode) return false;
+  const int i = M.m / d.mz, k = M.m - i * d.mz;
+  M.kx = __ldg(d.kx + i);
+  M.kz = __ldg(d.kz + k);
+  M.k2 = __ldg(d.k2 + M.m);
+  return true;
+}
+
+// the exact (FP64) 00 coefficient of transform output o at row j (mixed forms)
+__device__ __forceinline__ double2 mo00_row(const Dev &d, int o, int j) {
+  return make_double2(d.mo_cur[(size_t)o * d.my + j] / ((double)d.mgalx * (double)d.mgalz), 0.0);
+}
+
+// ----------------------------------------------------------------------
+// (1) Lapvdvhom: phi -> m_y, dm_y/dy (cross.f:329-335, 365-372)
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_lapv(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool zero = M.k2 == 0.0;
+  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m;
+  CT *MY = wsb<CT>(d, SB_MY) + M.m, *DMY = wsb<CT>(d, SB_DMY) + M.m;
+  {  // forward Poisson half; phi with its wall values set to zero
+    Rd<double2, 8> r;
+    r.start(d.phi + M.m, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) {
+      const double2 v = r.pop();
+      w.push(t == 0 ? czero() : v);
+    }
+    for (int j = 0; j < my; j++) {
+      const double2 v = r.pop();
+      w.push(j + 3 == my - 1 ? czero() : v);
+      s1[(size_t)j * ld] = pf(d, j, w, h, M.m);
+    }
+  }
+  {  // backward Poisson half -> m_y
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      double2 x = pb(d, j, r.pop(), h, M.m);
+      if (zero) x = czero();
+      put(MY, ld, j, x);
+      s2[(size_t)j * ld] = x;
+    }
+  }
+  {  // forward half of d/dy of m_y
+    Rd<double2, 8> r;
+    r.start(s2, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) w.push(r.pop());
+    for (int j = 0; j < my; j++) {
+      w.push(r.pop());
+      s1[(size_t)j * ld] = d1f(d, j, w, h);
+    }
+  }
+  {  // backward half -> dm_y/dy
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) put(DMY, ld, j, d1b(d, j, r.pop(), h));
+  }
+}
+
+// ----------------------------------------------------------------------
+// (2)-(3) m_x, m_z, rho u_i, xi-updates of Omega_y and phi, 00 modes
+// (cross.f:315-327, 395-499)
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const double dtxi = d.scal_d[0] * d.xi[rk];
+  const double ta = (M.k2 != 0.0) ? M.kx / M.k2 : 0.0, tb = (M.k2 != 0.0) ? M.kz / M.k2 : 0.0;
+  const bool m00 = M.m == 0;
+  double2 *s1 = d.ws[0] + M.m;
+  {
+    Rd<double2, 3> rvor, rrom, rphi, rrph;
+    Rd<CT, 3> rdmy;
+    Rd<double2, 4> rpsi;
+    rvor.start(d.vor + M.m, ld, my, 1, 0);
+    rrom.start(d.Rom + M.m, ld, my, 1, 0);
+    rphi.start(d.phi + M.m, ld, my, 1, 0);
+    rrph.start(d.Rphi + M.m, ld, my, 1, 0);
+    rdmy.start(wsb<CT>(d, SB_DMY) + M.m, ld, my, 1, 0);
+    rpsi.start(d.psi + M.m, ld, my, 1, 0);
+    CT *RU = wsb<CT>(d, SB_RU) + M.m, *RW = wsb<CT>(d, SB_RW) + M.m;
+    const double2 vor1 = __ldg(d.vor + ld + M.m);  // wall BC of Omega_y, cross.f:315-327
+    double2 vprev = czero();
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) w.push(rpsi.pop());
+    for (int j = 0; j < my; j++) {
+      w.push(rpsi.pop());
+      const double2 ps = w.c();
+      const double2 vr = rvor.pop();
+      const double2 vo = (j == 0) ? vor1 : (j == my - 1) ? vprev : vr;
+      vprev = vr;
+      const double2 a = rdmy.pop();
+      double2 b = cadd(csub(cik(ta, a), cik(tb, vo)), cik(M.kx, ps));   // rho u, cross.f:402,467
+      double2 c = cadd(cadd(cik(tb, a), cik(ta, vo)), cik(M.kz, ps));   // rho w, cross.f:404,469
+      if (m00) {  // 00 modes injected (cross.f:486-491), then u00**, w00** (cross.f:495-498)
+        b = make_double2(d.u00[j], 0.0);
+        c = make_double2(d.w00[j], 0.0);
+        if constexpr (mixed<CT>()) {
+          d.mi[j] = b.x;
+          d.mi[(size_t)2 * my + j] = c.x;
+        }
+        if (j >= 1 && j <= my - 2) {
+          d.u00[j] += dtxi * d.rf0u[j];
+          d.w00[j] += dtxi * d.rf0w[j];
+        }
+      }
+      put(RU, ld, j, b);
+      put(RW, ld, j, c);
+      put(d.vor + M.m, ld, j, cadd(vo, cscale(dtxi, rrom.pop())));  // cross.f:420-424
+      double2 ph = rphi.pop();
+      if (j == 0 || j == my - 1) ph = czero();
+      put(d.phi + M.m, ld, j, cadd(ph, cscale(dtxi, rrph.pop())));  // cross.f:424-425
+      s1[(size_t)j * ld] = d1f(d, j, w, h);
+    }
+  }
+  {  // rho v = m_y + d(psi)/dy (cross.f:434-437, 471)
+    Rd<double2, 4> r;
+    Rd<CT, 4> rmy;
+    r.start(s1, ld, my, -1, my - 1);
+    rmy.start(wsb<CT>(d, SB_MY) + M.m, ld, my, -1, my - 1);
+    CT *RV = wsb<CT>(d, SB_RV) + M.m;
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      double2 a = cadd(d1b(d, j, r.pop(), h), rmy.pop());
+      if (m00) {
+        a = make_double2(d.v00[j], 0.0);
+        if constexpr (mixed<CT>()) d.mi[(size_t)my + j] = a.x;
+      }
+      put(RV, ld, j, a);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
+// (4) T with its wall BCs, dT/dy, lap(T) (cross.f:336-349, 521-541)
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_tder(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool m00 = M.m == 0;
+  const double2 wb = m00 ? make_double2(1.0 / d.scal_d[3], 0.0) : czero();
+  const double2 wt = m00 ? make_double2(1.0 / d.scal_d[4], 0.0) : czero();
+  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m;
+  {
+    Rd<double2, 8> r;
+    r.start(d.scal + M.m, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h1, h2;
+    h1.clear();
+    h2.clear();
+    for (int t = 0; t < 3; t++) {
+      const double2 v = r.pop();
+      w.push(t == 0 ? wb : v);
+    }
+    for (int j = 0; j < my; j++) {
+      const double2 v = r.pop();
+      w.push(j + 3 == my - 1 ? wt : v);
+      const double2 T = w.c();
+      put(d.scal + M.m, ld, j, T);
+      if constexpr (mixed<CT>()) {
+        put(wsb<CT>(d, SB_T32) + M.m, ld, j, T);
+        if (m00) d.mi[(size_t)5 * my + j] = T.x;
+      }
+      s1[(size_t)j * ld] = d1f(d, j, w, h1);
+      s2[(size_t)j * ld] = d2f(d, j, w, h2);
+    }
+  }
+  {
+    Rd<double2, 4> r1, r2, rT;
+    r1.start(s1, ld, my, -1, my - 1);
+    r2.start(s2, ld, my, -1, my - 1);
+    rT.start(d.scal + M.m, ld, my, -1, my - 1);
+    CT *DY = wsb<CT>(d, SB_DTDY) + M.m, *LT = wsb<CT>(d, SB_LAPT) + M.m;
+    Hist h1, h2;
+    h1.clear();
+    h2.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 dT = d1b(d, j, r1.pop(), h1);
+      const double2 lT = csub(d2b(d, j, r2.pop(), h2), cscale(M.k2, rT.pop()));
+      if constexpr (mixed<CT>())
+        if (m00) {
+          d.mi[(size_t)4 * my + j] = dT.x;
+          d.mi[(size_t)3 * my + j] = lT.x;
+        }
+      put(DY, ld, j, dT);
+      put(LT, ld, j, lT);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
+// (6a)-(6b) T update and N_i (cross.f:619-682); rf0u / rf0w get the 00
+// pencils of d(rho uv)/dy and d(rho vw)/dy for the 00 tail.
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_post1(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool m00 = M.m == 0;
+  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m, *s3 = d.ws[2] + M.m;
+  {
+    Rd<double2, 2> rT;
+    Rd<CT, 2> rDT;
+    Rd<CT, 3> rvv, ruv, rvw;
+    rT.start(d.scal + M.m, ld, my, 1, 0);
+    rDT.start(wsb<CT>(d, ODT) + M.m, ld, my, 1, 0);
+    rvv.start(wsb<CT>(d, ORVV) + M.m, ld, my, 1, 0);
+    ruv.start(wsb<CT>(d, ORUV) + M.m, ld, my, 1, 0);
+    rvw.start(wsb<CT>(d, ORVW) + M.m, ld, my, 1, 0);
+    Win wvv, wuv, wvw;
+    wvv.clear();
+    wuv.clear();
+    wvw.clear();
+    Hist h1, h2, h3;
+    h1.clear();
+    h2.clear();
+    h3.clear();
+    auto feed = [&](int r) {  // row r of the three derivative inputs
+      double2 a = rvv.pop(), b = ruv.pop(), c = rvw.pop();
+      if constexpr (mixed<CT>())
+        if (m00 && r < my) {
+          b = mo00_row(d, ORUV, r);
+          c = mo00_row(d, ORVW, r);
+        }
+      wvv.push(a);
+      wuv.push(b);
+      wvw.push(c);
+    };
+    for (int t = 0; t < 3; t++) feed(t);
+    for (int j = 0; j < my; j++) {
+      feed(j + 3);
+      double2 dT = rDT.pop();
+      if constexpr (mixed<CT>())
+        if (m00) dT = mo00_row(d, ODT, j);
+      put(d.scal + M.m, ld, j, cadd(rT.pop(), dT));  // cross.f:619-627
+      s1[(size_t)j * ld] = d1f(d, j, wvv, h1);
+      s2[(size_t)j * ld] = d1f(d, j, wuv, h2);
+      s3[(size_t)j * ld] = d1f(d, j, wvw, h3);
+    }
+  }
+  {
+    Rd<double2, 2> r1, r2, r3;
+    Rd<CT, 2> ruv, rvw, ruu, ruw, rww;
+    r1.start(s1, ld, my, -1, my - 1);
+    r2.start(s2, ld, my, -1, my - 1);
+    r3.start(s3, ld, my, -1, my - 1);
+    CT *VV = wsb<CT>(d, ORVV) + M.m, *UU = wsb<CT>(d, ORUU) + M.m, *WW = wsb<CT>(d, ORWW) + M.m;
+    ruv.start(wsb<CT>(d, ORUV) + M.m, ld, my, -1, my - 1);
+    rvw.start(wsb<CT>(d, ORVW) + M.m, ld, my, -1, my - 1);
+    ruu.start(UU, ld, my, -1, my - 1);
+    ruw.start(wsb<CT>(d, ORUW) + M.m, ld, my, -1, my - 1);
+    rww.start(WW, ld, my, -1, my - 1);
+    Hist h1, h2, h3;
+    h1.clear();
+    h2.clear();
+    h3.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 dvv = d1b(d, j, r1.pop(), h1), duv = d1b(d, j, r2.pop(), h2), dvw = d1b(d, j, r3.pop(), h3);
+      const double2 uv = ruv.pop(), vw = rvw.pop(), uu = ruu.pop(), uw = ruw.pop(), ww = rww.pop();
+      if (m00) {
+        d.rf0u[j] = duv.x;
+        d.rf0w[j] = dvw.x;
+      }
+      put(VV, ld, j, csub(czero(), cadd(cadd(dvv, cik(M.kx, uv)), cik(M.kz, vw))));  // N_y
+      put(UU, ld, j, csub(czero(), cadd(cadd(duv, cik(M.kx, uu)), cik(M.kz, uw))));  // N_x
+      put(WW, ld, j, csub(czero(), cadd(cadd(dvw, cik(M.kx, uw)), cik(M.kz, ww))));  // N_z
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
+// (6c)-(9) vorticity, the two Laplacians, RHS(Omega_y), RHS(phi) and the
+// RK3 update (cross.f:748-981)
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const double kx = M.kx, kz = M.kz, k2 = M.k2;
+  const double dtg = d.scal_d[0] * d.gama[rk];
+  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m, *s3 = d.ws[2] + M.m, *s4 = d.ws[3] + M.m;
+  {  // forward halves of dw/dy, du/dy and d2(omega_y)/dy2
+    Rd<CT, 4> ru, rw;
+    ru.start(wsb<CT>(d, OU) + M.m, ld, my, 1, 0);
+    rw.start(wsb<CT>(d, OW) + M.m, ld, my, 1, 0);
+    Win wu, ww, wy;
+    wu.clear();
+    ww.clear();
+    wy.clear();
+    Hist h1, h2, h3;
+    h1.clear();
+    h2.clear();
+    h3.clear();
+    auto feed = [&]() {
+      const double2 u = ru.pop(), w = rw.pop();
+      wu.push(u);
+      ww.push(w);
+      wy.push(csub(cik(kz, u), cik(kx, w)));  // omega_y, cross.f:760
+    };
+    for (int t = 0; t < 3; t++) feed();
+    for (int j = 0; j < my; j++) {
+      feed();
+      s1[(size_t)j * ld] = d1f(d, j, ww, h1);
+      s2[(size_t)j * ld] = d1f(d, j, wu, h2);
+      s3[(size_t)j * ld] = d2f(d, j, wy, h3);
+    }
+  }
+  {  // forward half of d/dy of i kx N_x + i kz N_z (cross.f:900-907)
+    Rd<CT, 4> rx, rz;
+    rx.start(wsb<CT>(d, ORUU) + M.m, ld, my, 1, 0);
+    rz.start(wsb<CT>(d, ORWW) + M.m, ld, my, 1, 0);
+    Win wc;
+    wc.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) wc.push(cadd(cik(kx, rx.pop()), cik(kz, rz.pop())));
+    for (int j = 0; j < my; j++) {
+      wc.push(cadd(cik(kx, rx.pop()), cik(kz, rz.pop())));
+      s4[(size_t)j * ld] = d1f(d, j, wc, h);
+    }
+  }
+  {  // omega_x, omega_z, (curl omega)_y -> s1
+    Rd<double2, 4> r1, r2;
+    Rd<CT, 4> rv;
+    r1.start(s1, ld, my, -1, my - 1);
+    r2.start(s2, ld, my, -1, my - 1);
+    rv.start(wsb<CT>(d, OV) + M.m, ld, my, -1, my - 1);
+    Hist h1, h2;
+    h1.clear();
+    h2.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 dw = d1b(d, j, r1.pop(), h1), du = d1b(d, j, r2.pop(), h2), v = rv.pop();
+      const double2 ox = csub(dw, cik(kz, v));                 // cross.f:757
+      const double2 oz = csub(cik(kx, v), du);                 // cross.f:763
+      s1[(size_t)j * ld] = csub(cik(kz, ox), cik(kx, oz));     // cross.f:839
+    }
+  }
+  {  // RHS(Omega_y), Omega_y update; d/dy part of RHS(phi) (cross.f:885-917, 966-981)
+    Rd<double2, 2> r3, r4, rvo;
+    Rd<CT, 2> ru, rw, rx, rz, ry;
+    r3.start(s3, ld, my, -1, my - 1);
+    r4.start(s4, ld, my, -1, my - 1);
+    rvo.start(d.vor + M.m, ld, my, -1, my - 1);
+    ru.start(wsb<CT>(d, OU) + M.m, ld, my, -1, my - 1);
+    rw.start(wsb<CT>(d, OW) + M.m, ld, my, -1, my - 1);
+    rx.start(wsb<CT>(d, ORUU) + M.m, ld, my, -1, my - 1);
+    rz.start(wsb<CT>(d, ORWW) + M.m, ld, my, -1, my - 1);
+    ry.start(wsb<CT>(d, ORVV) + M.m, ld, my, -1, my - 1);
+    Hist h3, h4;
+    h3.clear();
+    h4.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 u = ru.pop(), w = rw.pop(), nx = rx.pop(), nz = rz.pop(), ny = ry.pop();
+      const double2 oy = csub(cik(kz, u), cik(kx, w));
+      const double2 lw = csub(d2b(d, j, r3.pop(), h3), cscale(k2, oy));                   // cross.f:822-832
+      const double2 rom = cadd(csub(cik(kz, nx), cik(kx, nz)), cscale(d.ire, lw));        // cross.f:889
+      put(d.Rom + M.m, ld, j, rom);
+      put(d.vor + M.m, ld, j, cadd(rvo.pop(), cscale(dtg, rom)));                         // cross.f:969
+      const double2 dc = d1b(d, j, r4.pop(), h4);
+      put(d.Rphi + M.m, ld, j, csub(cscale(-k2, ny), dc));
+    }
+  }
+  {  // forward half of d2/dy2 of (curl omega)_y
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) w.push(r.pop());
+    for (int j = 0; j < my; j++) {
+      w.push(r.pop());
+      s2[(size_t)j * ld] = d2f(d, j, w, h);
+    }
+  }
+  {  // lap(curl omega)_y, RHS(phi), phi update (cross.f:847-857, 917, 978)
+    Rd<double2, 3> r2, rc, rrp, rph;
+    r2.start(s2, ld, my, -1, my - 1);
+    rc.start(s1, ld, my, -1, my - 1);
+    rrp.start(d.Rphi + M.m, ld, my, -1, my - 1);
+    rph.start(d.phi + M.m, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 lc = csub(d2b(d, j, r2.pop(), h), cscale(k2, rc.pop()));
+      const double2 rp = csub(rrp.pop(), cscale(d.ire, lc));
+      put(d.Rphi + M.m, ld, j, rp);
+      put(d.phi + M.m, ld, j, cadd(rph.pop(), cscale(dtg, rp)));
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
+// (8) psi^{n+1} by solvepsi (cross.f:1092-1104, laps.f:580-730)
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_psi(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  double2 *s1 = d.ws[0] + M.m;
+  {
+    Rd<CT, 8> r;
+    r.start(wsb<CT>(d, ODRHO) + M.m, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) w.push(r.pop());
+    for (int j = 0; j < my; j++) {
+      w.push(r.pop());
+      s1[(size_t)j * ld] = pf(d, j, w, h, M.m);
+    }
+  }
+  double2 db = czero(), dt = czero();
+  {
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 x = pb(d, j, r.pop(), h, M.m);
+      const double eb = __ldg(d.r_ebot + j), et = __ldg(d.r_etop + j);
+      db.x = fma(eb, x.x, db.x);
+      db.y = fma(eb, x.y, db.y);
+      dt.x = fma(et, x.x, dt.x);
+      dt.y = fma(et, x.y, dt.y);
+      s1[(size_t)j * ld] = x;
+    }
+  }
+  {  // Neumann walls through the homogeneous solutions (laps.f:700-730)
+    const double *ai = d.AAinv + (size_t)M.m * 4;
+    const double a0 = __ldg(ai), a1 = __ldg(ai + 1), a2 = __ldg(ai + 2), a3 = __ldg(ai + 3);
+    const double2 c1 = make_double2(-(a0 * db.x + a1 * dt.x), -(a0 * db.y + a1 * dt.y));
+    const double2 c2 = make_double2(-(a2 * db.x + a3 * dt.x), -(a2 * db.y + a3 * dt.y));
+    const bool zero = M.k2 == 0.0;
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, 1, 0);
+    const size_t n = (size_t)d.nmode;
+    for (int j = 0; j < my; j++) {
+      double2 x = r.pop();
+      const double v1 = __ldg(d.V12t + (size_t)j * 2 * n + M.m), v2 = __ldg(d.V12t + (size_t)j * 2 * n + n + M.m);
+      x.x += c1.x * v1 + c2.x * v2;
+      x.y += c1.y * v1 + c2.y * v2;
+      put(d.psi + M.m, ld, j, zero ? czero() : x);
+    }
+  }
+}
+
+// single y operator on FP64 device-layout fields (tests): 1 d/dy, 2 d2/dy2,
+// 3 Lapvdvhom (out = v, out2 = dv/dy), 4 solvepsi
+__global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, double2 *out, double2 *out2) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool zero = M.k2 == 0.0;
+  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m;
+  in += M.m;
+  out += M.m;
+  {
+    Rd<double2, 8> r;
+    r.start(in, ld, my, 1, 0);
+    Win w;
+    w.clear();
+    Hist h;
+    h.clear();
+    for (int t = 0; t < 3; t++) w.push(r.pop());
+    for (int j = 0; j < my; j++) {
+      w.push(r.pop());
+      s1[(size_t)j * ld] = op == 1 ? d1f(d, j, w, h) : op == 2 ? d2f(d, j, w, h) : pf(d, j, w, h, M.m);
+    }
+  }
+  double2 db = czero(), dt = czero();
+  {
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 w = r.pop();
+      double2 x = op == 1 ? d1b(d, j, w, h) : op == 2 ? d2b(d, j, w, h) : pb(d, j, w, h, M.m);
+      if (op == 4) {
+        const double eb = __ldg(d.r_ebot + j), et = __ldg(d.r_etop + j);
+        db.x = fma(eb, x.x, db.x);
+        db.y = fma(eb, x.y, db.y);
+        dt.x = fma(et, x.x, dt.x);
+        dt.y = fma(et, x.y, dt.y);
+      }
+      if (op == 3 && zero) x = czero();
+      out[(size_t)j * ld] = x;
+      s2[(size_t)j * ld] = x;
+    }
+  }
+  if (op == 3) {
+    out2 += M.m;
+    {
+      Rd<double2, 8> r;
+      r.start(s2, ld, my, 1, 0);
+      Win w;
+      w.clear();
+      Hist h;
+      h.clear();
+      for (int t = 0; t < 3; t++) w.push(r.pop());
+      for (int j = 0; j < my; j++) {
+        w.push(r.pop());
+        s1[(size_t)j * ld] = d1f(d, j, w, h);
+      }
+    }
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) out2[(size_t)j * ld] = d1b(d, j, r.pop(), h);
+  } else if (op == 4) {
+    const double *ai = d.AAinv + (size_t)M.m * 4;
+    const double a0 = __ldg(ai), a1 = __ldg(ai + 1), a2 = __ldg(ai + 2), a3 = __ldg(ai + 3);
+    const double2 c1 = make_double2(-(a0 * db.x + a1 * dt.x), -(a0 * db.y + a1 * dt.y));
+    const double2 c2 = make_double2(-(a2 * db.x + a3 * dt.x), -(a2 * db.y + a3 * dt.y));
+    const size_t n = (size_t)d.nmode;
+    for (int j = 0; j < my; j++) {
+      double2 x = out[(size_t)j * ld];
+      const double v1 = __ldg(d.V12t + (size_t)j * 2 * n + M.m), v2 = __ldg(d.V12t + (size_t)j * 2 * n + n + M.m);
+      x.x += c1.x * v1 + c2.x * v2;
+      x.y += c1.y * v1 + c2.y * v2;
+      out[(size_t)j * ld] = zero ? czero() : x;
+    }
+  }
+}
+
+}  // namespace tpm
+}  // namespace lmc

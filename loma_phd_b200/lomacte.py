@@ -31,7 +31,7 @@ SYMBOLS = (
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
     "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
-    "lmc_device_bytes", "lmc_footprint",
+    "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
 )
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset")
@@ -103,6 +103,8 @@ def _lib():
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
         L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         L.lmc_use_graphs.argtypes = [vp, ctypes.c_int]
+        L.lmc_launches_per_step.argtypes = [vp]
+        L.lmc_y_family.argtypes = [vp]
         L.lmc_query.argtypes = [vp]
         L.lmc_device_bytes.argtypes = [vp]
         L.lmc_device_bytes.restype = ctypes.c_size_t
@@ -276,6 +278,15 @@ class Lomacte:
         if rc < 0:
             raise LomacteError(rc, "lmc_query")
         return rc == 1
+
+    @property
+    def launches_per_step(self) -> int:
+        return int(_lib().lmc_launches_per_step(self._h))
+
+    @property
+    def y_family(self) -> str:
+        """'mode' (one thread per mode) or 'warp' (one warp per mode)."""
+        return "mode" if _lib().lmc_y_family(self._h) == 1 else "warp"
 
     @property
     def device_bytes(self) -> int:
