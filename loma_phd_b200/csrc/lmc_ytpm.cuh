@@ -65,6 +65,64 @@ struct Rd {
   }
 };
 
+// queue depth giving K x 16 bytes in flight for values of type PT
+template <typename PT>
+__host__ __device__ constexpr int kq(int K) { return K * 16 / (int)sizeof(PT); }
+
+// the same for one real coefficient per row (per-mode tables)
+template <int K>
+struct RdS {
+  const double *p;
+  size_t ld;
+  int my, dir, nxt;
+  double q[K];
+  __device__ __forceinline__ double fetch(int r) const {
+    return (r >= 0 && r < my) ? __ldg(p + (size_t)r * ld) : 0.0;
+  }
+  __device__ __forceinline__ void start(const double *base, size_t ld_, int my_, int dir_, int first) {
+    p = base;
+    ld = ld_;
+    my = my_;
+    dir = dir_;
+    nxt = first;
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+      q[t] = fetch(nxt);
+      nxt += dir;
+    }
+  }
+  __device__ __forceinline__ double pop() {
+    const double v = q[0];
+#pragma unroll
+    for (int t = 0; t < K - 1; t++) q[t] = q[t + 1];
+    q[K - 1] = fetch(nxt);
+    nxt += dir;
+    return v;
+  }
+};
+
+// the per-mode LU rows of one mode, streamed: L (2 multipliers) forward,
+// U (reciprocal pivot + 2) backward
+template <int K>
+struct LRows {
+  RdS<K> l0, l1;
+  __device__ __forceinline__ void start(const Dev &d, int m) {
+    const size_t n = (size_t)d.nmode;
+    l0.start(d.PLt + m, 2 * n, d.my, 1, 0);
+    l1.start(d.PLt + n + m, 2 * n, d.my, 1, 0);
+  }
+};
+template <int K>
+struct URows {
+  RdS<K> u0, u1, u2;
+  __device__ __forceinline__ void start(const Dev &d, int m) {
+    const size_t n = (size_t)d.nmode;
+    u0.start(d.PUt + m, 3 * n, d.my, -1, d.my - 1);
+    u1.start(d.PUt + n + m, 3 * n, d.my, -1, d.my - 1);
+    u2.start(d.PUt + 2 * n + m, 3 * n, d.my, -1, d.my - 1);
+  }
+};
+
 template <typename PT>
 __device__ __forceinline__ void put(PT *base, size_t ld, int j, double2 v) {
   base[(size_t)j * ld] = from_d2<PT>(v);
@@ -147,7 +205,8 @@ __device__ __forceinline__ double2 d2b(const Dev &d, int j, double2 w, Hist &h) 
 }
 // Dirichlet Poisson of mode m (laps.f:375-401): right-hand side dt21 f with
 // zero wall rows, then the mode's LU (dt22 - k^2 dt21 with identity rows)
-__device__ __forceinline__ double2 pf(const Dev &d, int j, const Win &u, Hist &h, int m) {
+template <int K>
+__device__ __forceinline__ double2 pf(const Dev &d, int j, const Win &u, Hist &h, LRows<K> &L) {
   double2 r = czero();
   if (j > 0 && j < d.my - 1) {
     const double *c = d.r_dt21 + 5 * j;
@@ -158,15 +217,16 @@ __device__ __forceinline__ double2 pf(const Dev &d, int j, const Win &u, Hist &h
       r.y = fma(k, u.u[t + 1].y, r.y);
     }
   }
-  const size_t n = (size_t)d.nmode, b = (size_t)j * 2 * n + m;
-  r = fms(fms(r, __ldg(d.PLt + b + n), h.b), __ldg(d.PLt + b), h.a);
+  const double l0 = L.l0.pop(), l1 = L.l1.pop();
+  r = fms(fms(r, l1, h.b), l0, h.a);
   h.push(r);
   return r;
 }
-__device__ __forceinline__ double2 pb(const Dev &d, int j, double2 w, Hist &h, int m) {
-  const size_t n = (size_t)d.nmode, b = (size_t)j * 3 * n + m;
-  double2 x = fms(fms(w, __ldg(d.PUt + b + 2 * n), h.b), __ldg(d.PUt + b + n), h.a);
-  x = cscale(__ldg(d.PUt + b), x);
+template <int K>
+__device__ __forceinline__ double2 pb(double2 w, Hist &h, URows<K> &U) {
+  const double u0 = U.u0.pop(), u1 = U.u1.pop(), u2 = U.u2.pop();
+  double2 x = fms(fms(w, u2, h.b), u1, h.a);
+  x = cscale(u0, x);
   h.push(x);
   return x;
 }
@@ -205,6 +265,8 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
   {  // forward Poisson half; phi with its wall values set to zero
     Rd<double2, 8> r;
     r.start(d.phi + M.m, ld, my, 1, 0);
+    LRows<8> L;
+    L.start(d, M.m);
     Win w;
     w.clear();
     Hist h;
@@ -216,16 +278,18 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
     for (int j = 0; j < my; j++) {
       const double2 v = r.pop();
       w.push(j + 3 == my - 1 ? czero() : v);
-      s1[(size_t)j * ld] = pf(d, j, w, h, M.m);
+      s1[(size_t)j * ld] = pf(d, j, w, h, L);
     }
   }
   {  // backward Poisson half -> m_y
     Rd<double2, 8> r;
     r.start(s1, ld, my, -1, my - 1);
+    URows<8> U;
+    U.start(d, M.m);
     Hist h;
     h.clear();
     for (int j = my - 1; j >= 0; j--) {
-      double2 x = pb(d, j, r.pop(), h, M.m);
+      double2 x = pb(r.pop(), h, U);
       if (zero) x = czero();
       put(MY, ld, j, x);
       s2[(size_t)j * ld] = x;
@@ -269,7 +333,7 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
   double2 *s1 = d.ws[0] + M.m;
   {
     Rd<double2, 3> rvor, rrom, rphi, rrph;
-    Rd<CT, 3> rdmy;
+    Rd<CT, kq<CT>(3)> rdmy;
     Rd<double2, 4> rpsi;
     rvor.start(d.vor + M.m, ld, my, 1, 0);
     rrom.start(d.Rom + M.m, ld, my, 1, 0);
@@ -317,7 +381,7 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
   }
   {  // rho v = m_y + d(psi)/dy (cross.f:434-437, 471)
     Rd<double2, 4> r;
-    Rd<CT, 4> rmy;
+    Rd<CT, kq<CT>(4)> rmy;
     r.start(s1, ld, my, -1, my - 1);
     rmy.start(wsb<CT>(d, SB_MY) + M.m, ld, my, -1, my - 1);
     CT *RV = wsb<CT>(d, SB_RV) + M.m;
@@ -409,8 +473,8 @@ __global__ void __launch_bounds__(TB) t_post1(Dev d) {
   double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m, *s3 = d.ws[2] + M.m;
   {
     Rd<double2, 2> rT;
-    Rd<CT, 2> rDT;
-    Rd<CT, 3> rvv, ruv, rvw;
+    Rd<CT, kq<CT>(2)> rDT;
+    Rd<CT, kq<CT>(3)> rvv, ruv, rvw;
     rT.start(d.scal + M.m, ld, my, 1, 0);
     rDT.start(wsb<CT>(d, ODT) + M.m, ld, my, 1, 0);
     rvv.start(wsb<CT>(d, ORVV) + M.m, ld, my, 1, 0);
@@ -449,7 +513,7 @@ __global__ void __launch_bounds__(TB) t_post1(Dev d) {
   }
   {
     Rd<double2, 2> r1, r2, r3;
-    Rd<CT, 2> ruv, rvw, ruu, ruw, rww;
+    Rd<CT, kq<CT>(2)> ruv, rvw, ruu, ruw, rww;
     r1.start(s1, ld, my, -1, my - 1);
     r2.start(s2, ld, my, -1, my - 1);
     r3.start(s3, ld, my, -1, my - 1);
@@ -491,7 +555,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
   const double dtg = d.scal_d[0] * d.gama[rk];
   double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m, *s3 = d.ws[2] + M.m, *s4 = d.ws[3] + M.m;
   {  // forward halves of dw/dy, du/dy and d2(omega_y)/dy2
-    Rd<CT, 4> ru, rw;
+    Rd<CT, kq<CT>(4)> ru, rw;
     ru.start(wsb<CT>(d, OU) + M.m, ld, my, 1, 0);
     rw.start(wsb<CT>(d, OW) + M.m, ld, my, 1, 0);
     Win wu, ww, wy;
@@ -517,7 +581,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     }
   }
   {  // forward half of d/dy of i kx N_x + i kz N_z (cross.f:900-907)
-    Rd<CT, 4> rx, rz;
+    Rd<CT, kq<CT>(4)> rx, rz;
     rx.start(wsb<CT>(d, ORUU) + M.m, ld, my, 1, 0);
     rz.start(wsb<CT>(d, ORWW) + M.m, ld, my, 1, 0);
     Win wc;
@@ -532,7 +596,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
   }
   {  // omega_x, omega_z, (curl omega)_y -> s1
     Rd<double2, 4> r1, r2;
-    Rd<CT, 4> rv;
+    Rd<CT, kq<CT>(4)> rv;
     r1.start(s1, ld, my, -1, my - 1);
     r2.start(s2, ld, my, -1, my - 1);
     rv.start(wsb<CT>(d, OV) + M.m, ld, my, -1, my - 1);
@@ -548,7 +612,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
   }
   {  // RHS(Omega_y), Omega_y update; d/dy part of RHS(phi) (cross.f:885-917, 966-981)
     Rd<double2, 2> r3, r4, rvo;
-    Rd<CT, 2> ru, rw, rx, rz, ry;
+    Rd<CT, kq<CT>(2)> ru, rw, rx, rz, ry;
     r3.start(s3, ld, my, -1, my - 1);
     r4.start(s4, ld, my, -1, my - 1);
     rvo.start(d.vor + M.m, ld, my, -1, my - 1);
@@ -612,8 +676,10 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d) {
   const size_t ld = d.nmode;
   double2 *s1 = d.ws[0] + M.m;
   {
-    Rd<CT, 8> r;
+    Rd<CT, kq<CT>(8)> r;
     r.start(wsb<CT>(d, ODRHO) + M.m, ld, my, 1, 0);
+    LRows<8> L;
+    L.start(d, M.m);
     Win w;
     w.clear();
     Hist h;
@@ -621,17 +687,19 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d) {
     for (int t = 0; t < 3; t++) w.push(r.pop());
     for (int j = 0; j < my; j++) {
       w.push(r.pop());
-      s1[(size_t)j * ld] = pf(d, j, w, h, M.m);
+      s1[(size_t)j * ld] = pf(d, j, w, h, L);
     }
   }
   double2 db = czero(), dt = czero();
   {
     Rd<double2, 8> r;
     r.start(s1, ld, my, -1, my - 1);
+    URows<8> U;
+    U.start(d, M.m);
     Hist h;
     h.clear();
     for (int j = my - 1; j >= 0; j--) {
-      const double2 x = pb(d, j, r.pop(), h, M.m);
+      const double2 x = pb(r.pop(), h, U);
       const double eb = __ldg(d.r_ebot + j), et = __ldg(d.r_etop + j);
       db.x = fma(eb, x.x, db.x);
       db.y = fma(eb, x.y, db.y);
@@ -649,9 +717,12 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d) {
     Rd<double2, 8> r;
     r.start(s1, ld, my, 1, 0);
     const size_t n = (size_t)d.nmode;
+    RdS<8> rv1, rv2;
+    rv1.start(d.V12t + M.m, 2 * n, my, 1, 0);
+    rv2.start(d.V12t + n + M.m, 2 * n, my, 1, 0);
     for (int j = 0; j < my; j++) {
       double2 x = r.pop();
-      const double v1 = __ldg(d.V12t + (size_t)j * 2 * n + M.m), v2 = __ldg(d.V12t + (size_t)j * 2 * n + n + M.m);
+      const double v1 = rv1.pop(), v2 = rv2.pop();
       x.x += c1.x * v1 + c2.x * v2;
       x.y += c1.y * v1 + c2.y * v2;
       put(d.psi + M.m, ld, j, zero ? czero() : x);
@@ -677,21 +748,25 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
     w.clear();
     Hist h;
     h.clear();
+    LRows<4> L;
+    if (op >= 3) L.start(d, M.m);
     for (int t = 0; t < 3; t++) w.push(r.pop());
     for (int j = 0; j < my; j++) {
       w.push(r.pop());
-      s1[(size_t)j * ld] = op == 1 ? d1f(d, j, w, h) : op == 2 ? d2f(d, j, w, h) : pf(d, j, w, h, M.m);
+      s1[(size_t)j * ld] = op == 1 ? d1f(d, j, w, h) : op == 2 ? d2f(d, j, w, h) : pf(d, j, w, h, L);
     }
   }
   double2 db = czero(), dt = czero();
   {
     Rd<double2, 8> r;
     r.start(s1, ld, my, -1, my - 1);
+    URows<4> U;
+    if (op >= 3) U.start(d, M.m);
     Hist h;
     h.clear();
     for (int j = my - 1; j >= 0; j--) {
       const double2 w = r.pop();
-      double2 x = op == 1 ? d1b(d, j, w, h) : op == 2 ? d2b(d, j, w, h) : pb(d, j, w, h, M.m);
+      double2 x = op == 1 ? d1b(d, j, w, h) : op == 2 ? d2b(d, j, w, h) : pb(w, h, U);
       if (op == 4) {
         const double eb = __ldg(d.r_ebot + j), et = __ldg(d.r_etop + j);
         db.x = fma(eb, x.x, db.x);
