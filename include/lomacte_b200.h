@@ -50,6 +50,9 @@ typedef struct lmc_params {
                               and pointwise EOS / d(rho)/dt math
                            2: as 1 with FP64 FFT arithmetic (FP32 storage) */
   int device;           /* CUDA device ordinal */
+  int variant;          /* 0: trunk/lomacte3 (2017); 1: the 2014 code
+                           trunk/lomacte (spectral T, d(rho) by a transform
+                           round trip, Dirichlet psi; FP64 only) */
 } lmc_params;
 
 /* Per-step diagnostics (the .cf record of cross.f:1172-1176 without the

@@ -161,6 +161,7 @@ int do_load(lmc_handle *h, const double *vor, const double *phi, const double *p
   }
   LMC_CK(cudaMemsetAsync(d.Rom, 0, ns, h->s));
   LMC_CK(cudaMemsetAsync(d.Rphi, 0, ns, h->s));
+  if (d.variant) LMC_CK(cudaMemsetAsync(d.RT, 0, ns, h->s));
   LMC_CK(cudaMemsetAsync(d.rhst, 0, (size_t)d.my * d.mgalz * d.mgalx * sizeof(double), h->s));
   const size_t ny = (size_t)d.my * sizeof(double);
   LMC_CK(cudaMemcpyAsync(d.u00, u00, ny, cudaMemcpyHostToDevice, h->s));
@@ -210,6 +211,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   }
   if (p->device < 0 || p->device >= ndev) return LMC_EINVAL;
   if (p->precision < 0 || p->precision > 2) return LMC_EINVAL;
+  if (p->variant < 0 || p->variant > 1 || (p->variant == 1 && p->precision != 0)) return LMC_EINVAL;
   lmc_handle *h = new (std::nothrow) lmc_handle();
   if (!h) return LMC_ENOMEM;
   h->p = *p;
@@ -238,7 +240,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   d.my = g.my; d.mgalx = g.mgalx; d.mgalz = g.mgalz; d.nkx = g.nkx; d.mz = g.mz; d.nz1 = g.nz1; d.nmode = g.nmode;
   d.ldy = g.my | 1;
   d.ire = 1.0 / p->Re;
-  d.peclet = p->peclet > 0 ? p->peclet : p->Re * (double)0.7f;  // main.f:569
+  d.variant = p->variant;
+  // Pe = Re*0.7f (main.f:569); the 2014 code uses Pe = Re (lomacte/cross.f:1301)
+  d.peclet = p->peclet > 0 ? p->peclet : (d.variant ? p->Re : p->Re * (double)0.7f);
   d.cfl = (double)(float)p->cfl;
   d.hxalp = p->alp * (g.mgalx - 1) / M_PI;  // cross.f:1498
   d.hzbet = p->bet * (g.mgalz - 1) / M_PI;  // cross.f:1499
@@ -249,7 +253,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   // y-operator tables go to the device chunk-major (see lmcd::tab)
   const int C = d.C, lpm = d.lpm, base = d.base, extra = d.extra, my = g.my;
   auto cm = [&](const std::vector<double> &T, int W) { return lmc::chunk_major(T, my, W, C, lpm, base, extra); };
-  d.tpm = mode_parallel(g.nmode);
+  d.tpm = d.variant ? 1 : mode_parallel(g.nmode);  // the 2014 variant runs the mode-parallel kernels
   const size_t pm2 = (size_t)C * 2 * 32, pm3 = (size_t)C * 3 * 32;
   const size_t nm = d.tpm ? 0 : (size_t)g.nmode;  // chunk-major per-mode tables: warp kernels only
   std::vector<double> PLc(nm * pm2), PUc(nm * pm3), V12c(nm * pm2);
@@ -351,6 +355,12 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   if (d.tpm)
     for (int q = 0; q < 4; q++)
       if ((rc = dalloc(h, &d.ws[q], ns))) { lmc_destroy(h); return rc; }
+  if (d.variant &&
+      ((rc = dalloc(h, &d.Told, ns)) || (rc = dalloc(h, &d.dTs, ns)) || (rc = dalloc(h, &d.RT, ns)))) {
+    lmc_destroy(h);
+    return rc;
+  }
+  d.tsrc = d.variant ? d.Told : d.scal;
   double **vec[] = {&d.u00, &d.v00, &d.w00, &d.rf0u, &d.rf0w, &d.rf0v, &d.rhom};
   for (auto q : vec)
     if ((rc = dalloc(h, q, (size_t)g.my))) { lmc_destroy(h); return rc; }
@@ -478,10 +488,19 @@ int enqueue_step(lmc_handle *h, int cfl_step) {
       const int do_cfl = cfl_step && rk == 0;
       prof_mark(h, 4);
       lmc::launch_xphys(d, rk, do_cfl, rk == 0, s);
+      if (d.variant && rk == 0) lmc::launch_cfl14(d, do_cfl, s);
       prof_mark(h, 5);
       lmc::launch_zfwd(d, s);
       prof_mark(h, 6);
       lmc::launch_post1(d, rk, do_cfl, 1, s);
+      if (d.variant) {  // d(rho) from T and Delta T (tauij2, lomacte/cross.f:877)
+        prof_mark(h, 3);
+        lmc::launch_zinv(d, s, 1);
+        prof_mark(h, 4);
+        lmc::launch_xdrho(d, s);
+        prof_mark(h, 5);
+        lmc::launch_zfwd(d, s, 1);
+      }
       prof_mark(h, 7);
       lmc::launch_post2(d, rk, s);
       prof_mark(h, 8);
@@ -596,6 +615,9 @@ int lmc_launches_per_step(lmc_handle *h) {
   // (two kernels in the warp family), psi; the mode-parallel family adds
   // the 00 tails of post1 and psi and runs post2 as one kernel; the mixed
   // forms add the plane-sum reduction after xphys
+  // the 2014 variant: 14 kernels per substep (three for the d(rho) round
+  // trip, its own 00 tail) and the Deltat kernel in the first substep
+  if (h->d.variant) return 3 * 14 + 1;
   const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0);
   return 3 * per;
 }
@@ -612,7 +634,8 @@ size_t lmc_footprint(const lmc_params *p) {
   const size_t S = (size_t)g.nmode * g.my, Z = (size_t)g.nkx * g.my * g.mgalz;
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)
-  if (mode_parallel(g.nmode))
+  if (p->variant) b += 3 * S * 16;  // T before the substep, Delta T, RHS(T)
+  if (p->variant || mode_parallel(g.nmode))
     b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 4 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
   else
     b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8;  // per-mode Poisson tables

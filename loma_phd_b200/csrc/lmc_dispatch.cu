@@ -9,8 +9,9 @@ namespace lmc {
 
 #define LMC_FFT_DECL(SUF)                                                              \
   bool fft_has_##SUF(int n);                                                           \
-  bool fft_zinv_##SUF(const Dev &d, cudaStream_t s);                                   \
-  bool fft_zfwd_##SUF(const Dev &d, cudaStream_t s);                                   \
+  bool fft_zinv_##SUF(const Dev &d, int mode, cudaStream_t s);                         \
+  bool fft_zfwd_##SUF(const Dev &d, int mode, cudaStream_t s);                         \
+  bool fft_xdrho_##SUF(const Dev &d, cudaStream_t s);                                  \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
   size_t fft_zsm_##SUF(int n);                                                         \
   size_t fft_xsm_##SUF(int n);                                                         \
@@ -22,11 +23,14 @@ cudaError_t ykernels_init(int limit);
 
 bool fft_supported(int n) { return fft_has_a(n) || fft_has_b(n) || fft_has_c(n); }
 
-void launch_zinv(const Dev &d, cudaStream_t s) {
-  if (!fft_zinv_a(d, s) && !fft_zinv_b(d, s)) fft_zinv_c(d, s);
+void launch_zinv(const Dev &d, cudaStream_t s, int mode) {
+  if (!fft_zinv_a(d, mode, s) && !fft_zinv_b(d, mode, s)) fft_zinv_c(d, mode, s);
 }
-void launch_zfwd(const Dev &d, cudaStream_t s) {
-  if (!fft_zfwd_a(d, s) && !fft_zfwd_b(d, s)) fft_zfwd_c(d, s);
+void launch_zfwd(const Dev &d, cudaStream_t s, int mode) {
+  if (!fft_zfwd_a(d, mode, s) && !fft_zfwd_b(d, mode, s)) fft_zfwd_c(d, mode, s);
+}
+void launch_xdrho(const Dev &d, cudaStream_t s) {
+  if (!fft_xdrho_a(d, s) && !fft_xdrho_b(d, s)) fft_xdrho_c(d, s);
 }
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
   if (!fft_xphys_a(d, rk, do_cfl, do_diag, s) && !fft_xphys_b(d, rk, do_cfl, do_diag, s))

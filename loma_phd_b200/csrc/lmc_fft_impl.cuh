@@ -61,8 +61,10 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // current tile is transformed.  A bulk copy moves whole 16-byte units, so
 // for FP32 values the run is widened to an even start and length and the
 // tile is read from offset `lead` in the staging buffer.
+// mode 0: the eight transform inputs of the substep; mode 1 (2014 variant,
+// FP64): T before the substep and Delta T, for d(rho) (lomacte/cross.f:1760-1770)
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
+__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
@@ -75,6 +77,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
   __shared__ int s_ok;
   const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb;
   auto src_of = [&](int f) -> const ST * {
+    if constexpr (sizeof(ST) == sizeof(double2))
+      if (mode == 1) return f == 0 ? d.Told : d.dTs;
     switch (f) {
       case 0: return wsb<ST>(d, SB_RU);
       case 1: return wsb<ST>(d, SB_RV);
@@ -82,7 +86,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
       case 3: return wsb<ST>(d, SB_LAPT);
       case 5: return wsb<ST>(d, SB_DTDY);
       default:
-        if constexpr (sizeof(ST) == sizeof(double2)) return d.scal;
+        if constexpr (sizeof(ST) == sizeof(double2)) return d.tsrc;
         else return wsb<ST>(d, SB_T32);
     }
   };
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
     const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
     const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
     const int lead = lead_of(t);
-    const int mult = (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
+    const int mult = mode ? 0 : (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
     for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
       const int il = idx / gap, g = idx - il * gap;
       W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
@@ -146,16 +150,18 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles) {
   }
 }
 
+// mode 0: the substep's outputs (field blockIdx.z in place); mode 1 (2014
+// variant): d(rho) from z-physical buffer 0 into the d(rho) spectral slot
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zfwd(Dev d) {
+__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zfwd(Dev d, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *sm = (CT *)smraw;
-  const int f = blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
+  const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
   const int nb = min(G::KB, d.nkx - i0);
-  const ST *src = wzb<ST>(d, f) + (size_t)y * N1 * N2 * d.nkx + i0;
+  const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.nkx + i0;
   for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
     const int z = idx / G::KB, il = idx - z * G::KB;
     if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.nkx + il));
@@ -231,11 +237,11 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   const int nzk = (d.mgalz + ZB - 1) / ZB;
   auto issue = [&](int t) {
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
-    const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = (uint32_t)nzb * N * sizeof(double);
+    const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = d.variant ? 0u : (uint32_t)nzb * N * sizeof(double);
     mbar_expect_tx(&bar, 8 * rb + hb);
     const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
     for (int f = 0; f < 8; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
-    bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
+    if (hb) bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
   };
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -282,7 +288,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
-      rh[j] = (q < nzb * N) ? Sr[q] : 0.0;
+      rh[j] = (q < nzb * N && !d.variant) ? Sr[q] : 0.0;
     }
     __syncthreads();
     if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
@@ -333,14 +339,16 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
         double tn = T + dtxi * rhp;                                      // cross.f:1626
         double d8 = dtxi * rhp;                                          // cross.f:1627
         const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
-        d.rhst[((size_t)y * d.mgalz + z0 + l) * N + pos] = rhs;
-        tn = tn + dtg * rhs;                                             // cross.f:1641
-        d8 = d8 + dtg * rhs;                                             // cross.f:1642
+        if (!d.variant) {  // the 2014 variant keeps RHS(T) spectral (lomacte/cross.f:1452-1456)
+          d.rhst[((size_t)y * d.mgalz + z0 + l) * N + pos] = rhs;
+          tn = tn + dtg * rhs;                                           // cross.f:1641
+          d8 = d8 + dtg * rhs;                                           // cross.f:1642
+        }
         double o[11];
         o[OU] = u; o[OV] = v; o[OW] = w;
         o[ORUU] = ru * u; o[ORVV] = rv * v; o[ORWW] = rw * w;              // cross.f:1655-1666
         o[ORUV] = ru * v; o[ORUW] = ru * w; o[ORVW] = rv * w;
-        o[ODRHO] = (d8 / (T * tn)) / dtb - ab * rhs / (T * T);          // cross.f:1670-1671
+        o[ODRHO] = d.variant ? rhs : (d8 / (T * tn)) / dtb - ab * rhs / (T * T);  // cross.f:1670-1671
         o[ODT] = d8;                                                     // cross.f:1645-1647
         if constexpr (MX) {
 #pragma unroll
@@ -360,7 +368,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
           mu = fmax(mu, fabs(u));
           mv = fmax(mv, fabs(v));
           mw = fmax(mw, fabs(w));
-          atomic_max_pos(&s_tmax[l], fmax(T, 0.0));
+          if (!d.variant) atomic_max_pos(&s_tmax[l], fmax(T, 0.0));
         }
         if (do_diag) rs += 1.0 / T;
       }
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
     __syncthreads();
     F::template perm2nat<-1>(W, 2 * ZB, LD, wtwx<CT>(d));
     x_extract<N1, N2, CT, ST>(d, W, 0, ORVW, ODRHO, y, z0, nzb);
-    x_extract<N1, N2, CT, ST>(d, W, 1, ODT, -1, y, z0, nzb);
+    if (!d.variant) x_extract<N1, N2, CT, ST>(d, W, 1, ODT, -1, y, z0, nzb);
     __syncthreads();
   }
   if (do_cfl) {
@@ -429,6 +437,52 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
       atomic_max_pos(d.cflmax + 3, cft);
     }
   }
+}
+
+// 2014 variant: d(rho) = -Delta T / (T (T + Delta T)) at every physical
+// point (tensor2, lomacte/cross.f:1819-1908): T and Delta T arrive as one
+// complex line per (y, z), the result leaves in z-physical buffer 0.
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xdrho(Dev d) {
+  using F = Four<N1, N2, double2>;
+  using G = Geo<N1, N2>;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2 *W = (double2 *)smraw;
+  const int y = blockIdx.y, z0 = blockIdx.x * ZB, nzb = min(ZB, d.mgalz - z0), nkx = d.nkx;
+  const int gap = N - 2 * nkx + 1;
+  for (int idx = threadIdx.x; idx < ZB * gap; idx += blockDim.x) {
+    const int ln = idx / gap, g = idx - ln * gap;
+    W[ln * LD + F::sk(nkx + g)] = czero();
+  }
+  for (int l = 0; l < ZB; l++) {
+    double2 *line = W + l * LD;
+    const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
+    for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
+      double2 a = czero(), b = czero();
+      if (l < nzb) {
+        a = d.zb[0][g0 + k];
+        b = d.zb[1][g0 + k];
+      }
+      if (k == 0) {
+        line[F::sk(0)] = make_double2(a.x, b.x);
+      } else {
+        line[F::sk(k)] = make_double2(a.x - b.y, a.y + b.x);
+        line[F::sk(N - k)] = make_double2(a.x + b.y, b.x - a.y);
+      }
+    }
+  }
+  __syncthreads();
+  F::template nat2perm<+1>(W, ZB, LD, d.twx);
+  for (int q = threadIdx.x; q < ZB * N; q += blockDim.x) {
+    const int l = q / N, pos = q - l * N;
+    double2 *c = W + (size_t)l * LD + F::sk(pos);
+    const double T = c->x, dT = c->y;
+    *c = make_double2(-dT / (T * (T + dT)), 0.0);  // lomacte/cross.f:1881
+  }
+  __syncthreads();
+  F::template perm2nat<-1>(W, ZB, LD, d.twx);
+  x_extract<N1, N2, double2, double2>(d, W, 0, 0, -1, y, z0, nzb);
 }
 
 // Plane sums of the mixed form's outputs from the partial sums of k_xphys,
@@ -471,15 +525,21 @@ struct Launch {
     const int g = sms * per;
     return g < ntiles ? g : ntiles;
   }
-  static void zinv(const Dev &d, cudaStream_t s) {
-    const int ntiles = 8 * d.my * ((d.nkx + G::KB - 1) / G::KB);
+  static void zinv(const Dev &d, int mode, cudaStream_t s) {
+    const int ntiles = (mode ? 2 : 8) * d.my * ((d.nkx + G::KB - 1) / G::KB);
     const size_t sm = zinv_sm(d.mz);
     const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, G::ZT, sm, ntiles);
-    k_zinv<N1, N2, CT, ST><<<g, G::ZT, sm, s>>>(d, ntiles);
+    k_zinv<N1, N2, CT, ST><<<g, G::ZT, sm, s>>>(d, ntiles, mode);
   }
-  static void zfwd(const Dev &d, cudaStream_t s) {
-    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, 11);
-    k_zfwd<N1, N2, CT, ST><<<g, G::ZT, zsm(), s>>>(d);
+  static void zfwd(const Dev &d, int mode, cudaStream_t s) {
+    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, mode ? 1 : (d.variant ? 10 : 11));
+    k_zfwd<N1, N2, CT, ST><<<g, G::ZT, zsm(), s>>>(d, mode);
+  }
+  static void xdrho(const Dev &d, cudaStream_t s) {
+    if constexpr (sizeof(CT) == sizeof(double2) && sizeof(ST) == sizeof(double2)) {
+      dim3 g((d.mgalz + G::ZB - 1) / G::ZB, d.my);
+      k_xdrho<N1, N2><<<g, G::XT, (size_t)G::ZB * G::LD * sizeof(double2), s>>>(d);
+    }
   }
   static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
@@ -532,7 +592,9 @@ inline cudaError_t upload_twiddles() {
     default: Launch<N1, N2, double2, double2>::CALL; break;           \
   }
 #define LMC_FFT_CASE_Z(N, N1, N2, WHAT) \
-  case N: LMC_FFT_FORMS(N1, N2, WHAT(d, s)) return true;
+  case N: LMC_FFT_FORMS(N1, N2, WHAT(d, mode, s)) return true;
+#define LMC_FFT_CASE_XD(N, N1, N2) \
+  case N: Launch<N1, N2, double2, double2>::xdrho(d, s); return true;
 #define LMC_FFT_CASE_X(N, N1, N2) \
   case N: LMC_FFT_FORMS(N1, N2, xphys(d, rk, do_cfl, do_diag, s)) return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
@@ -551,11 +613,14 @@ inline cudaError_t upload_twiddles() {
   bool fft_has_##SUF(int n) {                                                                     \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_HAS) default: return false; }                         \
   }                                                                                               \
-  bool fft_zinv_##SUF(const Dev &d, cudaStream_t s) {                                             \
+  bool fft_zinv_##SUF(const Dev &d, int mode, cudaStream_t s) {                                   \
     switch (d.mgalz) { LMC_FFT_SIZES(LMC_FFT_CASE_ZI) default: return false; }                     \
   }                                                                                               \
-  bool fft_zfwd_##SUF(const Dev &d, cudaStream_t s) {                                             \
+  bool fft_zfwd_##SUF(const Dev &d, int mode, cudaStream_t s) {                                   \
     switch (d.mgalz) { LMC_FFT_SIZES(LMC_FFT_CASE_ZF) default: return false; }                     \
+  }                                                                                               \
+  bool fft_xdrho_##SUF(const Dev &d, cudaStream_t s) {                                            \
+    switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_XD) default: return false; }                     \
   }                                                                                               \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {           \
     switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_X) default: return false; }                      \

@@ -32,6 +32,12 @@ struct Dev {
   // Poisson tables mode-fastest ([my][band][nmode]), and four FP64
   // spectral scratch fields for the forward halves of the banded solves.
   int tpm;
+  // 2014 variant (trunk/lomacte): spectral T before this substep's update,
+  // its increment Delta T, and the previous substep's spectral RHS(T);
+  // tsrc is the T the transforms read (scal, or Told in the variant)
+  int variant;
+  double2 *Told, *dTs, *RT;
+  const double2 *tsrc;
   const double *r_dt12, *r_dt11, *r_dt22, *r_dt21, *r_p1L, *r_p1U, *r_p3L, *r_p3U, *r_fmap, *r_ebot, *r_etop;
   const double *PLt, *PUt, *V12t;
   double2 *ws[4];
@@ -99,9 +105,12 @@ bool fft_supported(int n);
 void launch_lapv(const Dev &d, cudaStream_t s);
 void launch_assemble(const Dev &d, int rk, cudaStream_t s);
 void launch_tder(const Dev &d, cudaStream_t s);
-void launch_zinv(const Dev &d, cudaStream_t s);
+// mode 1 (2014 variant): the d(rho) round trip of T and Delta T
+void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0);
+void launch_xdrho(const Dev &d, cudaStream_t s);
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
-void launch_zfwd(const Dev &d, cudaStream_t s);
+void launch_zfwd(const Dev &d, cudaStream_t s, int mode = 0);
+void launch_cfl14(const Dev &d, int do_cfl, cudaStream_t s);
 void launch_post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
 void launch_post2(const Dev &d, int rk, cudaStream_t s);
 void launch_psi(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);

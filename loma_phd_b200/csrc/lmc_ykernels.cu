@@ -70,20 +70,22 @@ void launch_tder(const Dev &d, cudaStream_t s) {
 }
 void launch_post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
   if (d.tpm) {
-    tpm_post1(d, s);
-    LMC_YDISPATCH(post1_00(d, rk, do_cfl, do_diag, s))
+    tpm_post1(d, rk, s);
+    LMC_YDISPATCH(post1_00(d, rk, d.variant ? 0 : do_cfl, do_diag, s))
   } else {
     LMC_YDISPATCH(post1(d, rk, do_cfl, do_diag, s))
   }
 }
+void launch_cfl14(const Dev &d, int do_cfl, cudaStream_t s) { tpm_cfl14(d, do_cfl, s); }
 void launch_post2(const Dev &d, int rk, cudaStream_t s) {
   if (d.tpm) tpm_post2(d, rk, s);
   else LMC_YDISPATCH(post2(d, rk, s))
 }
 void launch_psi(const Dev &d, int rk, int cfl_step, int do_diag, cudaStream_t s) {
   if (d.tpm) {
-    tpm_psi(d, s);
-    LMC_YDISPATCH(psi_00(d, rk, cfl_step, s))
+    tpm_psi(d, rk, s);
+    if (d.variant) tpm_psi00_14(d, rk, s);
+    else LMC_YDISPATCH(psi_00(d, rk, cfl_step, s))
   } else {
     LMC_YDISPATCH(psi(d, rk, cfl_step, do_diag, s))
   }

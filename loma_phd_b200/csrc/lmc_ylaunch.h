@@ -28,9 +28,11 @@ struct YL {
 void tpm_lapv(const Dev &d, cudaStream_t s);
 void tpm_assemble(const Dev &d, int rk, cudaStream_t s);
 void tpm_tder(const Dev &d, cudaStream_t s);
-void tpm_post1(const Dev &d, cudaStream_t s);
+void tpm_post1(const Dev &d, int rk, cudaStream_t s);
 void tpm_post2(const Dev &d, int rk, cudaStream_t s);
-void tpm_psi(const Dev &d, cudaStream_t s);
+void tpm_psi(const Dev &d, int rk, cudaStream_t s);
+void tpm_cfl14(const Dev &d, int do_cfl, cudaStream_t s);
+void tpm_psi00_14(const Dev &d, int rk, cudaStream_t s);
 void tpm_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s);
 
 #define LMC_Y_CHUNKS(X) X(4) X(5) X(7) X(9) X(13) X(17)

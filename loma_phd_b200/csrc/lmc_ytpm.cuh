@@ -321,7 +321,10 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
 // (2)-(3) m_x, m_z, rho u_i, xi-updates of Omega_y and phi, 00 modes
 // (cross.f:315-327, 395-499)
 // ----------------------------------------------------------------------
-template <typename CT>
+// V: the 2014 variant (trunk/lomacte/src/cross.f:293-461): d(Omega_y)/dy = 0
+// through two rows at each wall for m_x, m_z only, Omega_y** from the raw
+// Omega_y, and T, T** and Delta T from the spectral RHS(T).
+template <typename CT, bool V>
 __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
   Mode M;
   if (!mode_of(d, M)) return;
@@ -343,7 +346,13 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
     rpsi.start(d.psi + M.m, ld, my, 1, 0);
     CT *RU = wsb<CT>(d, SB_RU) + M.m, *RW = wsb<CT>(d, SB_RW) + M.m;
     const double2 vor1 = __ldg(d.vor + ld + M.m);  // wall BC of Omega_y, cross.f:315-327
-    double2 vprev = czero();
+    const double2 vor2 = __ldg(d.vor + 2 * ld + M.m);
+    double2 vprev = czero(), vprev2 = czero();
+    Rd<double2, 3> rT, rRT;
+    if constexpr (V) {
+      rT.start(d.scal + M.m, ld, my, 1, 0);
+      rRT.start(d.RT + M.m, ld, my, 1, 0);
+    }
     Win w;
     w.clear();
     Hist h;
@@ -353,7 +362,13 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
       w.push(rpsi.pop());
       const double2 ps = w.c();
       const double2 vr = rvor.pop();
-      const double2 vo = (j == 0) ? vor1 : (j == my - 1) ? vprev : vr;
+      double2 vo;
+      if constexpr (V) {  // lomacte/cross.f:306-311
+        vo = (j <= 1) ? vor2 : (j >= my - 2) ? (j == my - 2 ? vprev : vprev2) : vr;
+        if (j == my - 2) vprev2 = vprev;
+      } else {
+        vo = (j == 0) ? vor1 : (j == my - 1) ? vprev : vr;
+      }
       vprev = vr;
       const double2 a = rdmy.pop();
       double2 b = cadd(csub(cik(ta, a), cik(tb, vo)), cik(M.kx, ps));   // rho u, cross.f:402,467
@@ -372,7 +387,13 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
       }
       put(RU, ld, j, b);
       put(RW, ld, j, c);
-      put(d.vor + M.m, ld, j, cadd(vo, cscale(dtxi, rrom.pop())));  // cross.f:420-424
+      put(d.vor + M.m, ld, j, cadd(V ? vr : vo, cscale(dtxi, rrom.pop())));  // cross.f:420-424
+      if constexpr (V) {  // T saved, T** and Delta T: lomacte/cross.f:368-396
+        const double2 T = rT.pop(), inc = cscale(dtxi, rRT.pop());
+        put(d.Told + M.m, ld, j, T);
+        put(d.scal + M.m, ld, j, cadd(T, inc));
+        put(d.dTs + M.m, ld, j, inc);
+      }
       double2 ph = rphi.pop();
       if (j == 0 || j == my - 1) ph = czero();
       put(d.phi + M.m, ld, j, cadd(ph, cscale(dtxi, rrph.pop())));  // cross.f:424-425
@@ -401,33 +422,35 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
 // ----------------------------------------------------------------------
 // (4) T with its wall BCs, dT/dy, lap(T) (cross.f:336-349, 521-541)
 // ----------------------------------------------------------------------
-template <typename CT>
+// V: the 2014 variant differentiates the T saved before its update, with
+// no wall values imposed (lomacte/cross.f:486-519).
+template <typename CT, bool V>
 __global__ void __launch_bounds__(TB) t_tder(Dev d) {
   Mode M;
   if (!mode_of(d, M)) return;
   const int my = d.my;
   const size_t ld = d.nmode;
   const bool m00 = M.m == 0;
-  const double2 wb = m00 ? make_double2(1.0 / d.scal_d[3], 0.0) : czero();
-  const double2 wt = m00 ? make_double2(1.0 / d.scal_d[4], 0.0) : czero();
   double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m;
+  double2 *const Tsrc = V ? d.Told : d.scal;
   {
     Rd<double2, 8> r;
-    r.start(d.scal + M.m, ld, my, 1, 0);
+    r.start(Tsrc + M.m, ld, my, 1, 0);
+    const double2 v0 = r.pop();
+    const double2 wb = V ? v0 : (m00 ? make_double2(1.0 / d.scal_d[3], 0.0) : czero());
+    const double2 wt_bc = m00 ? make_double2(1.0 / d.scal_d[4], 0.0) : czero();
     Win w;
     w.clear();
     Hist h1, h2;
     h1.clear();
     h2.clear();
-    for (int t = 0; t < 3; t++) {
-      const double2 v = r.pop();
-      w.push(t == 0 ? wb : v);
-    }
+    w.push(wb);
+    for (int t = 1; t < 3; t++) w.push(r.pop());
     for (int j = 0; j < my; j++) {
       const double2 v = r.pop();
-      w.push(j + 3 == my - 1 ? wt : v);
+      w.push((!V && j + 3 == my - 1) ? wt_bc : v);
       const double2 T = w.c();
-      put(d.scal + M.m, ld, j, T);
+      if constexpr (!V) put(d.scal + M.m, ld, j, T);
       if constexpr (mixed<CT>()) {
         put(wsb<CT>(d, SB_T32) + M.m, ld, j, T);
         if (m00) d.mi[(size_t)5 * my + j] = T.x;
@@ -440,7 +463,7 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
     Rd<double2, 4> r1, r2, rT;
     r1.start(s1, ld, my, -1, my - 1);
     r2.start(s2, ld, my, -1, my - 1);
-    rT.start(d.scal + M.m, ld, my, -1, my - 1);
+    rT.start(Tsrc + M.m, ld, my, -1, my - 1);
     CT *DY = wsb<CT>(d, SB_DTDY) + M.m, *LT = wsb<CT>(d, SB_LAPT) + M.m;
     Hist h1, h2;
     h1.clear();
@@ -463,20 +486,25 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
 // (6a)-(6b) T update and N_i (cross.f:619-682); rf0u / rf0w get the 00
 // pencils of d(rho uv)/dy and d(rho vw)/dy for the 00 tail.
 // ----------------------------------------------------------------------
-template <typename CT>
-__global__ void __launch_bounds__(TB) t_post1(Dev d) {
+// V: the 2014 variant advances the spectral T with this substep's RHS(T)
+// (in the d(rho)/dt slot) and accumulates Delta T (lomacte/cross.f:563-570).
+template <typename CT, bool V>
+__global__ void __launch_bounds__(TB) t_post1(Dev d, int rk) {
   Mode M;
   if (!mode_of(d, M)) return;
   const int my = d.my;
   const size_t ld = d.nmode;
   const bool m00 = M.m == 0;
+  const double dtg = d.scal_d[0] * d.gama[rk];
   double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m, *s3 = d.ws[2] + M.m;
   {
     Rd<double2, 2> rT;
     Rd<CT, kq<CT>(2)> rDT;
     Rd<CT, kq<CT>(3)> rvv, ruv, rvw;
     rT.start(d.scal + M.m, ld, my, 1, 0);
-    rDT.start(wsb<CT>(d, ODT) + M.m, ld, my, 1, 0);
+    rDT.start(wsb<CT>(d, V ? ODRHO : ODT) + M.m, ld, my, 1, 0);
+    Rd<double2, 2> rdT;
+    if constexpr (V) rdT.start(d.dTs + M.m, ld, my, 1, 0);
     rvv.start(wsb<CT>(d, ORVV) + M.m, ld, my, 1, 0);
     ruv.start(wsb<CT>(d, ORUV) + M.m, ld, my, 1, 0);
     rvw.start(wsb<CT>(d, ORVW) + M.m, ld, my, 1, 0);
@@ -505,6 +533,11 @@ __global__ void __launch_bounds__(TB) t_post1(Dev d) {
       double2 dT = rDT.pop();
       if constexpr (mixed<CT>())
         if (m00) dT = mo00_row(d, ODT, j);
+      if constexpr (V) {
+        put(d.RT + M.m, ld, j, dT);
+        put(d.dTs + M.m, ld, j, cadd(rdT.pop(), cscale(dtg, dT)));
+        dT = cscale(dtg, dT);
+      }
       put(d.scal + M.m, ld, j, cadd(rT.pop(), dT));  // cross.f:619-627
       s1[(size_t)j * ld] = d1f(d, j, wvv, h1);
       s2[(size_t)j * ld] = d1f(d, j, wuv, h2);
@@ -668,13 +701,16 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
 // ----------------------------------------------------------------------
 // (8) psi^{n+1} by solvepsi (cross.f:1092-1104, laps.f:580-730)
 // ----------------------------------------------------------------------
-template <typename CT>
-__global__ void __launch_bounds__(TB) t_psi(Dev d) {
+// V: the 2014 variant solves the Dirichlet problem for
+// psi = -d(rho) / (Deltat (gamma + xi)) (lomacte/cross.f:970-983).
+template <typename CT, bool V>
+__global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
   Mode M;
   if (!mode_of(d, M)) return;
   const int my = d.my;
   const size_t ld = d.nmode;
   double2 *s1 = d.ws[0] + M.m;
+  const double sc = V ? -1.0 / (d.scal_d[0] * (d.gama[rk] + d.xi[rk])) : 1.0;
   {
     Rd<CT, kq<CT>(8)> r;
     r.start(wsb<CT>(d, ODRHO) + M.m, ld, my, 1, 0);
@@ -684,11 +720,25 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d) {
     w.clear();
     Hist h;
     h.clear();
-    for (int t = 0; t < 3; t++) w.push(r.pop());
+    for (int t = 0; t < 3; t++) w.push(cscale(sc, r.pop()));
     for (int j = 0; j < my; j++) {
-      w.push(r.pop());
+      w.push(cscale(sc, r.pop()));
       s1[(size_t)j * ld] = pf(d, j, w, h, L);
     }
+  }
+  if constexpr (V) {
+    const bool zero = M.k2 == 0.0;
+    Rd<double2, 8> r;
+    r.start(s1, ld, my, -1, my - 1);
+    URows<8> U;
+    U.start(d, M.m);
+    Hist h;
+    h.clear();
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 x = pb(r.pop(), h, U);
+      put(d.psi + M.m, ld, j, zero ? czero() : x);
+    }
+    return;
   }
   double2 db = czero(), dt = czero();
   {
@@ -812,6 +862,65 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
       x.y += c1.y * v1 + c2.y * v2;
       out[(size_t)j * ld] = zero ? czero() : x;
     }
+  }
+}
+
+// 2014 variant: Deltat of the first substep of a CFL step, from the
+// velocity maxima of the x stage (lomacte/cross.f:1547-1574); the new
+// Deltat applies from this substep on.
+__global__ void k_cfl14(Dev d, int do_cfl) {
+  if (!do_cfl || threadIdx.x != 0 || blockIdx.x != 0) return;
+  double hmin = d.hy[0];
+  for (int j = 1; j < d.my; j++) hmin = fmin(hmin, d.hy[j]);
+  const double hyy = 2.0 * d.ire * pow(fmax(1.0 / hmin, fmax(0.5 * d.hxalp, 0.5 * d.hzbet)), 2.0);
+  const double cx = __longlong_as_double((long long)d.cflmax[0]) * d.hxalp;
+  const double cy = __longlong_as_double((long long)d.cflmax[1]);
+  const double cz = __longlong_as_double((long long)d.cflmax[2]) * d.hzbet;
+  const double reig = fmax(fmax(cx, fmax(cy, cz)), hyy);
+  d.scal_d[0] = (double)(float)(d.cfl / reig);  // Deltat is real*4
+}
+
+// 2014 variant, 00 modes after the substep (lomacte/cross.f:931-1002):
+// rho u00 / rho w00 RK3 update, masses, rho v00 = -(cumulative trapezoid of
+// d(rho)00 / (Deltat (gamma + xi)) - rho_bot trapz / (rho_top + rho_bot)),
+// end-of-step time.  One thread: the sums run in the reference's order.
+__global__ void k_psi00_14(Dev d, int rk) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int my = d.my;
+  const double dt = d.scal_d[0], dtg = dt * d.gama[rk], den = dt * (d.gama[rk] + d.xi[rk]);
+  double mu = 0.0, mv = 0.0, mw = 0.0;
+  for (int j = 0; j < my; j++) {
+    if (j >= 1 && j <= my - 2) {
+      d.u00[j] += dtg * d.rf0u[j];
+      d.w00[j] += dtg * d.rf0w[j];
+    }
+    mu += d.u00[j] * d.hy[j];
+    mv += d.v00[j] * d.hy[j];
+    mw += d.w00[j] * d.hy[j];
+  }
+  const double2 *dr = d.sb[ODRHO];
+  const size_t ld = d.nmode;
+  double f = 0.0, prev = dr[0].x / den;
+  d.rf0v[0] = 0.0;
+  for (int j = 0; j < my - 1; j++) {
+    const double nxt = dr[(size_t)(j + 1) * ld].x / den;
+    f += 0.5 * (d.y[j + 1] - d.y[j]) * (nxt + prev);
+    d.rf0v[j + 1] = f;
+    prev = nxt;
+  }
+  const double trapz = f;
+  const double sh = d.scal_d[3] * trapz / (d.scal_d[4] + d.scal_d[3]);
+  for (int j = 0; j < my; j++) {
+    d.rf0v[j] -= sh;
+    d.v00[j] = -d.rf0v[j];
+  }
+  d.diag[5] = trapz;
+  d.diag[7] = mu; d.diag[8] = mv; d.diag[9] = mw;
+  if (rk == 2) {
+    d.diag[0] = d.scal_d[2];
+    d.diag[1] = dt;
+    d.scal_d[2] += dt;
+    d.diag[12] = dt;
   }
 }
 

@@ -49,7 +49,7 @@ class lmc_params(ctypes.Structure):
                 ("Re", ctypes.c_double), ("alp", ctypes.c_double), ("bet", ctypes.c_double),
                 ("peclet", ctypes.c_double), ("cfl", ctypes.c_double), ("ncfl", ctypes.c_int),
                 ("dt_mode", ctypes.c_int), ("dt", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("variant", ctypes.c_int)]
 
 
 class lmc_diag(ctypes.Structure):
@@ -149,6 +149,7 @@ class Params:
     dt: float = 0.01
     precision: int = 0
     device: int = 0
+    variant: int = 0          # 0 trunk/lomacte3 (2017), 1 trunk/lomacte (2014)
 
     def c(self) -> lmc_params:
         return lmc_params(*[getattr(self, f.name) for f in dataclasses.fields(self)])

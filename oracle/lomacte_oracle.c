@@ -438,6 +438,8 @@ struct lmo {
   double *u00wk, *v00wk, *w00wk, *rf0u, *rf0w, *rf0v;
   double Deltat, time, dtr, rhobot, rhotop;
   int icfl, istep_total;
+  int variant;  /* 0: trunk/lomacte3 (2017), 1: trunk/lomacte (2014) */
+  cplx *rts;    /* 2014 variant: spectral RHS(T) of the previous substep */
   double diag[LMO_NDIAG];
   fftplan px, pz;
   /* work buffers: spectral [kx][kz][y] (size nmode*my) */
@@ -507,7 +509,7 @@ lmo *lmo_create(int mgalx, int mgalz, int my, const double *y, double Re,
   size_t ns = (size_t)o->nmode * my;
   cplx **bufs[] = {&o->vor, &o->phi, &o->psi, &o->scal, &o->ten12p, &o->ten13p,
                    &o->w_mx, &o->w_my, &o->w_mz, &o->w_nx, &o->w_ny, &o->w_nz,
-                   &o->w_t12, &o->w_t13, &o->w_t23, &o->w_drho, &o->w_chwk, &o->w_chwk2};
+                   &o->w_t12, &o->w_t13, &o->w_t23, &o->w_drho, &o->w_chwk, &o->w_chwk2, &o->rts};
   for (size_t b = 0; b < sizeof(bufs) / sizeof(bufs[0]); b++) *bufs[b] = xcalloc(ns, sizeof(cplx));
   size_t nl = (size_t)mgalz * my;
   for (int f = 0; f < 11; f++) o->ln[f] = xcalloc(nl * o->nkx, sizeof(cplx));
@@ -525,7 +527,8 @@ void lmo_destroy(lmo *o) {
   void *p[] = {o->y, o->hy, o->trp, o->fmap, o->prem1, o->dt11, o->dt12, o->prem3, o->dt21, o->dt22,
                o->kxv, o->kzv, o->vor, o->phi, o->psi, o->scal, o->ten12p, o->ten13p, o->rhst,
                o->u00wk, o->v00wk, o->w00wk, o->rf0u, o->rf0w, o->rf0v, o->w_mx, o->w_my, o->w_mz,
-               o->w_nx, o->w_ny, o->w_nz, o->w_t12, o->w_t13, o->w_t23, o->w_drho, o->w_chwk, o->w_chwk2};
+               o->w_nx, o->w_ny, o->w_nz, o->w_t12, o->w_t13, o->w_t23, o->w_drho, o->w_chwk, o->w_chwk2,
+               o->rts};
   for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
   for (int f = 0; f < 11; f++) free(o->ln[f]);
   plan_free(&o->px); plan_free(&o->pz);
@@ -541,6 +544,7 @@ int lmo_set_state(lmo *o, const double *vor, const double *phi, const double *ps
   memcpy(o->vor, vor, ns * sizeof(cplx)); memcpy(o->phi, phi, ns * sizeof(cplx));
   memcpy(o->psi, psi, ns * sizeof(cplx)); memcpy(o->scal, scal, ns * sizeof(cplx));
   memset(o->ten12p, 0, ns * sizeof(cplx)); memset(o->ten13p, 0, ns * sizeof(cplx));
+  memset(o->rts, 0, ns * sizeof(cplx));
   memset(o->rhst, 0, (size_t)o->mgalz * o->my * o->mgalx * 8);
   /* cross.f:276-280 (first step copies the 00 modes to the work vectors) */
   memcpy(o->u00wk, u00, o->my * 8); memcpy(o->v00wk, v00, o->my * 8); memcpy(o->w00wk, w00, o->my * 8);
@@ -1136,8 +1140,351 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
   (void)nkx;
 }
 
+/* ------------------------------------------------------------------ */
+/* The 2014 variant, trunk/lomacte/src/cross.f (below "lomacte/"):     */
+/* spectral T with its own RK3 RHS, d(rho) from a transform round trip */
+/* of T and Delta T, psi by the Dirichlet Poisson solver and rho v00   */
+/* by a cumulative trapezoid.                                          */
+/* ------------------------------------------------------------------ */
+
+/* phys2 of lomacte/cross.f:1268-1578 on all lines: u_i, RHS(T) with
+ * Pe = Re (lomacte/cross.f:1301), the six products; CFL maxima. */
+static void phys2_14(lmo *o, int do_cfl, int do_mass, double *cflout /*3*/, double *rhom) {
+  int mgalx = o->mgalx, mgalz = o->mgalz, my = o->my, nkx = o->nkx;
+  size_t nlines = (size_t)mgalz * my;
+  double cflx = 0, cfly = 0, cflz = 0;
+  const double pe = o->Re;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *ph = malloc(sizeof(double) * mgalx * 8), *out = malloc(sizeof(double) * mgalx * 10);
+    cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
+    cplx *spec = malloc(sizeof(cplx) * nkx * 10);
+#pragma omp for schedule(static)
+    for (long L = 0; L < (long)nlines; L++) {
+      int jj = (int)(L / mgalz);
+      cplx *sp[8];
+      double *p[8];
+      for (int f = 0; f < 8; f++) { sp[f] = o->ln[f] + (size_t)L * nkx; p[f] = ph + (size_t)f * mgalx; }
+      for (int f = 0; f < 8; f += 2) xinv2(o, sp[f], sp[f + 1], p[f], p[f + 1], buf, fo);
+      double *ru = p[0], *rv = p[1], *rw = p[2], *lapT = p[3], *tx = p[4], *ty = p[5], *tz = p[6], *T = p[7];
+      double *q[10];
+      for (int f = 0; f < 10; f++) q[f] = out + (size_t)f * mgalx;
+      double lmx = 0, lmy = 0, lmz = 0, rsum = 0;
+      for (int x = 0; x < mgalx; x++) {
+        double u = ru[x] * T[x], v = rv[x] * T[x], w = rw[x] * T[x]; /* lomacte/cross.f:1440-1449 */
+        q[9][x] = -u * tx[x] - v * ty[x] - w * tz[x] + (1 / pe) * T[x] * lapT[x]; /* :1452-1456 */
+        q[0][x] = u; q[1][x] = v; q[2][x] = w;
+        q[3][x] = ru[x] * u; q[4][x] = rv[x] * v; q[5][x] = rw[x] * w; /* :1465-1469 */
+        q[6][x] = ru[x] * v; q[7][x] = ru[x] * w; q[8][x] = rv[x] * w; /* :1472-1476 */
+        if (do_cfl) { lmx = fmax(lmx, fabs(u)); lmy = fmax(lmy, fabs(v)); lmz = fmax(lmz, fabs(w)); }
+        if (do_mass) rsum += 1.0 / T[x];
+      }
+      if (do_cfl) { /* :1492-1503 */
+#pragma omp critical
+        { cflx = fmax(cflx, lmx); cflz = fmax(cflz, lmz); cfly = fmax(cfly, lmy / o->hy[jj]); }
+      }
+      if (do_mass) {
+#pragma omp atomic
+        rhom[jj] += rsum;
+      }
+      cplx *so[10];
+      for (int f = 0; f < 10; f++) so[f] = spec + (size_t)f * nkx;
+      for (int f = 0; f < 10; f += 2) xfwd2(o, q[f], q[f + 1], so[f], so[f + 1], buf, fo);
+      for (int f = 0; f < 10; f++) memcpy(o->ln[f] + (size_t)L * nkx, so[f], sizeof(cplx) * nkx);
+    }
+    free(ph); free(out); free(buf); free(fo); free(spec);
+  }
+  cflout[0] = cflx; cflout[1] = cfly; cflout[2] = cflz;
+}
+
+/* foup2 of lomacte/cross.f:1109-1258 and the Deltat of phys2
+ * (lomacte/cross.f:1547-1574): applied at once, in the first substep. */
+static void foup2_14(lmo *o, int do_cfl, int do_diag, cplx *in8[8], cplx *out10[10]) {
+  int nkx = o->nkx, mgalz = o->mgalz, my = o->my;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for collapse(2) schedule(static)
+    for (int f = 0; f < 8; f++)
+      for (int i = 0; i < nkx; i++) zinv_plane(o, i, in8[f], o->ln[f], buf, out);
+    free(buf); free(out);
+  }
+  double cfl[3];
+  double *rhom = xcalloc(my, 8);
+  phys2_14(o, do_cfl, do_diag, cfl, rhom);
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for collapse(2) schedule(static)
+    for (int f = 0; f < 10; f++)
+      for (int i = 0; i < nkx; i++) zfwd_plane(o, i, o->ln[f], out10[f], buf, out);
+    free(buf); free(out);
+  }
+  if (do_diag) { /* dm: lomacte/cross.f:1240-1256; masst as in the 2017 path */
+    const cplx *u = out10[0];
+    double dm = 0.0;
+    for (int j = 1; j <= my - 2; j++) {
+      double a = creal(u[j + 1]), b = creal(u[j - 1]);
+      dm += o->trp[j] * (a * a + b * b);
+    }
+    {
+      double a = creal(u[1]), b = creal(u[0]), c = creal(u[my - 1]), d = creal(u[my - 2]);
+      dm += o->trp[0] * (a * a + b * b) + o->trp[my - 1] * (c * c + d * d);
+    }
+    double du = creal(u[my - 1]) - creal(u[0]);
+    o->diag[2] = 0.25 * (o->y[my - 1] - o->y[0]) - dm / (du * du);
+    double fac = 1.0 / ((double)o->mgalx * o->mgalz), mt = 0.0;
+    for (int j = 0; j < my; j++) mt += fac * rhom[j] * o->hy[j];
+    o->diag[6] = mt;
+  }
+  free(rhom);
+  if (do_cfl) {
+    double hxalp = o->alp * (o->mgalx - 1) / M_PI, hzbet = o->bet * (o->mgalz - 1) / M_PI;
+    double hmin = o->hy[0];
+    for (int j = 1; j < my; j++) hmin = fmin(hmin, o->hy[j]);
+    double hyy = 1.0 / hmin;
+    hyy = 2.0 / o->Re * pow(fmax(hyy, fmax(hxalp / 2, hzbet / 2)), 2); /* viscous limit */
+    double c0 = fmax(cfl[0] * hxalp, fmax(cfl[1], cfl[2] * hzbet));
+    double reig = fmax(c0, hyy);
+    o->Deltat = (double)(float)(o->cfl / reig); /* Deltat is real*4 */
+  }
+}
+
+/* tauij2 / tensor2 of lomacte/cross.f:1738-1908: d(rho) = 1/(T + Delta T)
+ * - 1/T = -Delta T / (T (T + Delta T)) in physical space. */
+static void tauij2_14(lmo *o, cplx *T, cplx *dT) {
+  int nkx = o->nkx, mgalz = o->mgalz, mgalx = o->mgalx, my = o->my;
+  cplx *in2[2] = {T, dT};
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for collapse(2) schedule(static)
+    for (int f = 0; f < 2; f++)
+      for (int i = 0; i < nkx; i++) zinv_plane(o, i, in2[f], o->ln[f], buf, out);
+    free(buf); free(out);
+  }
+  size_t nlines = (size_t)mgalz * my;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *a = malloc(sizeof(double) * mgalx * 2), *b = a + mgalx;
+    cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
+#pragma omp for schedule(static)
+    for (long L = 0; L < (long)nlines; L++) {
+      cplx *s0 = o->ln[0] + (size_t)L * nkx, *s1 = o->ln[1] + (size_t)L * nkx;
+      xinv2(o, s0, s1, a, b, buf, fo);
+      for (int x = 0; x < mgalx; x++) a[x] = -b[x] / (a[x] * (a[x] + b[x])); /* :1881 */
+      xfwd2(o, a, NULL, s0, NULL, buf, fo);
+    }
+    free(a); free(buf); free(fo);
+  }
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
+#pragma omp for schedule(static)
+    for (int i = 0; i < nkx; i++) zfwd_plane(o, i, o->ln[0], T, buf, out);
+    free(buf); free(out);
+  }
+}
+
+/* One RK3 substep of the 2014 variant: lomacte/cross.f:286-989. */
+static void substep14(lmo *o, int r, int ihist) {
+  int my = o->my, mz = o->mz;
+  double dtxi = o->Deltat * o->xi[r];
+  double ire = o->ire;
+  cplx *mxw = o->w_mx, *myw = o->w_my, *mzw = o->w_mz, *nxw = o->w_nx, *nyw = o->w_ny, *nzw = o->w_nz;
+  cplx *t12 = o->w_t12, *t13 = o->w_t13, *t23 = o->w_t23, *drho = o->w_drho, *chwk = o->w_chwk, *chwk2 = o->w_chwk2;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 20 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
+      size_t b = (size_t)m * my;
+      /* work copies and BCs: lomacte/cross.f:293-320 */
+      for (int j = 0; j < my; j++) { nxw[b + j] = o->vor[b + j]; nyw[b + j] = o->psi[b + j]; }
+      nxw[b + 1] = nxw[b + 2];
+      nxw[b + 0] = nxw[b + 2];
+      nxw[b + my - 2] = nxw[b + my - 3];
+      nxw[b + my - 1] = nxw[b + my - 2];
+      o->phi[b] = 0;
+      o->phi[b + my - 1] = 0;
+      /* (1) Lapvdvhom: :322-329 */
+      lapvdvhom_c(o, o->phi + b, myw + b, nzw + b, rK, sc);
+      /* (2) mx, mz: :353-366 */
+      cplx ta = 0, tb = 0;
+      if (rK != 0.0) { ta = I * kx / rK; tb = I * kz / rK; }
+      for (int j = 0; j < my; j++) {
+        mxw[b + j] = nzw[b + j] * ta - nxw[b + j] * tb;
+        mzw[b + j] = nzw[b + j] * tb + nxw[b + j] * ta;
+      }
+      /* T saved, xi-updates (T too, from its spectral RHS): :368-396 */
+      for (int j = 0; j < my; j++) {
+        drho[b + j] = o->scal[b + j];
+        o->vor[b + j] = o->vor[b + j] + o->ten12p[b + j] * dtxi;
+        o->phi[b + j] = o->phi[b + j] + o->ten13p[b + j] * dtxi;
+        o->scal[b + j] = o->scal[b + j] + o->rts[b + j] * dtxi;
+        chwk2[b + j] = o->rts[b + j] * dtxi;
+      }
+      /* d(psi)/dy and rho u_i: :400-444 */
+      deryr2_c(o, nyw + b, t23 + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        mxw[b + j] = mxw[b + j] + I * kx * nyw[b + j];
+        mzw[b + j] = mzw[b + j] + I * kz * nyw[b + j];
+        myw[b + j] = myw[b + j] + t23[b + j];
+      }
+      /* (4) derivatives of the saved T: :486-519 */
+      deryr2_c(o, drho + b, t13 + b, w1, w2, tt1, tt2);
+      deryyr2_c(o, drho + b, nyw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        nyw[b + j] = nyw[b + j] - rK * drho[b + j];
+        t23[b + j] = I * kz * drho[b + j];
+        t12[b + j] = I * kx * drho[b + j];
+      }
+    }
+    free(s);
+  }
+  /* 00 modes: :447-461 */
+  for (int j = 0; j < my; j++) { mxw[j] = o->u00wk[j]; myw[j] = o->v00wk[j]; mzw[j] = o->w00wk[j]; }
+  for (int j = 1; j < my - 1; j++) {
+    o->u00wk[j] += dtxi * o->rf0u[j];
+    o->w00wk[j] += dtxi * o->rf0w[j];
+  }
+  /* (5) foup2, new Deltat in the first substep of a CFL step: :544-556 */
+  int do_cfl = (r == 0 && o->icfl == 1 && o->dtmode == 0);
+  cplx *rtn = chwk; /* RHS(T) of this substep */
+  cplx *in8[8] = {mxw, myw, mzw, nyw, t12, t13, t23, drho};
+  cplx *out10[10] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, rtn};
+  foup2_14(o, do_cfl, ihist && r == 0, in8, out10);
+  if (r == 0) o->diag[1] = o->Deltat;
+  double dtgamma = o->Deltat * o->gama[r];
+  dtxi = o->Deltat * o->xi[r];
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 20 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k];
+      size_t b = (size_t)m * my;
+      /* (6a) T: :563-570 */
+      for (int j = 0; j < my; j++) {
+        o->scal[b + j] = o->scal[b + j] + dtgamma * rtn[b + j];
+        chwk2[b + j] = chwk2[b + j] + dtgamma * rtn[b + j];
+        o->rts[b + j] = rtn[b + j];
+      }
+      /* (6b) N_x, N_y, N_z: :594-625 */
+      deryr2_c(o, nyw + b, nyw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) nyw[b + j] = -I * kx * t12[b + j] - nyw[b + j] - I * kz * t23[b + j];
+      deryr2_c(o, t12 + b, t12 + b, w1, w2, tt1, tt2);
+      deryr2_c(o, t23 + b, t23 + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        nxw[b + j] = -I * kx * nxw[b + j] - t12[b + j] - I * kz * t13[b + j];
+        nzw[b + j] = -I * kx * t13[b + j] - t23[b + j] - I * kz * nzw[b + j];
+      }
+    }
+    free(s);
+  }
+  /* 00 modes: :628-653 (dw and the hy-weighted H00 as in the 2017 path) */
+  {
+    double *dudy = xcalloc(my, 8);
+    for (int j = 0; j < my; j++) { o->rf0u[j] = creal(mxw[j]); o->rf0w[j] = creal(mzw[j]); }
+    if (r == 2 && ihist) {
+      lmo_deryr(o, o->rf0u, dudy);
+      double dw = 0.0;
+      for (int j = 0; j < my; j++) dw = fmax(fabs(dudy[j]), dw);
+      o->diag[3] = 1.0 / dw;
+      o->diag[4] = o->diag[3] * o->Re;
+    }
+    lmo_deryyr(o, o->rf0u, o->rf0u);
+    lmo_deryyr(o, o->rf0w, o->rf0w);
+    for (int j = 0; j < my; j++) {
+      o->rf0u[j] = creal(nxw[j]) + ire * o->rf0u[j];
+      o->rf0w[j] = creal(nzw[j]) + ire * o->rf0w[j];
+    }
+    if (r == 2 && ihist) {
+      double hu = 0, hw = 0;
+      for (int j = 0; j < my; j++) { hu += o->rf0u[j] * o->hy[j]; hw += o->rf0w[j] * o->hy[j]; }
+      o->diag[10] = 0.25 * hu;
+      o->diag[11] = 0.25 * hw;
+    }
+    free(dudy);
+  }
+  /* d(rho) from T and Delta T: :877 */
+  tauij2_14(o, drho, chwk2);
+  const double den = dtgamma + dtxi;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 24 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
+    cplx *c1 = malloc(sizeof(cplx) * 2 * my), *c2 = c1 + my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
+      size_t b = (size_t)m * my;
+      /* vorticities, Laplacians, RHS(Omega_y), RHS(phi): :656-872 */
+      deryr2_c(o, mxw + b, t12 + b, w1, w2, tt1, tt2);
+      deryr2_c(o, mzw + b, t23 + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        t23[b + j] = t23[b + j] - I * kz * myw[b + j];
+        t13[b + j] = I * kz * mxw[b + j] - I * kx * mzw[b + j];
+        t12[b + j] = I * kx * myw[b + j] - t12[b + j];
+      }
+      deryyr2_c(o, t13 + b, c1, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t13[b + j] = c1[j] - rK * t13[b + j];
+      for (int j = 0; j < my; j++) t23[b + j] = I * kz * t23[b + j] - I * kx * t12[b + j];
+      deryyr2_c(o, t23 + b, c1, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t23[b + j] = c1[j] - rK * t23[b + j];
+      for (int j = 0; j < my; j++) t12[b + j] = I * kz * nxw[b + j] - I * kx * nzw[b + j] + ire * t13[b + j];
+      for (int j = 0; j < my; j++) nxw[b + j] = I * kx * nxw[b + j] + I * kz * nzw[b + j];
+      deryr2_c(o, nxw + b, nxw + b, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) t13[b + j] = -rK * nyw[b + j] - nxw[b + j] - ire * t23[b + j];
+      /* (10) RK3 update: :912-928 */
+      for (int j = 0; j < my; j++) {
+        o->vor[b + j] = o->vor[b + j] + dtgamma * t12[b + j];
+        o->phi[b + j] = o->phi[b + j] + dtgamma * t13[b + j];
+        o->ten12p[b + j] = t12[b + j];
+        o->ten13p[b + j] = t13[b + j];
+      }
+      /* psi(n+1) = Lapvdvhom(-d(rho)/(dt (gamma + xi))): :974-983 */
+      for (int j = 0; j < my; j++) c2[j] = -drho[b + j] / den;
+      lapvdvhom_c(o, c2, o->psi + b, c1, rK, sc);
+    }
+    free(s);
+    free(c1);
+  }
+  /* 00 modes: :950-1002 */
+  {
+    for (int j = 1; j < my - 1; j++) {
+      o->u00wk[j] += dtgamma * o->rf0u[j];
+      o->w00wk[j] += dtgamma * o->rf0w[j];
+    }
+    double mu = 0, mv = 0, mw = 0;
+    for (int j = 0; j < my; j++) {
+      mu += o->u00wk[j] * o->hy[j];
+      mv += o->v00wk[j] * o->hy[j];
+      mw += o->w00wk[j] * o->hy[j];
+    }
+    o->diag[7] = mu; o->diag[8] = mv; o->diag[9] = mw;
+    /* cumulative trapezoid of d(rho)00 / (dt (gamma + xi)) */
+    o->rf0v[0] = 0.0;
+    for (int j = 0; j < my - 1; j++)
+      o->rf0v[j + 1] = o->rf0v[j] + 0.5 * (o->y[j + 1] - o->y[j]) * (creal(drho[j + 1]) / den + creal(drho[j]) / den);
+    double trapz = o->rf0v[my - 1];
+    o->diag[5] = trapz;
+    for (int j = 0; j < my; j++) {
+      o->rf0v[j] = o->rf0v[j] - o->rhobot * trapz / (o->rhotop + o->rhobot);
+      o->v00wk[j] = -o->rf0v[j];
+    }
+  }
+}
+
 /* Time loop body: cross.f:225-1226 (stats, images and .cf output are the
- * caller's business). */
+ * caller's business); the 2014 variant follows lomacte/cross.f:212-1040,
+ * whose Deltat changes inside the first substep of a CFL step. */
 int lmo_step(lmo *o, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     int istep = ++o->istep_total;
@@ -1145,6 +1492,13 @@ int lmo_step(lmo *o, int nsteps) {
     int ihist = 1; /* diagnostics every step */
     o->diag[0] = o->time;
     o->diag[1] = o->Deltat;
+    if (o->variant == 1) {
+      for (int r = 0; r < 3; r++) substep14(o, r, ihist);
+      o->time += o->Deltat;
+      o->icfl = 0;
+      o->diag[12] = o->Deltat;
+      continue;
+    }
     for (int r = 0; r < 3; r++) substep(o, r, ihist);
     o->time += o->Deltat;
     if (o->dtmode == 0 && o->icfl == 1) {
@@ -1156,11 +1510,18 @@ int lmo_step(lmo *o, int nsteps) {
   return 0;
 }
 
+int lmo_set_variant(lmo *o, int variant) {
+  if (!o || variant < 0 || variant > 1) return -1;
+  o->variant = variant;
+  return 0;
+}
+
 /* One substep with RK coefficient r (0..2) on the current state, without
  * the step bookkeeping: used only to time bounded CPU samples. */
 int lmo_substep(lmo *o, int r) {
   if (r < 0 || r > 2) return -1;
-  substep(o, r, 0);
+  if (o->variant == 1) substep14(o, r, 0);
+  else substep(o, r, 0);
   return 0;
 }
 

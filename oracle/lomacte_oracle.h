@@ -48,6 +48,9 @@ int lmo_get_state(const lmo *o, double *vor, double *phi, double *psi,
                   double *time);
 /* Advance nsteps full RK3 steps (3 substeps each). */
 int lmo_step(lmo *o, int nsteps);
+/* 0: trunk/lomacte3 (2017, default); 1: the 2014 variant trunk/lomacte
+ * (spectral T, d(rho) transform round trip, Dirichlet psi). */
+int lmo_set_variant(lmo *o, int variant);
 
 /* One substep with RK coefficient r on the current state (timing samples). */
 int lmo_substep(lmo *o, int r);

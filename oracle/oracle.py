@@ -52,6 +52,7 @@ def lib():
         L.lmo_set_state.argtypes = [ctypes.c_void_p] + [_dp] * 7 + [ctypes.c_double]
         L.lmo_get_state.argtypes = [ctypes.c_void_p] + [_dp] * 8
         L.lmo_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.lmo_set_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.lmo_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.lmo_get_diag.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_get_coefs.argtypes = [ctypes.c_void_p] + [_dp] * 7
@@ -74,7 +75,7 @@ class Oracle:
     """FP64 CPU restatement of one lomacte run (cross1's time loop)."""
 
     def __init__(self, mgalx, mgalz, y, Re, alp, bet, peclet=None, cfl=0.5,
-                 ncfl=10, dtmode=1, dt0=0.01, nthreads=None):
+                 ncfl=10, dtmode=1, dt0=0.01, nthreads=None, variant=0):
         self.y = np.ascontiguousarray(y, dtype=np.float64)
         self.my = len(self.y)
         self.mgalx, self.mgalz = mgalx, mgalz
@@ -91,6 +92,8 @@ class Oracle:
                                   peclet, cfl, ncfl, dtmode, dt0, nthreads)
         if not self.h:
             raise ValueError("oracle: bad grid")
+        if variant:
+            lib().lmo_set_variant(self.h, int(variant))
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -17,7 +17,8 @@ def case(nx=32, nz=32, ny=65, seed=0, s=4.0, dt_mode=1, dt=0.01, Re=160.0, **kw)
 
 def oracle_for(p, y, st, nthreads=None):
     o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, peclet=None if p.peclet <= 0 else p.peclet,
-               cfl=p.cfl, ncfl=p.ncfl, dtmode=p.dt_mode, dt0=p.dt, nthreads=nthreads)
+               cfl=p.cfl, ncfl=p.ncfl, dtmode=p.dt_mode, dt0=p.dt, nthreads=nthreads,
+               variant=getattr(p, "variant", 0))
     o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"], st.get("time", 0.0))
     return o
 
