@@ -219,7 +219,9 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 // [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
 // current tile is transformed.
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
+// FP32 butterflies: at most about 128 registers, so that eight 64-thread
+// blocks (or the same thread count in larger blocks) share an SM
+__global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) ? 512 / Geo<N1, N2>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
@@ -234,6 +236,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
   __shared__ int s_ok;
   __shared__ unsigned long long s_tmax[ZB], s_vmax;
   __shared__ double s_red[3][8];
+  __shared__ double s_min[6], s_est[11];  // mixed form, per tile
   const int nzk = (d.mgalz + ZB - 1) / ZB;
   auto issue = [&](int t) {
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
@@ -263,6 +266,33 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
     if (!s_ok) return;
     ph ^= 1;
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
+    if constexpr (sizeof(ST) == sizeof(float2)) {  // mixed form: see s_min / s_est below
+      const int q = threadIdx.x;
+      if (q < 6) s_min[q] = d.mi[(size_t)q * d.my + y];
+      if (q < 11) {
+        double e;
+        if (d.mean_ok) {
+          e = d.mo_prev[(size_t)q * d.my + y] / ((double)d.mgalx * (double)d.mgalz);
+        } else {  // products of the input means
+          const double ru = d.mi[y], rv = d.mi[(size_t)d.my + y], rw = d.mi[(size_t)2 * d.my + y];
+          const double T = d.mi[(size_t)5 * d.my + y];
+          const double u = ru * T, v = rv * T, w = rw * T;
+          switch (q) {
+            case OU: e = u; break;
+            case OV: e = v; break;
+            case OW: e = w; break;
+            case ORUU: e = ru * u; break;
+            case ORVV: e = rv * v; break;
+            case ORWW: e = rw * w; break;
+            case ORUV: e = ru * v; break;
+            case ORUW: e = ru * w; break;
+            case ORVW: e = rv * w; break;
+            default: e = 0.0; break;
+          }
+        }
+        s_est[q] = e;
+      }
+    }
     // zero the dealiased gap kx = nkx .. N-nkx of the 4 input lines
     const int gap = N - 2 * nkx + 1;
     for (int idx = threadIdx.x; idx < 4 * ZB * gap; idx += blockDim.x) {
@@ -297,24 +327,12 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
     }
     F::template nat2perm<+1>(W, 4 * ZB, LD, wtwx<CT>(d));
 
-    // mixed form: FP64 00 profiles of the inputs at this y, and the values
-    // subtracted from the outputs before they are rounded to FP32
+    // mixed form: s_min / s_est (filled before the transform above) hold the
+    // FP64 00 profiles of the inputs at this y and the values subtracted from
+    // the outputs before they are rounded to FP32
     constexpr bool MX = sizeof(ST) == sizeof(float2);
-    double m_in[6], est[11], acc[11];
+    double acc[11];
     if constexpr (MX) {
-#pragma unroll
-      for (int q = 0; q < 6; q++) m_in[q] = d.mi[(size_t)q * d.my + y];
-      if (d.mean_ok) {
-        const double inn = 1.0 / ((double)d.mgalx * (double)d.mgalz);
-#pragma unroll
-        for (int o = 0; o < 11; o++) est[o] = d.mo_prev[(size_t)o * d.my + y] * inn;
-      } else {  // products of the input means
-        const double eu = m_in[0] * m_in[5], ev = m_in[1] * m_in[5], ew = m_in[2] * m_in[5];
-        est[OU] = eu; est[OV] = ev; est[OW] = ew;
-        est[ORUU] = m_in[0] * eu; est[ORVV] = m_in[1] * ev; est[ORWW] = m_in[2] * ew;
-        est[ORUV] = m_in[0] * ev; est[ORUW] = m_in[0] * ew; est[ORVW] = m_in[1] * ew;
-        est[ODRHO] = 0.0; est[ODT] = 0.0;
-      }
 #pragma unroll
       for (int o = 0; o < 11; o++) acc[o] = 0.0;
     }
@@ -331,7 +349,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
         CT *c1 = c0 + (size_t)ZB * LD, *c2 = c1 + (size_t)ZB * LD, *c3 = c2 + (size_t)ZB * LD;
         double2 p0 = to_d2(*c0), p1 = to_d2(*c1), p2 = to_d2(*c2), p3 = to_d2(*c3);
         if constexpr (MX) {
-          p0.x += m_in[0]; p0.y += m_in[1]; p1.x += m_in[2]; p1.y += m_in[3]; p2.y += m_in[4]; p3.y += m_in[5];
+          p0.x += s_min[0]; p0.y += s_min[1]; p1.x += s_min[2]; p1.y += s_min[3]; p2.y += s_min[4];
+          p3.y += s_min[5];
         }
         const double ru = p0.x, rv = p0.y, rw = p1.x, lapT = p1.y, tx = p2.x, ty = p2.y, tz = p3.x, T = p3.y;
         const double rhp = rh[j];
@@ -354,7 +373,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xphys(Dev d, int rk, int do
 #pragma unroll
           for (int q = 0; q < 11; q++) {
             acc[q] += o[q];
-            o[q] -= est[q];
+            o[q] -= s_est[q];
           }
         }
         *c0 = from_d2<CT>(make_double2(o[OU], o[OV]));
