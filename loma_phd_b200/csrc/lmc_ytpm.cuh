@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
       const double2 v = r.pop();
       w.push(t == 0 ? czero() : v);
     }
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       const double2 v = r.pop();
       w.push(j + 3 == my - 1 ? czero() : v);
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
     U.start(d, M.m);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       double2 x = pb(r.pop(), h, U);
       if (zero) x = czero();
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
     Hist h;
     h.clear();
     for (int t = 0; t < 3; t++) w.push(r.pop());
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       w.push(r.pop());
       s1[(size_t)j * ld] = d1f(d, j, w, h);
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(TB) t_lapv(Dev d) {
     r.start(s1, ld, my, -1, my - 1);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) put(DMY, ld, j, d1b(d, j, r.pop(), h));
   }
 }
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
     Hist h;
     h.clear();
     for (int t = 0; t < 3; t++) w.push(rpsi.pop());
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       w.push(rpsi.pop());
       const double2 ps = w.c();
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(TB) t_assemble(Dev d, int rk) {
     CT *RV = wsb<CT>(d, SB_RV) + M.m;
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       double2 a = cadd(d1b(d, j, r.pop(), h), rmy.pop());
       if (m00) {
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
     h2.clear();
     w.push(wb);
     for (int t = 1; t < 3; t++) w.push(r.pop());
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       const double2 v = r.pop();
       w.push((!V && j + 3 == my - 1) ? wt_bc : v);
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
     Hist h1, h2;
     h1.clear();
     h2.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 dT = d1b(d, j, r1.pop(), h1);
       const double2 lT = csub(d2b(d, j, r2.pop(), h2), cscale(M.k2, rT.pop()));
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
       wy.push(csub(cik(kz, u), cik(kx, w)));  // omega_y, cross.f:760
     };
     for (int t = 0; t < 3; t++) feed();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       feed();
       s1[(size_t)j * ld] = d1f(d, j, ww, h1);
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     Hist h;
     h.clear();
     for (int t = 0; t < 3; t++) wc.push(cadd(cik(kx, rx.pop()), cik(kz, rz.pop())));
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       wc.push(cadd(cik(kx, rx.pop()), cik(kz, rz.pop())));
       s4[(size_t)j * ld] = d1f(d, j, wc, h);
@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     Hist h1, h2;
     h1.clear();
     h2.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 dw = d1b(d, j, r1.pop(), h1), du = d1b(d, j, r2.pop(), h2), v = rv.pop();
       const double2 ox = csub(dw, cik(kz, v));                 // cross.f:757
@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     Hist h3, h4;
     h3.clear();
     h4.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 u = ru.pop(), w = rw.pop(), nx = rx.pop(), nz = rz.pop(), ny = ry.pop();
       const double2 oy = csub(cik(kz, u), cik(kx, w));
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     Hist h;
     h.clear();
     for (int t = 0; t < 3; t++) w.push(r.pop());
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       w.push(r.pop());
       s2[(size_t)j * ld] = d2f(d, j, w, h);
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(TB) t_post2(Dev d, int rk) {
     rph.start(d.phi + M.m, ld, my, -1, my - 1);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 lc = csub(d2b(d, j, r2.pop(), h), cscale(k2, rc.pop()));
       const double2 rp = csub(rrp.pop(), cscale(d.ire, lc));
@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
     Hist h;
     h.clear();
     for (int t = 0; t < 3; t++) w.push(cscale(sc, r.pop()));
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       w.push(cscale(sc, r.pop()));
       s1[(size_t)j * ld] = pf(d, j, w, h, L);
@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
     U.start(d, M.m);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 x = pb(r.pop(), h, U);
       put(d.psi + M.m, ld, j, zero ? czero() : x);
@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
     U.start(d, M.m);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 x = pb(r.pop(), h, U);
       const double eb = __ldg(d.r_ebot + j), et = __ldg(d.r_etop + j);
@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
     RdS<8> rv1, rv2;
     rv1.start(d.V12t + M.m, 2 * n, my, 1, 0);
     rv2.start(d.V12t + n + M.m, 2 * n, my, 1, 0);
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       double2 x = r.pop();
       const double v1 = rv1.pop(), v2 = rv2.pop();
@@ -821,7 +821,7 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
     LRows<4> L;
     if (op >= 3) L.start(d, M.m);
     for (int t = 0; t < 3; t++) w.push(r.pop());
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       w.push(r.pop());
       s1[(size_t)j * ld] = op == 1 ? d1f(d, j, w, h) : op == 2 ? d2f(d, j, w, h) : pf(d, j, w, h, L);
@@ -835,7 +835,7 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
     if (op >= 3) U.start(d, M.m);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) {
       const double2 w = r.pop();
       double2 x = op == 1 ? d1b(d, j, w, h) : op == 2 ? d2b(d, j, w, h) : pb(w, h, U);
@@ -861,7 +861,7 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
       Hist h;
       h.clear();
       for (int t = 0; t < 3; t++) w.push(r.pop());
-      #pragma unroll 2
+      #pragma unroll 4
       for (int j = 0; j < my; j++) {
         w.push(r.pop());
         s1[(size_t)j * ld] = d1f(d, j, w, h);
@@ -871,7 +871,7 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
     r.start(s1, ld, my, -1, my - 1);
     Hist h;
     h.clear();
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = my - 1; j >= 0; j--) out2[(size_t)j * ld] = d1b(d, j, r.pop(), h);
   } else if (op == 4) {
     const double *ai = d.AAinv + (size_t)M.m * 4;
@@ -879,7 +879,7 @@ __global__ void __launch_bounds__(TB) t_op_y(Dev d, int op, const double2 *in, d
     const double2 c1 = make_double2(-(a0 * db.x + a1 * dt.x), -(a0 * db.y + a1 * dt.y));
     const double2 c2 = make_double2(-(a2 * db.x + a3 * dt.x), -(a2 * db.y + a3 * dt.y));
     const size_t n = (size_t)d.nmode;
-    #pragma unroll 2
+    #pragma unroll 4
     for (int j = 0; j < my; j++) {
       double2 x = out[(size_t)j * ld];
       const double v1 = __ldg(d.V12t + (size_t)j * 2 * n + M.m), v2 = __ldg(d.V12t + (size_t)j * 2 * n + n + M.m);
@@ -914,7 +914,7 @@ __global__ void k_psi00_14(Dev d, int rk) {
   const int my = d.my;
   const double dt = d.scal_d[0], dtg = dt * d.gama[rk], den = dt * (d.gama[rk] + d.xi[rk]);
   double mu = 0.0, mv = 0.0, mw = 0.0;
-  #pragma unroll 2
+  #pragma unroll 4
   for (int j = 0; j < my; j++) {
     if (j >= 1 && j <= my - 2) {
       d.u00[j] += dtg * d.rf0u[j];
@@ -936,7 +936,7 @@ __global__ void k_psi00_14(Dev d, int rk) {
   }
   const double trapz = f;
   const double sh = d.scal_d[3] * trapz / (d.scal_d[4] + d.scal_d[3]);
-  #pragma unroll 2
+  #pragma unroll 4
   for (int j = 0; j < my; j++) {
     d.rf0v[j] -= sh;
     d.v00[j] = -d.rf0v[j];
