@@ -40,11 +40,20 @@ template <int N1, int N2>
 struct Geo {
   static constexpr int N = N1 * N2;
   static constexpr int LD = Four<N1, N2>::LD | 1;           // odd line stride
-  static constexpr int KB = (64 / N1) > 0 ? (64 / N1) : 1;  // kx lines per z-transform block
-  static constexpr int ZT = round32(KB * N1);               // threads of a z-transform block
+  static constexpr int KB = (64 / N1) > 0 ? (64 / N1) : 1;  // kx lines per z-transform block (FP64)
+  static constexpr int ZT = round32(KB * N1);               // threads of a z-transform block (FP64)
   static constexpr int ZB = (16 / N1) > 0 ? (16 / N1) : 1;  // z lines per x-transform block
   static constexpr int XT = round32(4 * ZB * N1);           // threads of an x-transform block
   static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
+};
+
+// z-transform blocks by storage type: twice as many kx lines for FP32
+// storage, so that every strided z row moves the same number of bytes
+template <int N1, int N2, typename ST>
+struct ZGeo {
+  static constexpr int W = sizeof(ST) == sizeof(float2) ? 2 : 1;
+  static constexpr int KB = (64 * W / N1) > 0 ? (64 * W / N1) : 1;
+  static constexpr int ZT = round32(KB * N1);
 };
 
 __host__ __device__ constexpr size_t round16(size_t b) { return (b + 15) / 16 * 16; }
@@ -64,11 +73,11 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // mode 0: the eight transform inputs of the substep; mode 1 (2014 variant,
 // FP64): T before the substep and Delta T, for d(rho) (lomacte/cross.f:1760-1770)
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles, int mode) {
+__global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zinv(Dev d, int ntiles, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
-  constexpr int KB = G::KB, LD = G::LD;
+  constexpr int KB = ZGeo<N1, N2, ST>::KB, LD = G::LD;
   constexpr int E = 16 / (int)sizeof(ST);  // stored values per 16-byte unit
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *W = (CT *)smraw;
@@ -153,17 +162,18 @@ __global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zinv(Dev d, int ntiles, int
 // mode 0: the substep's outputs (field blockIdx.z in place); mode 1 (2014
 // variant): d(rho) from z-physical buffer 0 into the d(rho) spectral slot
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::ZT) k_zfwd(Dev d, int mode) {
+__global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zfwd(Dev d, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *sm = (CT *)smraw;
-  const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * G::KB;
-  const int nb = min(G::KB, d.nkx - i0);
+  constexpr int KB = ZGeo<N1, N2, ST>::KB;
+  const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * KB;
+  const int nb = min(KB, d.nkx - i0);
   const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.nkx + i0;
-  for (int idx = threadIdx.x; idx < F::N * G::KB; idx += blockDim.x) {
-    const int z = idx / G::KB, il = idx - z * G::KB;
+  for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
+    const int z = idx / KB, il = idx - z * KB;
     if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.nkx + il));
   }
   __syncthreads();
@@ -526,9 +536,10 @@ template <int N1, int N2, typename CT, typename ST>
 struct Launch {
   using G = Geo<N1, N2>;
   static constexpr int E = 16 / (int)sizeof(ST);
-  static size_t zsm() { return (size_t)G::KB * G::LD * sizeof(CT); }
+  using ZG = ZGeo<N1, N2, ST>;
+  static size_t zsm() { return (size_t)ZG::KB * G::LD * sizeof(CT); }
   static size_t zinv_sm(int mz) {
-    return round16(sizeof(CT) * G::KB * G::LD) + ((size_t)G::KB * mz + 2 * E) * sizeof(ST);
+    return round16(sizeof(CT) * ZG::KB * G::LD) + ((size_t)ZG::KB * mz + 2 * E) * sizeof(ST);
   }
   static size_t xsm() { return round16(sizeof(CT) * 4 * G::ZB * G::LD); }
   static size_t xphys_sm(int nkx) {
@@ -545,14 +556,14 @@ struct Launch {
     return g < ntiles ? g : ntiles;
   }
   static void zinv(const Dev &d, int mode, cudaStream_t s) {
-    const int ntiles = (mode ? 2 : 8) * d.my * ((d.nkx + G::KB - 1) / G::KB);
+    const int ntiles = (mode ? 2 : 8) * d.my * ((d.nkx + ZG::KB - 1) / ZG::KB);
     const size_t sm = zinv_sm(d.mz);
-    const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, G::ZT, sm, ntiles);
-    k_zinv<N1, N2, CT, ST><<<g, G::ZT, sm, s>>>(d, ntiles, mode);
+    const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, ZG::ZT, sm, ntiles);
+    k_zinv<N1, N2, CT, ST><<<g, ZG::ZT, sm, s>>>(d, ntiles, mode);
   }
   static void zfwd(const Dev &d, int mode, cudaStream_t s) {
-    dim3 g((d.nkx + G::KB - 1) / G::KB, d.my, mode ? 1 : (d.variant ? 10 : 11));
-    k_zfwd<N1, N2, CT, ST><<<g, G::ZT, zsm(), s>>>(d, mode);
+    dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : 11));
+    k_zfwd<N1, N2, CT, ST><<<g, ZG::ZT, zsm(), s>>>(d, mode);
   }
   static void xdrho(const Dev &d, cudaStream_t s) {
     if constexpr (sizeof(CT) == sizeof(double2) && sizeof(ST) == sizeof(double2)) {
