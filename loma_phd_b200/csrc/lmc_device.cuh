@@ -512,8 +512,9 @@ struct Four {
   __device__ static __forceinline__ int sk(int n) { return n + n / N1; }
 
   // natural -> permuted: X[k2 + N2 k1] lands at skew position k1 + N1 k2
-  template <int SIGN>
+  template <int SIGN, int U = 1>
   __device__ static void nat2perm(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
+    #pragma unroll U
     for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
       const int b = idx / N1, n1 = idx - b * N1;
       CT *p = sm + (size_t)b * ld + n1;
@@ -533,6 +534,7 @@ struct Four {
       }
     }
     __syncthreads();
+    #pragma unroll U
     for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
       const int b = idx / N2, k2 = idx - b * N2;
       CT *p = sm + (size_t)b * ld + k2 * (N1 + 1);
@@ -547,8 +549,9 @@ struct Four {
   }
 
   // permuted -> natural (transpose of nat2perm)
-  template <int SIGN>
+  template <int SIGN, int U = 1>
   __device__ static void perm2nat(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
+    #pragma unroll U
     for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
       const int b = idx / N2, k2 = idx - b * N2;
       CT *p = sm + (size_t)b * ld + k2 * (N1 + 1);
@@ -568,6 +571,7 @@ struct Four {
       }
     }
     __syncthreads();
+    #pragma unroll U
     for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
       const int b = idx / N1, n1 = idx - b * N1;
       CT *p = sm + (size_t)b * ld + n1;

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zfwd(Dev d, int mode) 
     if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.nkx + il));
   }
   __syncthreads();
-  F::template perm2nat<-1>(sm, nb, G::LD, wtwz<CT>(d));
+  F::template perm2nat<-1, 2>(sm, nb, G::LD, wtwz<CT>(d));
   const Re dn = (Re)(1.0 / (double)F::N);
   for (int il = 0; il < nb; il++) {
     ST *row = wsb<ST>(d, f) + ((size_t)y * d.nkx + i0 + il) * d.mz;
