@@ -62,17 +62,16 @@ ALGO = {
     "psi": lambda S, Z, P, w: S * 16 + S * w + S * 7 * 8 // 2,
 }
 
-# DRAM bytes (read + write) per launch measured by ncu on the 256x65x256 case
-# of this workload (profiles/kernels_lomacte_fp64_256x65x256.md).  Traffic
+# DRAM bytes (read + write) per launch measured by ncu (full-set capture of
+# the 256x65x256 case of this workload, one launch per kernel).  Traffic
 # grows in proportion to ny at fixed x/z sizes, so for nx = nz = 256 it is
-# scaled by ny/65; other sizes report null.
+# scaled by ny/65; other sizes, and kernels not captured, report null.
 NCU_TRAFFIC_256x65 = {
-    "lapv": 226.3e6, "assemble": 368.4e6, "tder": 79.9e6, "zinv": 603.6e6, "xphys": 1064.6e6,
-    "zfwd": 900.8e6, "post1": 368.6e6, "post2": 469.6e6, "psi": 265.6e6,
+    "zinv": 611.0e6, "xphys": 1065.9e6, "zfwd": 902.9e6, "post1": 612.3e6, "post2": 956.4e6,
 }
-
-# The same for the mixed form (not captured yet: null).
-NCU_TRAFFIC_MIXED_256x65 = {}
+NCU_TRAFFIC_MIXED_256x65 = {
+    "zinv": 261.4e6, "xphys": 587.2e6, "zfwd": 432.9e6, "post1": 411.1e6, "post2": 768.5e6,
+}
 
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
                2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
