@@ -24,6 +24,8 @@ struct lmc_handle {
   lmc::RK3 rk;
   lmc::Dev d;
   cudaStream_t s = nullptr;
+  cudaStream_t s2 = nullptr;  // side stream for the independent kernels of a substep
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::vector<void *> allocs;
   int steps = 0;
   int err = 0;
@@ -120,20 +122,27 @@ bool mode_parallel(int nmode) {
   return nmode >= 16384;
 }
 
-// Record a profiling boundary: the work enqueued after it (until the next
-// boundary) is attributed to kernel id `kid`.
-void prof_mark(lmc_handle *h, int kid) {
-  if (!h->prof) return;
-  if (h->ev_used == h->ev_pool.size()) {
-    if (h->ev_pool.size() >= 65536) return;
+// Profiling: a (start, stop) pair of events around each group of launches,
+// recorded on the stream that runs the group; lmc_profile_read sums the
+// pairs per kernel id.  Returns the pair's index, or -1 when not profiling.
+int prof_begin(lmc_handle *h, cudaStream_t st) {
+  if (!h->prof) return -1;
+  while (h->ev_used + 2 > h->ev_pool.size()) {
+    if (h->ev_pool.size() >= 65536) return -1;
     cudaEvent_t e;
-    if (cudaEventCreate(&e) != cudaSuccess) return;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
     h->ev_pool.push_back(e);
     h->ev_kid.push_back(-1);
   }
-  cudaEventRecord(h->ev_pool[h->ev_used], h->s);
-  h->ev_kid[h->ev_used] = kid;
-  h->ev_used++;
+  const int a = (int)h->ev_used;
+  cudaEventRecord(h->ev_pool[a], st);
+  h->ev_used += 2;
+  return a;
+}
+void prof_end(lmc_handle *h, int kid, int a, cudaStream_t st) {
+  if (a < 0) return;
+  cudaEventRecord(h->ev_pool[a + 1], st);
+  h->ev_kid[a] = kid;
 }
 
 int check_launch(lmc_handle *h) {
@@ -370,7 +379,10 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     lmc_destroy(h);
     return rc;
   }
-  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     lmc_destroy(h);
     return LMC_ECUDA;
   }
@@ -395,6 +407,10 @@ int lmc_destroy(lmc_handle *h) {
   drop_graphs(h);
   for (void *q : h->allocs) cudaFree(q);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->s2) cudaStreamSynchronize(h->s2);
+  if (h->s2) cudaStreamDestroy(h->s2);
   if (h->s) cudaStreamDestroy(h->s);
   delete h;
   return LMC_OK;
@@ -461,55 +477,77 @@ int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi, float *
 
 namespace {
 
-// Enqueue the kernels of one RK3 step on the handle's stream (directly, or
+// Enqueue the kernels of one RK3 step on the handle's streams (directly, or
 // into a graph being captured) and advance the host-side bookkeeping.
+// Two independent pieces of each substep run on the second stream, beside
+// the main chain: the T derivatives beside Lapvdvhom and the assembly of
+// rho u_i (neither reads what the other writes), and, in the mode-parallel
+// family, the psi solve beside post1 (it reads only d(rho)/dt).  The 2014
+// variant differentiates the T that its assembly saves, and takes d(rho)
+// from a transform round trip after post1, so it runs in one chain.
 int enqueue_step(lmc_handle *h, int cfl_step) {
   lmc::Dev &d = h->d;
-  cudaStream_t s = h->s;
-  {
-    for (int rk = 0; rk < 3; rk++) {
-      if (d.prec) {  // this substep's plane sums, and the previous ones
-        d.mo_cur = h->mo[h->mo_flip];
-        d.mo_prev = h->mo[1 - h->mo_flip];
-      }
-      prof_mark(h, 0);
-      lmc::launch_lapv(d, s);
-      prof_mark(h, 1);
-      lmc::launch_assemble(d, rk, s);
-      prof_mark(h, 2);
-      lmc::launch_tder(d, s);
-      prof_mark(h, 3);
-      lmc::launch_zinv(d, s);
-      if (rk == 0) {
-        prof_mark(h, 9);
-        LMC_CK(cudaMemsetAsync(d.rhom, 0, (size_t)d.my * sizeof(double), s));
-        if (cfl_step) LMC_CK(cudaMemsetAsync(d.cflmax, 0, 4 * sizeof(unsigned long long), s));
-      }
-      const int do_cfl = cfl_step && rk == 0;
-      prof_mark(h, 4);
+  cudaStream_t s = h->s, s2 = h->s2;
+  auto run = [&](int kid, cudaStream_t st, auto &&launch) {
+    const int a = prof_begin(h, st);
+    launch();
+    prof_end(h, kid, a, st);
+  };
+  auto fork = [&]() {
+    if (cudaEventRecord(h->ev_fork, s) != cudaSuccess) return false;
+    return cudaStreamWaitEvent(s2, h->ev_fork, 0) == cudaSuccess;
+  };
+  auto join = [&]() {
+    if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return false;
+    return cudaStreamWaitEvent(s, h->ev_join, 0) == cudaSuccess;
+  };
+  const bool side_t = !d.variant;
+  const bool side_psi = d.tpm && !d.variant;
+  for (int rk = 0; rk < 3; rk++) {
+    if (d.prec) {  // this substep's plane sums, and the previous ones
+      d.mo_cur = h->mo[h->mo_flip];
+      d.mo_prev = h->mo[1 - h->mo_flip];
+    }
+    if (side_t) {
+      if (!fork()) return LMC_ECUDA;
+      run(2, s2, [&] { lmc::launch_tder(d, s2); });
+      if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
+    }
+    run(0, s, [&] { lmc::launch_lapv(d, s); });
+    run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
+    if (side_t) {
+      if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
+    } else {
+      run(2, s, [&] { lmc::launch_tder(d, s); });
+    }
+    run(3, s, [&] { lmc::launch_zinv(d, s); });
+    if (rk == 0) {
+      LMC_CK(cudaMemsetAsync(d.rhom, 0, (size_t)d.my * sizeof(double), s));
+      if (cfl_step) LMC_CK(cudaMemsetAsync(d.cflmax, 0, 4 * sizeof(unsigned long long), s));
+    }
+    const int do_cfl = cfl_step && rk == 0;
+    run(4, s, [&] {
       lmc::launch_xphys(d, rk, do_cfl, rk == 0, s);
       if (d.variant && rk == 0) lmc::launch_cfl14(d, do_cfl, s);
-      prof_mark(h, 5);
-      lmc::launch_zfwd(d, s);
-      prof_mark(h, 6);
-      lmc::launch_post1(d, rk, do_cfl, 1, s);
-      if (d.variant) {  // d(rho) from T and Delta T (tauij2, lomacte/cross.f:877)
-        prof_mark(h, 3);
-        lmc::launch_zinv(d, s, 1);
-        prof_mark(h, 4);
-        lmc::launch_xdrho(d, s);
-        prof_mark(h, 5);
-        lmc::launch_zfwd(d, s, 1);
-      }
-      prof_mark(h, 7);
-      lmc::launch_post2(d, rk, s);
-      prof_mark(h, 8);
-      lmc::launch_psi(d, rk, cfl_step, 1, s);
-      prof_mark(h, -1);
-      if (d.prec) {
-        d.mean_ok = 1;
-        h->mo_flip = 1 - h->mo_flip;
-      }
+    });
+    run(5, s, [&] { lmc::launch_zfwd(d, s); });
+    if (side_psi) {
+      if (!fork()) return LMC_ECUDA;
+      run(8, s2, [&] { lmc::launch_psi_main(d, rk, s2); });
+    }
+    run(6, s, [&] { lmc::launch_post1(d, rk, do_cfl, 1, s); });
+    if (d.variant) {  // d(rho) from T and Delta T (tauij2, lomacte/cross.f:877)
+      run(3, s, [&] { lmc::launch_zinv(d, s, 1); });
+      run(4, s, [&] { lmc::launch_xdrho(d, s); });
+      run(5, s, [&] { lmc::launch_zfwd(d, s, 1); });
+    }
+    if (side_psi && !join()) return LMC_ECUDA;
+    run(7, s, [&] { lmc::launch_post2(d, rk, s); });
+    if (side_psi) run(8, s, [&] { lmc::launch_psi_tail(d, rk, cfl_step, s); });
+    else run(8, s, [&] { lmc::launch_psi(d, rk, cfl_step, 1, s); });
+    if (d.prec) {
+      d.mean_ok = 1;
+      h->mo_flip = 1 - h->mo_flip;
     }
   }
   return LMC_OK;
@@ -698,8 +736,9 @@ int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count) {
   if (!h || nk < 0 || (nk && (!ms || !count))) return LMC_EINVAL;
   LMC_CK(cudaSetDevice(h->p.device));
   LMC_CK(cudaStreamSynchronize(h->s));
+  LMC_CK(cudaStreamSynchronize(h->s2));
   for (int k = 0; k < nk; k++) { ms[k] = 0.0; count[k] = 0; }
-  for (size_t i = 0; i + 1 < h->ev_used; i++) {
+  for (size_t i = 0; i + 1 < h->ev_used; i += 2) {
     const int k = h->ev_kid[i];
     if (k < 0 || k >= nk) continue;
     float t = 0.f;

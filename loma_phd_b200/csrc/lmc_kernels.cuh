@@ -114,6 +114,8 @@ void launch_cfl14(const Dev &d, int do_cfl, cudaStream_t s);
 void launch_post1(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
 void launch_post2(const Dev &d, int rk, cudaStream_t s);
 void launch_psi(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
+void launch_psi_main(const Dev &d, int rk, cudaStream_t s);
+void launch_psi_tail(const Dev &d, int rk, int cfl_step, cudaStream_t s);
 // reference layout [kx][kz][y] <-> device layout [y][kx][kz]
 void launch_ref2dev(const Dev &d, const double2 *in, double2 *out, cudaStream_t s);
 void launch_dev2ref(const Dev &d, const double2 *in, double2 *out, cudaStream_t s);

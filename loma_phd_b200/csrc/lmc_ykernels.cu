@@ -81,6 +81,12 @@ void launch_post2(const Dev &d, int rk, cudaStream_t s) {
   if (d.tpm) tpm_post2(d, rk, s);
   else LMC_YDISPATCH(post2(d, rk, s))
 }
+// mode-parallel family, non-variant: the psi solve and its 00 tail apart,
+// so that the solve can run beside post1 on a second stream
+void launch_psi_main(const Dev &d, int rk, cudaStream_t s) { tpm_psi(d, rk, s); }
+void launch_psi_tail(const Dev &d, int rk, int cfl_step, cudaStream_t s) {
+  LMC_YDISPATCH(psi_00(d, rk, cfl_step, s))
+}
 void launch_psi(const Dev &d, int rk, int cfl_step, int do_diag, cudaStream_t s) {
   if (d.tpm) {
     tpm_psi(d, rk, s);

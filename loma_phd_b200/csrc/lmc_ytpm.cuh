@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
   const int my = d.my;
   const size_t ld = d.nmode;
   const bool m00 = M.m == 0;
-  double2 *s1 = d.ws[0] + M.m, *s2 = d.ws[1] + M.m;
+  double2 *s1 = d.ws[2] + M.m, *s2 = d.ws[3] + M.m;  // 2, 3: runs beside lapv/assemble
   double2 *const Tsrc = V ? d.Told : d.scal;
   {
     Rd<double2, 8> r;
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
   if (!mode_of(d, M)) return;
   const int my = d.my;
   const size_t ld = d.nmode;
-  double2 *s1 = d.ws[0] + M.m;
+  double2 *s1 = d.ws[3] + M.m;  // 3: runs beside post1
   const double sc = V ? -1.0 / (d.scal_d[0] * (d.gama[rk] + d.xi[rk])) : 1.0;
   {
     Rd<CT, kq<CT>(8)> r;
