@@ -318,7 +318,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     # fraction of the timed region during which each kernel group runs; the
     # T derivatives and the psi solve run on a second stream beside the main
     # chain, so the fractions can sum above 1
-    share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES}
+    share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES if prof[k][1]}
     traffic = None
     table = NCU_TRAFFIC_256x65 if prec == 0 else NCU_TRAFFIC_MIXED_256x65
     if a.nx == 256 and a.nz == 256 and top in table:

@@ -124,7 +124,8 @@ int lmc_state_device_ptrs(lmc_handle *h, double **vor, double **phi,
  *   0 lapv (Lapvdvhom), 1 assemble (rho u_i), 2 tder (T derivatives),
  *   3 zinv (inverse z transforms), 4 xphys (x transforms + products),
  *   5 zfwd (direct z transforms), 6 post1 (N_i), 7 post2 (vorticity,
- *   RHS, RK3 update), 8 psi (solvepsi + 00 modes), 9 memsets. */
+ *   RHS, RK3 update), 8 psi (solvepsi + 00 modes), 9 memsets,
+ *   10 statistics (lmc_stats_step). */
 int lmc_profile_start(lmc_handle *h);
 int lmc_profile_read(lmc_handle *h, int nk, double *ms, int *count);
 
@@ -149,6 +150,41 @@ int lmc_use_graphs(lmc_handle *h, int on);
 int lmc_query(lmc_handle *h);
 size_t lmc_device_bytes(lmc_handle *h);
 size_t lmc_footprint(const lmc_params *p);
+
+/* Statistics and spectra on the device: what the reference accumulates
+ * while istati = 1 (addstats1 cross.f:1981-2064 and addstats2
+ * cross.f:2070-2290 at the first substep, cross.f:578-585 and 794-812; the
+ * physical sums of phys2 cross.f:1583-1607), with resetstats
+ * (escru.f:485-580) and the data writestats writes (escru.f:276-484).
+ * lmc_stats_reset: zero every accumulator, nacum and nacumsp, and set the
+ *   nsp spectra planes jsp (1-based y indices: the reference's jsptot,
+ *   main.f:698-703) and the exponent sigma of mu/mu0 = T^sigma (main.f:570
+ *   sets 0).  Allocates the statistics buffers on first use (3 spectral
+ *   FP64 fields and the accumulators).  LMC_EINVAL for the 2014 variant.
+ * lmc_stats_step: nsteps RK3 steps like lmc_step that also accumulate at
+ *   their first substep (five extra kernels); nacum and nacumsp grow by one
+ *   per step (cross.f:800-801).  Steps taken with lmc_step accumulate
+ *   nothing, as with istati = 0.
+ * lmc_stats_read: synchronises and copies out (NULL skips)
+ *   prof[33*my]  profile q of row j at prof[q*my + j], raw (writestats
+ *                multiplies the last eleven by 1/(mgalx*mgalz)), in the
+ *                order of the .sta record (escru.f:381-402): um vm wm rum
+ *                rvm rwm Tm w1m w2m w3m them up vp wp uvr uwr vwr w1p w2p
+ *                w3p Tp ep ruu ruv ruw rvv rvw rww rhom thep theup mum num
+ *   spec[nplanes*12*nsp*(nz1+1)] the spectra in the order of the .spe plane
+ *                records (escru.f:445-448): kx plane, then field (u v w
+ *                uv_re uv_im o1 o2 o3 rhou rhov rhow T), then spectra
+ *                plane, then |kz| = 0..nz1 fastest (FP64 sums; the
+ *                reference sums in real*4)
+ *   uner[9]      the nine hy-weighted energies of the last accumulating
+ *                step (cross.f:2207-2210; the .cf writes their square roots)
+ *   counts[2]    nacum, nacumsp
+ *   clear_spectra != 0 then zeroes the spectra and nacumsp, as writestats
+ *   does after writing them (escru.f:466-477). */
+int lmc_stats_reset(lmc_handle *h, int nsp, const int *jsp, double sigma);
+int lmc_stats_step(lmc_handle *h, int nsteps);
+int lmc_stats_read(lmc_handle *h, double *prof, double *spec, double *uner,
+                   int *counts, int clear_spectra);
 
 /* Seeded initial condition (host only, no GPU): the structure of the
  * reference generator trunk/initloma3/src/main.f:95-609 with a

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "liblomacte_b200.so")
 SOURCES = ["lmc_y_d.cu", "lmc_y_c.cu", "lmc_y_b.cu", "lmc_y_a.cu", "lmc_ytpm.cu", "lmc_fft_c.cu", "lmc_fft_b.cu",
            "lmc_fft_a.cu", "lmc_api.cu", "lmc_dispatch.cu", "lmc_ykernels.cu", "lmc_noalloc.cu", "lmc_host.cpp"]
 HEADERS = ["lmc_internal.h", "lmc_kernels.cuh", "lmc_device.cuh", "lmc_fft_impl.cuh", "lmc_async.cuh",
-           "lmc_ykernels.cuh", "lmc_ylaunch.h", "lmc_ytpm.cuh"]
+           "lmc_ykernels.cuh", "lmc_ylaunch.h", "lmc_ytpm.cuh", "lmc_stats.cuh"]
 
 
 def nvcc() -> str:

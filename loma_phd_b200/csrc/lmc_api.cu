@@ -36,6 +36,13 @@ struct lmc_handle {
   bool graphs = true;
   cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   size_t bytes = 0;  // device bytes held
+  // statistics (lmc_stats_*): device accumulators, the capacity of the
+  // spectra buffers in planes, and the reference's counters
+  lmc::Stats st{};
+  bool st_on = false;
+  int st_cap = -1;
+  size_t st_spec_bytes = 0;
+  int nacum = 0, nacumsp = 0;
   // per-kernel CUDA-event profiling (lmc_profile_start / lmc_profile_read)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -305,12 +312,18 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     lmc_destroy(h);
     return rc;
   }
+  // row form of d/dy in every family (the statistics differentiate u, v, w
+  // one thread per mode); the rest only for the mode-parallel kernels
+  if ((rc = dupload(h, &d.r_dt12, o.dt12)) || (rc = dupload(h, &d.r_p1L, o.p1L)) ||
+      (rc = dupload(h, &d.r_p1U, o.p1U)) || (rc = dupload(h, &d.r_fmap, o.fmap))) {
+    lmc_destroy(h);
+    return rc;
+  }
   if (d.tpm &&
-      ((rc = dupload(h, &d.r_dt12, o.dt12)) || (rc = dupload(h, &d.r_dt11, o.dt11)) ||
+      ((rc = dupload(h, &d.r_dt11, o.dt11)) ||
        (rc = dupload(h, &d.r_dt22, o.dt22)) || (rc = dupload(h, &d.r_dt21, o.dt21)) ||
-       (rc = dupload(h, &d.r_p1L, o.p1L)) || (rc = dupload(h, &d.r_p1U, o.p1U)) ||
        (rc = dupload(h, &d.r_p3L, o.p3L)) || (rc = dupload(h, &d.r_p3U, o.p3U)) ||
-       (rc = dupload(h, &d.r_fmap, o.fmap)) || (rc = dupload(h, &d.r_ebot, o.ebot)) ||
+       (rc = dupload(h, &d.r_ebot, o.ebot)) ||
        (rc = dupload(h, &d.r_etop, o.etop)) || (rc = dupload(h, &d.PLt, PLt)) || (rc = dupload(h, &d.PUt, PUt)) ||
        (rc = dupload(h, &d.V12t, V12t)))) {
     lmc_destroy(h);
@@ -485,7 +498,7 @@ namespace {
 // family, the psi solve beside post1 (it reads only d(rho)/dt).  The 2014
 // variant differentiates the T that its assembly saves, and takes d(rho)
 // from a transform round trip after post1, so it runs in one chain.
-int enqueue_step(lmc_handle *h, int cfl_step) {
+int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
   lmc::Dev &d = h->d;
   cudaStream_t s = h->s, s2 = h->s2;
   auto run = [&](int kid, cudaStream_t st, auto &&launch) {
@@ -520,7 +533,12 @@ int enqueue_step(lmc_handle *h, int cfl_step) {
     } else {
       run(2, s, [&] { lmc::launch_tder(d, s); });
     }
+    // statistics of an accumulating step, first substep (cross.f:578-585,
+    // 794-812, 1583-1607); id 10 in the profile
+    const bool st_now = stats && rk == 0;
+    if (st_now) run(10, s, [&] { lmc::launch_stats1(d, h->st, s); });
     run(3, s, [&] { lmc::launch_zinv(d, s); });
+    if (st_now) run(10, s, [&] { lmc::launch_xstats(d, h->st, s); });
     if (rk == 0) {
       LMC_CK(cudaMemsetAsync(d.rhom, 0, (size_t)d.my * sizeof(double), s));
       if (cfl_step) LMC_CK(cudaMemsetAsync(d.cflmax, 0, 4 * sizeof(unsigned long long), s));
@@ -531,6 +549,7 @@ int enqueue_step(lmc_handle *h, int cfl_step) {
       if (d.variant && rk == 0) lmc::launch_cfl14(d, do_cfl, s);
     });
     run(5, s, [&] { lmc::launch_zfwd(d, s); });
+    if (st_now) run(10, s, [&] { lmc::launch_stats2(d, h->st, s); });
     if (side_psi) {
       if (!fork()) return LMC_ECUDA;
       run(8, s2, [&] { lmc::launch_psi_main(d, rk, s2); });
@@ -628,6 +647,100 @@ int lmc_step(lmc_handle *h, int nsteps) {
   return LMC_OK;
 }
 
+int lmc_stats_reset(lmc_handle *h, int nsp, const int *jsp, double sigma) {
+  if (!h || nsp < 0 || (nsp > 0 && !jsp) || h->d.variant) return LMC_EINVAL;
+  if (h->err) return h->err;
+  const int my = h->d.my;
+  for (int i = 0; i < nsp; i++)
+    if (jsp[i] < 1 || jsp[i] > my) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  LMC_CK(cudaStreamSynchronize(h->s));  // no accumulating step may still read the old set-up
+  lmc::Stats &st = h->st;
+  lmc::Dev &d = h->d;
+  int rc;
+  if (!st.prof) {
+    const size_t ns = (size_t)d.nmode * my;
+    if ((rc = dalloc(h, &st.prof, (size_t)lmc::NSTAT * my)) || (rc = dalloc(h, &st.erow, (size_t)9 * my)) ||
+        (rc = dalloc(h, &st.uner, (size_t)9)))
+      return rc;
+    for (int q = 0; q < 3; q++)
+      if ((rc = dalloc(h, &st.dy[q], ns))) return rc;
+  }
+  const size_t nspec = (size_t)d.nkx * 12 * nsp * (d.nz1 + 1);
+  if (nsp > h->st_cap) {  // (re)size the spectra and plane buffers
+    for (void *q : {(void *)st.spec, (void *)st.jsp}) {
+      if (!q) continue;
+      for (size_t i = 0; i < h->allocs.size(); i++)
+        if (h->allocs[i] == q) {
+          h->allocs.erase(h->allocs.begin() + i);
+          break;
+        }
+      cudaFree(q);
+    }
+    h->bytes -= h->st_spec_bytes;
+    st.spec = nullptr;
+    st.jsp = nullptr;
+    h->st_cap = -1;
+    int *pj = nullptr;
+    const size_t b0 = h->bytes;
+    if ((rc = dalloc(h, &st.spec, nspec)) || (rc = dalloc(h, &pj, (size_t)(nsp > 0 ? nsp : 1)))) return rc;
+    st.jsp = pj;
+    h->st_spec_bytes = h->bytes - b0;
+    h->st_cap = nsp;
+  }
+  std::vector<int> rows(nsp > 0 ? nsp : 1, 0);
+  for (int i = 0; i < nsp; i++) rows[i] = jsp[i] - 1;
+  LMC_CK(cudaMemcpy((void *)st.jsp, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+  LMC_CK(cudaMemsetAsync(st.prof, 0, (size_t)lmc::NSTAT * my * sizeof(double), h->s));
+  LMC_CK(cudaMemsetAsync(st.spec, 0, (nspec ? nspec : 1) * sizeof(double), h->s));
+  LMC_CK(cudaMemsetAsync(st.erow, 0, (size_t)9 * my * sizeof(double), h->s));
+  LMC_CK(cudaMemsetAsync(st.uner, 0, 9 * sizeof(double), h->s));
+  st.nsp = nsp;
+  st.sigma = sigma;
+  h->nacum = h->nacumsp = 0;
+  h->st_on = true;
+  return LMC_OK;
+}
+
+int lmc_stats_step(lmc_handle *h, int nsteps) {
+  if (!h || nsteps < 0 || !h->st_on) return LMC_EINVAL;
+  if (h->err) return h->err;
+  LMC_CK(cudaSetDevice(h->p.device));
+  const int ncfl = h->p.ncfl > 0 ? h->p.ncfl : 1;
+  for (int n = 0; n < nsteps; n++) {
+    const int cfl_step = (h->p.dt_mode == 0) && (h->steps % ncfl == 0);  // cross.f:240
+    const int rc = enqueue_step(h, cfl_step, true);
+    if (rc) return rc;
+    h->steps++;
+    h->nacum++;  // cross.f:800-801
+    h->nacumsp++;
+    if (check_launch(h)) return LMC_ECUDA;
+  }
+  return LMC_OK;
+}
+
+int lmc_stats_read(lmc_handle *h, double *prof, double *spec, double *uner, int *counts, int clear_spectra) {
+  if (!h || !h->st_on) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  const lmc::Stats &st = h->st;
+  const size_t nspec = (size_t)h->d.nkx * 12 * st.nsp * (h->d.nz1 + 1);
+  if (prof)
+    LMC_CK(cudaMemcpyAsync(prof, st.prof, (size_t)lmc::NSTAT * h->d.my * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->s));
+  if (spec && nspec) LMC_CK(cudaMemcpyAsync(spec, st.spec, nspec * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  if (uner) LMC_CK(cudaMemcpyAsync(uner, st.uner, 9 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  if (counts) {
+    counts[0] = h->nacum;
+    counts[1] = h->nacumsp;
+  }
+  if (clear_spectra) {  // escru.f:466-477
+    if (nspec) LMC_CK(cudaMemsetAsync(st.spec, 0, nspec * sizeof(double), h->s));
+    h->nacumsp = 0;
+  }
+  return h->err;
+}
+
 int lmc_use_graphs(lmc_handle *h, int on) {
   if (!h) return LMC_EINVAL;
   if (!on) drop_graphs(h);
@@ -676,7 +789,7 @@ size_t lmc_footprint(const lmc_params *p) {
   if (p->variant || mode_parallel(g.nmode))
     b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 4 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
   else
-    b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8;  // per-mode Poisson tables
+    b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8 + (size_t)g.my * 15 * 8;  // Poisson, d/dy rows
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
   else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;
   b += (size_t)C * 32 * 64 * 8 + 6 * 5 * 32 * 16 * 8 + (size_t)(g.mgalx + g.mgalz) * 24;  // y tables, twiddles

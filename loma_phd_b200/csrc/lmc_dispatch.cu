@@ -13,6 +13,7 @@ namespace lmc {
   bool fft_zfwd_##SUF(const Dev &d, int mode, cudaStream_t s);                         \
   bool fft_xdrho_##SUF(const Dev &d, cudaStream_t s);                                  \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
+  bool fft_xstats_##SUF(const Dev &d, const Stats &st, cudaStream_t s);                \
   size_t fft_zsm_##SUF(int n);                                                         \
   size_t fft_xsm_##SUF(int n);                                                         \
   cudaError_t fft_init_##SUF(int limit);
@@ -35,6 +36,9 @@ void launch_xdrho(const Dev &d, cudaStream_t s) {
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
   if (!fft_xphys_a(d, rk, do_cfl, do_diag, s) && !fft_xphys_b(d, rk, do_cfl, do_diag, s))
     fft_xphys_c(d, rk, do_cfl, do_diag, s);
+}
+void launch_xstats(const Dev &d, const Stats &st, cudaStream_t s) {
+  if (!fft_xstats_a(d, st, s) && !fft_xstats_b(d, st, s)) fft_xstats_c(d, st, s);
 }
 size_t xphys_smem(const Dev &d) {
   size_t v = fft_xsm_a(d.mgalx);

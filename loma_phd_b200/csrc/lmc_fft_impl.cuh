@@ -514,6 +514,93 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xdrho(Dev d) {
   x_extract<N1, N2, double2, double2>(d, W, 0, 0, -1, y, z0, nzb);
 }
 
+// Statistics of the physical fields on an accumulating substep (phys2,
+// cross.f:1583-1607): per y row the plane sums of u rho u, u rho v,
+// u rho w, v rho v, v rho w, w rho w (u_i = rho u_i T), 1/T, T^sigma and
+// T^(sigma+1).  One block per row inverts rho u, rho v, rho w and T (three
+// complex x transforms per z line, the same packing as k_xphys) before
+// k_xphys overwrites its inputs, and adds its sums in a fixed order.
+template <int N1, int N2, typename CT, typename ST>
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xstats(Dev d, Stats st) {
+  using F = Four<N1, N2, CT>;
+  using G = Geo<N1, N2>;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, NW = G::XT / 32;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  CT *W = (CT *)smraw;  // 3 groups x ZB lines x LD
+  __shared__ double sh[NW * 9];
+  const int y = blockIdx.x, nkx = d.nkx, my = d.my;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m5 = 0.0;  // mixed form: FP64 00 profiles
+  if constexpr (sizeof(ST) == sizeof(float2)) {
+    m0 = d.mi[y];
+    m1 = d.mi[(size_t)my + y];
+    m2 = d.mi[(size_t)2 * my + y];
+    m5 = d.mi[(size_t)5 * my + y];
+  }
+  const double sg = st.sigma, sg1 = st.sigma + 1.0;
+  double a[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) a[q] = 0.0;
+  const int gap = N - 2 * nkx + 1;
+  for (int z0 = 0; z0 < d.mgalz; z0 += ZB) {
+    const int nzb = min(ZB, d.mgalz - z0);
+    for (int idx = threadIdx.x; idx < 3 * ZB * gap; idx += blockDim.x) {
+      const int ln = idx / gap, g = idx - ln * gap;
+      W[ln * LD + F::sk(nkx + g)] = cz<CT>();
+    }
+    for (int gp = 0; gp < 3; gp++) {
+      const int p = gp < 2 ? gp : 3;  // line pairs (rho u, rho v), (rho w, -), (-, T)
+      for (int l = 0; l < ZB; l++) {
+        CT *line = W + (gp * ZB + l) * LD;
+        const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * nkx;
+        const ST *A = wzb<ST>(d, 2 * p) + g0, *B = wzb<ST>(d, 2 * p + 1) + g0;
+        for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
+          CT ca = cz<CT>(), cb = cz<CT>();
+          if (l < nzb) { ca = ccvt<CT>(A[k]); cb = ccvt<CT>(B[k]); }
+          if (k == 0) {
+            line[F::sk(0)] = cmk<CT>(ca.x, cb.x);
+          } else {
+            line[F::sk(k)] = cmk<CT>(ca.x - cb.y, ca.y + cb.x);
+            line[F::sk(N - k)] = cmk<CT>(ca.x + cb.y, cb.x - ca.y);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    F::template nat2perm<+1>(W, 3 * ZB, LD, wtwx<CT>(d));
+    for (int q = threadIdx.x; q < nzb * N; q += blockDim.x) {
+      const int l = q / N, pos = q - l * N;
+      const CT *c0 = W + (size_t)l * LD + F::sk(pos);
+      const double2 p0 = to_d2(c0[0]), p1 = to_d2(c0[(size_t)ZB * LD]), p3 = to_d2(c0[(size_t)2 * ZB * LD]);
+      const double ru = p0.x + m0, rv = p0.y + m1, rw = p1.x + m2, T = p3.y + m5;
+      const double u = ru * T, v = rv * T, w = rw * T;
+      a[0] += u * ru;
+      a[1] += u * rv;
+      a[2] += u * rw;
+      a[3] += v * rv;
+      a[4] += v * rw;
+      a[5] += w * rw;
+      a[6] += 1.0 / T;
+      a[7] += pow(T, sg);
+      a[8] += pow(T, sg1);
+    }
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    const double v = warp_sum(a[q]);
+    if (lane == 0) sh[wid * 9 + q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    const int q = threadIdx.x;
+    double s = 0.0;
+    for (int w = 0; w < NW; w++) s += sh[w * 9 + q];
+    const int dst = q < 7 ? ST_RUU + q : ST_MUM + (q - 7);  // ruu..rww, rhom, mum, num
+    st.prof[(size_t)dst * my + y] += s;
+  }
+}
+
 // Plane sums of the mixed form's outputs from the partial sums of k_xphys,
 // added in a fixed order so that a run is reproducible bit for bit.
 template <int N1, int N2>
@@ -581,6 +668,10 @@ struct Launch {
       k_msum<N1, N2><<<dim3(d.my, 11), 128, 0, s>>>(d, nslot);
     }
   }
+  static size_t xstats_sm() { return (size_t)3 * G::ZB * G::LD * sizeof(CT); }
+  static void xstats(const Dev &d, const Stats &st, cudaStream_t s) {
+    k_xstats<N1, N2, CT, ST><<<d.my, G::XT, xstats_sm(), s>>>(d, st);
+  }
   static cudaError_t optin1(const void *fn, int limit) {
     cudaError_t e;
     cudaFuncAttributes fa;
@@ -591,6 +682,7 @@ struct Launch {
     cudaError_t e;
     if ((e = optin1((const void *)k_zinv<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_zfwd<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
+    if ((e = optin1((const void *)k_xstats<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     return optin1((const void *)k_xphys<N1, N2, CT, ST>, limit);
   }
 };
@@ -627,6 +719,8 @@ inline cudaError_t upload_twiddles() {
   case N: Launch<N1, N2, double2, double2>::xdrho(d, s); return true;
 #define LMC_FFT_CASE_X(N, N1, N2) \
   case N: LMC_FFT_FORMS(N1, N2, xphys(d, rk, do_cfl, do_diag, s)) return true;
+#define LMC_FFT_CASE_XST(N, N1, N2) \
+  case N: LMC_FFT_FORMS(N1, N2, xstats(d, st, s)) return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
@@ -654,6 +748,9 @@ inline cudaError_t upload_twiddles() {
   }                                                                                               \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {           \
     switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_X) default: return false; }                      \
+  }                                                                                               \
+  bool fft_xstats_##SUF(const Dev &d, const Stats &st, cudaStream_t s) {                          \
+    switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_XST) default: return false; }                    \
   }                                                                                               \
   size_t fft_zsm_##SUF(int n) {                                                                   \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_ZS) default: return 0; }                             \

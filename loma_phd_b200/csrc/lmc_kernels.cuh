@@ -74,6 +74,31 @@ struct Dev {
   int *status;
 };
 
+// Statistics accumulators of one case (lmc_stats_reset allocates them):
+// what addstats1 / addstats2 (cross.f:1981-2290) and the physical sums of
+// phys2 (cross.f:1583-1607) accumulate while istati = 1.
+//   prof [NSTAT][my]  raw profiles in the order of the .sta record
+//                     (escru.f:381-402), without its 1/(mgalx*mgalz)
+//   spec [nkx][12][nsp][nz1+1] spectra (the .spe plane records,
+//                     escru.f:445-448), FP64 here, real*4 in the reference
+//   erow [9][my]      this step's per-row sums of the nine energies
+//   uner [9]          sum_j hy_j erow_j (cross.f:2207-2210)
+//   dy   [3]          du/dy, dv/dy, dw/dy of the step ([y][kx][kz])
+//   jsp  [nsp]        0-based rows of the spectra planes
+struct Stats {
+  double *prof, *spec, *erow, *uner;
+  double2 *dy[3];
+  const int *jsp;
+  int nsp;
+  double sigma;  // mu/mu0 = T^sigma (main.f:570)
+};
+constexpr int NSTAT = 33;
+enum {
+  ST_UM = 0, ST_VM, ST_WM, ST_RUM, ST_RVM, ST_RWM, ST_TM, ST_W1M, ST_W2M, ST_W3M, ST_THEM,
+  ST_UP, ST_VP, ST_WP, ST_UVR, ST_UWR, ST_VWR, ST_W1P, ST_W2P, ST_W3P, ST_TP, ST_EP,
+  ST_RUU, ST_RUV, ST_RUW, ST_RVV, ST_RVW, ST_RWW, ST_RHOM, ST_THEP, ST_THEUP, ST_MUM, ST_NUM
+};
+
 // Spectral work-buffer roles before / after the transforms.
 // SB_T32 holds an FP32 copy of T for the z transforms of the mixed form.
 enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32 };
@@ -121,6 +146,12 @@ void launch_ref2dev(const Dev &d, const double2 *in, double2 *out, cudaStream_t 
 void launch_dev2ref(const Dev &d, const double2 *in, double2 *out, cudaStream_t s);
 // operator-level entry point (tests), device layout
 void launch_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s);
+// statistics of an accumulating substep: addstats1 after the assembly of
+// rho u_i (before the transforms), the physical sums between the inverse z
+// transforms and k_xphys, addstats2 after the direct z transforms
+void launch_stats1(const Dev &d, const Stats &st, cudaStream_t s);
+void launch_xstats(const Dev &d, const Stats &st, cudaStream_t s);
+void launch_stats2(const Dev &d, const Stats &st, cudaStream_t s);
 size_t xphys_smem(const Dev &d);
 size_t z_smem(const Dev &d);
 cudaError_t kernels_init(const Dev &d);

@@ -1,6 +1,7 @@
 // lmc_ytpm.cu -- launchers of the mode-parallel y kernels (lmc_ytpm.cuh)
 // for both work-buffer types and, in FP64, the 2014 variant.
 #include "lmc_ylaunch.h"
+#include "lmc_stats.cuh"
 #include "lmc_ytpm.cuh"
 
 namespace lmc {
@@ -34,5 +35,21 @@ void tpm_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *ou
 }
 void tpm_cfl14(const Dev &d, int do_cfl, cudaStream_t s) { tpm::k_cfl14<<<1, 32, 0, s>>>(d, do_cfl); }
 void tpm_psi00_14(const Dev &d, int rk, cudaStream_t s) { tpm::k_psi00_14<<<1, 32, 0, s>>>(d, rk); }
+
+// statistics (lmc_stats.cuh); every grid, either y family
+void launch_stats1(const Dev &d, const Stats &st, cudaStream_t s) {
+  if (d.prec) stats::k_srow1<float2><<<d.my, stats::SRT, 0, s>>>(d, st);
+  else stats::k_srow1<double2><<<d.my, stats::SRT, 0, s>>>(d, st);
+}
+void launch_stats2(const Dev &d, const Stats &st, cudaStream_t s) {
+  if (d.prec) {
+    stats::t_sdy<float2><<<tgrid(d), tpm::TB, 0, s>>>(d, st);
+    stats::k_srow2<float2><<<d.my, stats::SRT, 0, s>>>(d, st);
+  } else {
+    stats::t_sdy<double2><<<tgrid(d), tpm::TB, 0, s>>>(d, st);
+    stats::k_srow2<double2><<<d.my, stats::SRT, 0, s>>>(d, st);
+  }
+  stats::k_suner<<<1, 32, 0, s>>>(d, st);
+}
 
 }  // namespace lmc

@@ -15,6 +15,19 @@
 * hre.dat (main.f:502-545): lines that start with "CC" are comments; then
   Re alp bet a0 / nstep nimag nhist / CFL ncfl / id22 nstart ntimes /
   output, input and statistics file names.
+* Statistics (.sta) and spectra (.spe) files of writestats (escru.f:276-484),
+  Fortran unformatted sequential like the images:
+    .sta record 1: my (i4), time, Re, alp, bet, a0 (real*4), nacum (i4)
+         record 2: (y_j, fmap_j) real*8 pairs, j = 1..my
+         record 3: 33 real*8 per row j = 1..my: um vm wm rum rvm rwm Tm w1m
+                   w2m w3m them up vp wp uvr uwr vwr w1p w2p w3p Tp ep and
+                   fac * (ruu ruv ruw rvv rvw rww rhom thep theup mum num),
+                   fac = 1/(mgalx*mgalz) in real*4
+    .spe record 1: time, Re, alp, bet (real*4), mx, my, mz, nspec+1,
+                   nacumsp (i4)
+         record 2: the nspec+1 planes jsptot (i4), then (y_j, fmap_j) real*8
+         then one record per kx plane: 12*(nz1+1)*(nspec+1) real*4, |kz|
+                   fastest, then spectra plane, then field
 * The .cf history line (cross.f:1172-1176): 21 values in format 21(d22.14):
   time, dm, dw, Re*dw, trapz, masst, enerdis, energy(1..9), massu, massv,
   massw, wall time, communication time.
@@ -236,3 +249,82 @@ def cf_line(diag: Dict[str, float], energies: Optional[Iterable[float]] = None, 
     vals = [diag["time"], diag["dm"], diag["dw"], diag["Redw"], diag["trapz"], diag["masst"], enerdis] + en + \
         [diag["massu"], diag["massv"], diag["massw"], wall, comm]
     return "".join(fortran_d(v) for v in vals)
+
+
+# --------------------------------------------------------------------------
+# statistics and spectra files (writestats, escru.f:276-484)
+# --------------------------------------------------------------------------
+def write_sta(path: str, data, y: np.ndarray, fmap: np.ndarray, *, time: float, Re: float, alp: float,
+              bet: float, mgalx: int, mgalz: int, a0: float = 0.0) -> None:
+    """Write a .sta file from a StatsData read-back (escru.f:381-402)."""
+    from .stats import FAC_FROM, NSTAT, fac32
+    prof = np.asarray(data.prof, dtype=np.float64)
+    if prof.ndim != 2 or prof.shape[0] != NSTAT:
+        raise ValueError("prof must be [33, my]")
+    my = prof.shape[1]
+    if np.shape(y) != (my,) or np.shape(fmap) != (my,):
+        raise ValueError("y and fmap must have my entries")
+    rows = np.array(prof.T, dtype="<f8")  # [my][33]
+    rows[:, FAC_FROM:] *= fac32(mgalx, mgalz)
+    yf = np.empty((my, 2), dtype="<f8")
+    yf[:, 0] = y
+    yf[:, 1] = fmap
+    with open(path, "wb") as f:
+        _write_record(f, struct.pack("<i5fi", my, time, Re, alp, bet, a0, int(data.nacum)))
+        _write_record(f, yf.tobytes())
+        _write_record(f, rows.tobytes())
+
+
+def read_sta(path: str) -> Dict[str, object]:
+    """Read a .sta file: header values, y, fmap and the [33, my] profiles as
+    written (the last eleven times fac)."""
+    with open(path, "rb") as f:
+        r1, r2, r3 = _read_record(f), _read_record(f), _read_record(f)
+    if r1 is None or r2 is None or r3 is None or len(r1) != 28:
+        raise ValueError("not a .sta file")
+    my, time, Re, alp, bet, a0, nacum = struct.unpack("<i5fi", r1)
+    yf = np.frombuffer(r2, dtype="<f8").reshape(my, 2)
+    rows = np.frombuffer(r3, dtype="<f8").reshape(my, -1)
+    return dict(my=my, time=time, Re=Re, alp=alp, bet=bet, a0=a0, nacum=nacum, y=yf[:, 0].copy(),
+                fmap=yf[:, 1].copy(), prof=rows.T.copy())
+
+
+def write_spe(path: str, data, y: np.ndarray, fmap: np.ndarray, *, time: float, Re: float, alp: float,
+              bet: float, mx: int, mz: int) -> None:
+    """Write a .spe file from a StatsData read-back (escru.f:435-448); the
+    spectra are stored in real*4 as the reference accumulates them."""
+    spec = np.asarray(data.spec, dtype=np.float64)
+    nkx, nf, nsp, nk = spec.shape
+    my = len(y)
+    if nf != 12 or nsp != len(data.planes) or nkx != mx // 2 or nk != (mz - 1) // 2 + 1:
+        raise ValueError("spectra shape does not match the grid")
+    yf = np.empty((my, 2), dtype="<f8")
+    yf[:, 0] = y
+    yf[:, 1] = fmap
+    with open(path, "wb") as f:
+        _write_record(f, struct.pack("<4f5i", time, Re, alp, bet, mx, my, mz, nsp, int(data.nacumsp)))
+        _write_record(f, np.asarray(data.planes, dtype="<i4").tobytes() + yf.tobytes())
+        for i in range(nkx):
+            _write_record(f, np.ascontiguousarray(spec[i], dtype="<f4").tobytes())
+
+
+def read_spe(path: str) -> Dict[str, object]:
+    """Read a .spe file: header values, planes, y, fmap and the spectra
+    [mx/2, 12, nspec+1, nz1+1] (real*4)."""
+    with open(path, "rb") as f:
+        r1 = _read_record(f)
+        if r1 is None or len(r1) != 36:
+            raise ValueError("not a .spe file")
+        time, Re, alp, bet, mx, my, mz, nsp, nacumsp = struct.unpack("<4f5i", r1)
+        r2 = _read_record(f)
+        planes = np.frombuffer(r2[:4 * nsp], dtype="<i4").copy()
+        yf = np.frombuffer(r2[4 * nsp:], dtype="<f8").reshape(my, 2)
+        nk = (mz - 1) // 2 + 1
+        spec = np.empty((mx // 2, 12, nsp, nk), dtype=np.float32)
+        for i in range(mx // 2):
+            r = _read_record(f)
+            if r is None:
+                raise ValueError("truncated .spe file")
+            spec[i] = np.frombuffer(r, dtype="<f4").reshape(12, nsp, nk)
+    return dict(time=time, Re=Re, alp=alp, bet=bet, mx=mx, my=my, mz=mz, nacumsp=nacumsp, planes=planes,
+                y=yf[:, 0].copy(), fmap=yf[:, 1].copy(), spec=spec)

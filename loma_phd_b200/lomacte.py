@@ -32,9 +32,10 @@ SYMBOLS = (
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
     "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
+    "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read",
 )
 
-KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset")
+KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset", "stats")
 
 
 class LomacteError(RuntimeError):
@@ -108,6 +109,9 @@ def _lib():
         L.lmc_query.argtypes = [vp]
         L.lmc_device_bytes.argtypes = [vp]
         L.lmc_device_bytes.restype = ctypes.c_size_t
+        L.lmc_stats_reset.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_double]
+        L.lmc_stats_step.argtypes = [vp, ctypes.c_int]
+        L.lmc_stats_read.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.lmc_footprint.argtypes = [ctypes.POINTER(lmc_params)]
         L.lmc_footprint.restype = ctypes.c_size_t
         _LIB = L
@@ -306,6 +310,38 @@ class Lomacte:
 
     def sync(self):
         _check(_lib().lmc_sync(self._h), "lmc_sync")
+
+    # statistics: addstats1/2 and the phys2 sums on the device
+    # (cross.f:578-585, 794-812, 1583-1607), resetstats (escru.f:485-580)
+    def stats_reset(self, planes=None, sigma: float = 0.0):
+        """Zero the accumulators; planes are 1-based y rows of the spectra
+        (default: the centre row (my+1)/2, the reference's jsptot(nspec+1))."""
+        planes = [(self.p.my + 1) // 2] if planes is None else [int(j) for j in planes]
+        arr = (ctypes.c_int * max(1, len(planes)))(*planes)
+        _check(_lib().lmc_stats_reset(self._h, len(planes), arr, float(sigma)), "lmc_stats_reset")
+        self._stats_planes = planes
+        self._stats_sigma = float(sigma)
+
+    def stats_step(self, n: int = 1):
+        """n RK3 steps that accumulate statistics (istati = 1)."""
+        _check(_lib().lmc_stats_step(self._h, int(n)), "lmc_stats_step")
+
+    def stats_read(self, clear_spectra: bool = False):
+        """Read the accumulators back as a StatsData; clear_spectra zeroes the
+        spectra and nacumsp afterwards, as writestats does."""
+        from .stats import NSTAT, StatsData
+        planes = getattr(self, "_stats_planes", None)
+        if planes is None:
+            raise LomacteError(LMC_EINVAL, "stats_read before stats_reset")
+        nkx, mz, my = self.shape
+        prof = np.zeros((NSTAT, my))
+        spec = np.zeros((nkx, 12, len(planes), (mz - 1) // 2 + 1))
+        uner = np.zeros(9)
+        cnt = (ctypes.c_int * 2)()
+        _check(_lib().lmc_stats_read(self._h, _ptr(prof), _ptr(spec), _ptr(uner), cnt, int(bool(clear_spectra))),
+               "lmc_stats_read")
+        return StatsData(prof=prof, spec=spec, uner=uner, nacum=int(cnt[0]), nacumsp=int(cnt[1]),
+                         planes=list(planes), sigma=self._stats_sigma)
 
     def diag(self) -> dict:
         d = lmc_diag()

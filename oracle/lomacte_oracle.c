@@ -446,6 +446,14 @@ struct lmo {
   cplx *w_mx, *w_my, *w_mz, *w_nx, *w_ny, *w_nz, *w_t12, *w_t13, *w_t23, *w_drho, *w_chwk, *w_chwk2;
   /* line buffers [line][kx] complex, line = z + mgalz*y */
   cplx *ln[11];
+  /* statistics (cross.f:578-585, 794-812, 1583-1607; escru.f:276-580):
+   * st[LMO_NSTAT][my] raw accumulators in the order of the .sta record,
+   * sp[nkx][12][nsp][nz1+1] spectra, uner[9] energies of the last
+   * accumulating step, jsp the 0-based rows of the spectra planes */
+  int istati, nsp, nacum, nacumsp;
+  int *jsp;
+  double sigma;
+  double *st, *sp, uner[9];
 };
 
 #define SIDX(o, i, k, j) (((size_t)(i) * (o)->mz + (k)) * (o)->my + (j))
@@ -531,6 +539,7 @@ void lmo_destroy(lmo *o) {
                o->rts};
   for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
   for (int f = 0; f < 11; f++) free(o->ln[f]);
+  free(o->jsp); free(o->st); free(o->sp);
   plan_free(&o->px); plan_free(&o->pz);
   free(o);
 }
@@ -822,6 +831,10 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
                   double *cflout /*4*/, double *rhom /*my*/) {
   int mgalx = o->mgalx, mgalz = o->mgalz, my = o->my, nkx = o->nkx;
   size_t nlines = (size_t)mgalz * my;
+  /* statistics of the physical fields (cross.f:1583-1607), per line, added
+   * into the profiles in line order after the parallel loop */
+  const int do_st = o->istati && rk == 0 && o->st;
+  double *lst = do_st ? xcalloc(nlines * 9, 8) : NULL;
   double cflx = 0, cfly = 0, cflz = 0, cflT = 0;
   double hxalp = o->alp * (mgalx - 1) / M_PI, hzbet = o->bet * (mgalz - 1) / M_PI;
   double ab = o->alpha[rk] / o->beta[rk];
@@ -864,6 +877,26 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         }
         if (do_mass) rsum += 1.0 / T[x];
       }
+      if (do_st) { /* cross.f:1587-1607 */
+        double *a = lst + (size_t)L * 9;
+        for (int x = 0; x < mgalx; x++) {
+          double uu = ru[x] * T[x];
+          a[0] += uu * ru[x]; a[1] += uu * rv[x]; a[2] += uu * rw[x];
+        }
+        for (int x = 0; x < mgalx; x++) {
+          double vv = rv[x] * T[x];
+          a[3] += vv * rv[x]; a[4] += vv * rw[x];
+        }
+        for (int x = 0; x < mgalx; x++) {
+          double ww = rw[x] * T[x];
+          a[5] += ww * rw[x];
+        }
+        for (int x = 0; x < mgalx; x++) {
+          a[6] += 1.0 / T[x];
+          a[7] += pow(T[x], o->sigma);
+          a[8] += pow(T[x], o->sigma + 1.0);
+        }
+      }
       if (do_cfl) { /* cross.f:1690-1708 */
         double DD = 1.0 / o->peclet * Tmax;
         double c0 = lmy / o->hy[jj];
@@ -886,6 +919,15 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
     free(ph); free(out); free(buf); free(fo); free(spec);
   }
   cflout[0] = cflx; cflout[1] = cfly; cflout[2] = cflz; cflout[3] = cflT;
+  if (do_st) {
+    static const int dst[9] = {LMO_S_RUU, LMO_S_RUV, LMO_S_RUW, LMO_S_RVV, LMO_S_RVW,
+                               LMO_S_RWW, LMO_S_RHOM, LMO_S_MUM, LMO_S_NUM};
+    for (size_t L = 0; L < nlines; L++) {
+      int jj = (int)(L / mgalz);
+      for (int q = 0; q < 9; q++) o->st[(size_t)dst[q] * my + jj] += lst[L * 9 + q];
+    }
+    free(lst);
+  }
 }
 
 /* foup2: cross.f:1282-1430 */
@@ -938,6 +980,117 @@ static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
     double reig = cflx + cfl[1] + cflz + cfl[3];
     o->dtr = (double)(float)(o->cfl / reig); /* dtr is real*4 */
   }
+}
+
+/* ------------------------------------------------------------------ */
+/* Statistics: addstats1 (cross.f:1981-2064), addstats2                */
+/* (cross.f:2070-2290).  Weights: kx plane 0 once, the others twice    */
+/* (the conjugate half of the x spectrum).                             */
+/* ------------------------------------------------------------------ */
+static inline double cabs2(cplx c) { return creal(c) * creal(c) + cimag(c) * cimag(c); }
+static inline size_t spidx(const lmo *o, int i, int var, int iy, int k) {
+  return (((size_t)i * 12 + var) * o->nsp + iy) * (o->nz1 + 1) + k;
+}
+/* |kz| index of kz index kk (icx, main.f:769-782) */
+static inline int icx(const lmo *o, int kk) { return kk <= o->nz1 ? kk : o->mz - kk; }
+
+static void addstats1(lmo *o, const cplx *ru, const cplx *rv, const cplx *rw, const cplx *T) {
+  int my = o->my, mz = o->mz;
+  double *Tp = o->st + (size_t)LMO_S_TP * my;
+  for (int i = 0; i < o->nkx; i++) {
+    double f = i == 0 ? 1.0 : 2.0;
+    for (int iy = 0; iy < o->nsp; iy++) { /* cross.f:2005-2031 */
+      int j = o->jsp[iy];
+      for (int kk = 0; kk < mz; kk++) {
+        int k = icx(o, kk);
+        size_t b = SIDX(o, i, kk, j);
+        o->sp[spidx(o, i, 8, iy, k)] += f * cabs2(ru[b]);
+        o->sp[spidx(o, i, 9, iy, k)] += f * cabs2(rv[b]);
+        o->sp[spidx(o, i, 10, iy, k)] += f * cabs2(rw[b]);
+        o->sp[spidx(o, i, 11, iy, k)] += f * cabs2(T[b]);
+      }
+    }
+    for (int kk = 0; kk < mz; kk++) /* cross.f:2034-2046 */
+      for (int j = 0; j < my; j++) Tp[j] += f * cabs2(T[SIDX(o, i, kk, j)]);
+  }
+  for (int j = 0; j < my; j++) { /* cross.f:2050-2058 */
+    o->st[(size_t)LMO_S_RUM * my + j] += creal(ru[j]);
+    o->st[(size_t)LMO_S_RVM * my + j] += creal(rv[j]);
+    o->st[(size_t)LMO_S_RWM * my + j] += creal(rw[j]);
+    o->st[(size_t)LMO_S_TM * my + j] += creal(T[j]);
+  }
+}
+
+static void addstats2(lmo *o, const cplx *u1, const cplx *u2, const cplx *u3) {
+  int my = o->my, mz = o->mz, nkx = o->nkx;
+  size_t ns = (size_t)o->nmode * my;
+  /* du/dy, dv/dy, dw/dy (cross.f:749-750 and 2152) */
+  cplx *du = xcalloc(ns, sizeof(cplx)), *dv = xcalloc(ns, sizeof(cplx)), *dw = xcalloc(ns, sizeof(cplx));
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 4 * my);
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      size_t b = (size_t)m * my;
+      deryr2_c(o, u1 + b, du + b, s, s + my, s + 2 * my, s + 3 * my);
+      deryr2_c(o, u2 + b, dv + b, s, s + my, s + 2 * my, s + 3 * my);
+      deryr2_c(o, u3 + b, dw + b, s, s + my, s + 2 * my, s + 3 * my);
+    }
+    free(s);
+  }
+  double *P[11];
+  for (int q = 0; q < 11; q++) P[q] = o->st + (size_t)(LMO_S_UP + q) * my;
+  double *thep = o->st + (size_t)LMO_S_THEP * my, *theup = o->st + (size_t)LMO_S_THEUP * my;
+  for (int q = 0; q < 9; q++) o->uner[q] = 0.0; /* cross.f:801-803 */
+  for (int i = 0; i < nkx; i++) {
+    double f = i == 0 ? 1.0 : 2.0, a = o->kxv[i];
+    for (int kk = 0; kk < mz; kk++) {
+      double bz = o->kzv[kk];
+      for (int j = 0; j < my; j++) {
+        size_t b = SIDX(o, i, kk, j);
+        cplx u = u1[b], v = u2[b], w = u3[b];
+        cplx o1 = dw[b] - I * bz * v, o2 = I * bz * u - I * a * w, o3 = I * a * v - du[b]; /* cross.f:755-766 */
+        double e[9];
+        e[0] = f * cabs2(u); e[1] = f * cabs2(v); e[2] = f * cabs2(w);       /* cross.f:2153-2182 */
+        e[3] = f * creal(u * conj(v)); e[4] = f * creal(u * conj(w));
+        e[5] = f * creal(w * conj(v));
+        e[6] = f * cabs2(o1); e[7] = f * cabs2(o2); e[8] = f * cabs2(o3);
+        for (int q = 0; q < 9; q++) P[q][j] += e[q];
+        cplx cc = I * a * u + dv[b] + I * bz * w; /* cross.f:2184-2188 */
+        thep[j] += f * cabs2(cc);
+        theup[j] += f * creal(cc * conj(v));
+        double aa = (a * a + bz * bz) * (cabs2(u) + cabs2(v) + cabs2(w)) + cabs2(dv[b]); /* cross.f:2190-2203 */
+        cplx c1 = o1 + I * bz * v, c3 = o3 - I * a * v;
+        aa += cabs2(c1) + cabs2(c3);
+        P[10][j] += f * aa;
+        for (int q = 0; q < 9; q++) o->uner[q] += e[q] * o->hy[j]; /* cross.f:2207-2210 */
+      }
+    }
+    for (int iy = 0; iy < o->nsp; iy++) { /* cross.f:2100-2147 */
+      int j = o->jsp[iy];
+      for (int kk = 0; kk < mz; kk++) {
+        int k = icx(o, kk);
+        double bz = o->kzv[kk];
+        size_t b = SIDX(o, i, kk, j);
+        cplx u = u1[b], v = u2[b], w = u3[b];
+        cplx o1 = dw[b] - I * bz * v, o2 = I * bz * u - I * a * w, o3 = I * a * v - du[b];
+        cplx uv = u * conj(v);
+        double c[8] = {cabs2(u), cabs2(v), cabs2(w), creal(uv), cimag(uv), cabs2(o1), cabs2(o2), cabs2(o3)};
+        for (int q = 0; q < 8; q++) o->sp[spidx(o, i, q, iy, k)] += f * c[q];
+      }
+    }
+  }
+  for (int j = 0; j < my; j++) { /* cross.f:2279-2289, kx = kz = 0 */
+    cplx o1 = dw[j], o3 = -du[j];
+    o->st[(size_t)LMO_S_UM * my + j] += creal(u1[j]);
+    o->st[(size_t)LMO_S_VM * my + j] += creal(u2[j]);
+    o->st[(size_t)LMO_S_WM * my + j] += creal(u3[j]);
+    o->st[(size_t)LMO_S_W1M * my + j] += creal(o1);
+    o->st[(size_t)LMO_S_W2M * my + j] += 0.0;
+    o->st[(size_t)LMO_S_W3M * my + j] += creal(o3);
+    o->st[(size_t)LMO_S_THEM * my + j] += creal(dv[j]);
+  }
+  free(du); free(dv); free(dw);
 }
 
 /* ------------------------------------------------------------------ */
@@ -1016,11 +1169,18 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     o->u00wk[j] += dtxi * o->rf0u[j];
     o->w00wk[j] += dtxi * o->rf0w[j];
   }
+  const int do_st = o->istati && r == 0 && o->st;
+  if (do_st) addstats1(o, mxw, myw, mzw, drho); /* cross.f:578-585 */
   /* (5) foup2 */
   int do_cfl = (r == 0 && o->icfl == 1 && o->dtmode == 0);
   cplx *in8[8] = {mxw, myw, mzw, nyw, t12, t13, t23, drho};
   cplx *out11[11] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, drho, chwk2};
   foup2(o, r, dtxi, dtgamma, dtbeta, do_cfl, ihist && r == 0, in8, out11);
+  if (do_st) { /* cross.f:796-812 (u, v, w are not changed in between) */
+    o->nacum++;
+    o->nacumsp++;
+    addstats2(o, mxw, myw, mzw);
+  }
 
 #pragma omp parallel num_threads(o->nthreads)
   {
@@ -1482,7 +1642,7 @@ static void substep14(lmo *o, int r, int ihist) {
   }
 }
 
-/* Time loop body: cross.f:225-1226 (stats, images and .cf output are the
+/* Time loop body: cross.f:225-1226 (images, .sta/.spe and .cf output are the
  * caller's business); the 2014 variant follows lomacte/cross.f:212-1040,
  * whose Deltat changes inside the first substep of a CFL step. */
 int lmo_step(lmo *o, int nsteps) {
@@ -1513,6 +1673,44 @@ int lmo_step(lmo *o, int nsteps) {
 int lmo_set_variant(lmo *o, int variant) {
   if (!o || variant < 0 || variant > 1) return -1;
   o->variant = variant;
+  return 0;
+}
+
+int lmo_stats_reset(lmo *o, int nsp, const int *jsp, double sigma) {
+  if (!o || nsp < 0 || (nsp && !jsp) || o->variant) return -1;
+  for (int i = 0; i < nsp; i++)
+    if (jsp[i] < 1 || jsp[i] > o->my) return -1;
+  free(o->jsp); free(o->st); free(o->sp);
+  o->nsp = nsp;
+  o->jsp = xcalloc(nsp, sizeof(int));
+  for (int i = 0; i < nsp; i++) o->jsp[i] = jsp[i] - 1;
+  o->sigma = sigma;
+  o->st = xcalloc((size_t)LMO_NSTAT * o->my, 8);
+  o->sp = xcalloc((size_t)o->nkx * 12 * nsp * (o->nz1 + 1), 8);
+  memset(o->uner, 0, sizeof(o->uner));
+  o->nacum = o->nacumsp = 0;
+  return 0;
+}
+
+int lmo_stats_step(lmo *o, int nsteps) {
+  if (!o || !o->st) return -1;
+  o->istati = 1;
+  int rc = lmo_step(o, nsteps);
+  o->istati = 0;
+  return rc;
+}
+
+int lmo_stats_read(lmo *o, double *prof, double *spec, double *uner, int *counts, int clear_spectra) {
+  if (!o || !o->st) return -1;
+  size_t nsp = (size_t)o->nkx * 12 * o->nsp * (o->nz1 + 1);
+  if (prof) memcpy(prof, o->st, sizeof(double) * LMO_NSTAT * o->my);
+  if (spec) memcpy(spec, o->sp, sizeof(double) * nsp);
+  if (uner) memcpy(uner, o->uner, sizeof(o->uner));
+  if (counts) { counts[0] = o->nacum; counts[1] = o->nacumsp; }
+  if (clear_spectra) { /* escru.f:466-477 */
+    memset(o->sp, 0, sizeof(double) * nsp);
+    o->nacumsp = 0;
+  }
   return 0;
 }
 

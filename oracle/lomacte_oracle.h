@@ -61,6 +61,26 @@ int lmo_substep(lmo *o, int r);
 #define LMO_NDIAG 13
 void lmo_get_diag(const lmo *o, double *d);
 
+/* Statistics (addstats1 cross.f:1981-2064, addstats2 cross.f:2070-2290,
+ * the physical sums of phys2 cross.f:1583-1607, writestats
+ * escru.f:276-484, resetstats escru.f:485-580).  Profiles are kept raw
+ * (without the 1/(mgalx*mgalz) of writestats) in the order of the .sta
+ * record; spectra as [kx plane][field 0..11][spectra plane][|kz|].
+ * reset: zero everything, set the 1-based spectra rows and the exponent of
+ * mu/mu0 = T^sigma; step: nsteps RK3 steps with istati = 1; read: copy
+ * out (NULL skips), counts = {nacum, nacumsp}; clear_spectra zeroes the
+ * spectra and nacumsp as writestats does. */
+#define LMO_NSTAT 33
+enum {
+  LMO_S_UM, LMO_S_VM, LMO_S_WM, LMO_S_RUM, LMO_S_RVM, LMO_S_RWM, LMO_S_TM, LMO_S_W1M, LMO_S_W2M,
+  LMO_S_W3M, LMO_S_THEM, LMO_S_UP, LMO_S_VP, LMO_S_WP, LMO_S_UVR, LMO_S_UWR, LMO_S_VWR, LMO_S_W1P,
+  LMO_S_W2P, LMO_S_W3P, LMO_S_TP, LMO_S_EP, LMO_S_RUU, LMO_S_RUV, LMO_S_RUW, LMO_S_RVV, LMO_S_RVW,
+  LMO_S_RWW, LMO_S_RHOM, LMO_S_THEP, LMO_S_THEUP, LMO_S_MUM, LMO_S_NUM
+};
+int lmo_stats_reset(lmo *o, int nsp, const int *jsp, double sigma);
+int lmo_stats_step(lmo *o, int nsteps);
+int lmo_stats_read(lmo *o, double *prof, double *spec, double *uner, int *counts, int clear_spectra);
+
 /* Coefficient access for tests (band storage row-major [row][band]). */
 void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12,
                    double *prem3_lu, double *dt21, double *dt22, double *fmap);

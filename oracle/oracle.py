@@ -60,6 +60,10 @@ def lib():
             getattr(L, n).argtypes = [ctypes.c_void_p, _dp, _dp]
         for n in ("lmo_lapvdvhom", "lmo_solvepsi"):
             getattr(L, n).argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.c_double]
+        L.lmo_stats_reset.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.c_double]
+        L.lmo_stats_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.lmo_stats_read.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.lmo_cft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         L.lmo_rft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         _lib = L
@@ -128,6 +132,31 @@ class Oracle:
 
     def substep(self, r=0):
         lib().lmo_substep(self.h, r)
+
+    # statistics: addstats1/2 and the phys2 sums (cross.f:578-585, 794-812,
+    # 1583-1607), resetstats (escru.f:485-580)
+    def stats_reset(self, planes, sigma=0.0):
+        jsp = (ctypes.c_int * max(1, len(planes)))(*[int(j) for j in planes])
+        if lib().lmo_stats_reset(self.h, len(planes), jsp, float(sigma)) != 0:
+            raise ValueError("lmo_stats_reset rejected its arguments")
+        self._nsp = len(planes)
+
+    def stats_step(self, n=1):
+        if lib().lmo_stats_step(self.h, n) != 0:
+            raise RuntimeError("lmo_stats_step: no statistics set up")
+
+    def stats_read(self, clear_spectra=False):
+        """(profiles [33, my], spectra [nkx, 12, nsp, nz1+1], uner [9],
+        nacum, nacumsp) -- the raw accumulators, .sta order."""
+        nkx, mz, _ = self.shape
+        nz1 = (mz - 1) // 2
+        prof = np.zeros((33, self.my))
+        spec = np.zeros((nkx, 12, self._nsp, nz1 + 1))
+        uner = np.zeros(9)
+        cnt = (ctypes.c_int * 2)()
+        if lib().lmo_stats_read(self.h, _p(prof), _p(spec), _p(uner), cnt, int(bool(clear_spectra))) != 0:
+            raise RuntimeError("lmo_stats_read: no statistics set up")
+        return prof, spec, uner, cnt[0], cnt[1]
 
     def diag(self):
         d = np.zeros(NDIAG)

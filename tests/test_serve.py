@@ -55,7 +55,9 @@ def test_graph_replay_matches_direct(gpu, prec):
 
 def _requests(prec):
     grids = [(64, 129), (96, 97), (64, 65), (128, 129)]
-    return [RunRequest(rid=i, nx=nx, nz=nx, ny=ny, steps=12 + 3 * i, Re=150.0 + 50 * i, s=2.0 + i,
+    # long enough (>= 150 steps) that a case is still running when the
+    # next one has been prepared, so the mix really overlaps
+    return [RunRequest(rid=i, nx=nx, nz=nx, ny=ny, steps=150 + 30 * i, Re=150.0 + 50 * i, s=2.0 + i,
                        seed=100 + i, precision=prec, arrival=0.0) for i, (nx, ny) in enumerate(grids)]
 
 
