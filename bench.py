@@ -305,6 +305,24 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
         nbytes = 4 * S * 16 + 3 * p.my * 8
         e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
+
+    # cost of a statistics step (addstats1/2 and the phys2 sums at the first
+    # substep, lmc_stats_step) beside a plain step, CUDA events on the
+    # library's stream, best of three each; plain steps replay a CUDA graph,
+    # statistics steps enqueue their kernels directly
+    def one(fn):
+        g.sync()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        fn(1)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        return s0.elapsed_time(s1)
+    g.stats_reset([(p.my + 1) // 2])
+    t_plain = min(one(g.step) for _ in range(3))
+    t_stats = min(one(g.stats_step) for _ in range(3))
+    stats_step = {"plain_step_ms": t_plain, "stats_step_ms": t_stats, "spectra_planes": 1}
     g.close()
 
     # roofline of the dominant kernel, live CUDA-event times of the timed region
@@ -332,6 +350,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     step_bytes = 3 * sum(f(S, Z, P, w) for f in ALGO.values())
     return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
             "kernel_share": share, "e2e": e2e, "state": state, "diag": diag, "step_bytes": step_bytes,
+            "stats_step": stats_step,
             "launches_per_step": launches, "y_family": y_family,
             "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
 
@@ -411,12 +430,13 @@ def main():
             "y_kernels": head["y_family"],
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "step_roofline_frac": head["step_roofline_frac"],
-            "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving,
+            "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving, "stats_step": head["stats_step"],
         }
         if mixed and 0 in arms:
             f64 = arms[0]
             line["fp64"] = {"value": f64["value"], "ms_per_step": f64["ms"] / a.steps, "roofline": f64["roofline"],
-                            "kernel_share": f64["kernel_share"], "e2e": f64["e2e"], "clocks": f64["clocks"]}
+                            "kernel_share": f64["kernel_share"], "e2e": f64["e2e"], "clocks": f64["clocks"],
+                            "stats_step": f64["stats_step"]}
             line["mixed_over_fp64"] = head["value"] / f64["value"]
             line["error_vs_fp64"] = {"rel_l2": errs, "steps": a.warmup + a.steps,
                                      "note": "mixed vs FP64 GPU path from the same seeded state"}

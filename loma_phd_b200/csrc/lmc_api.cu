@@ -661,7 +661,7 @@ int lmc_stats_reset(lmc_handle *h, int nsp, const int *jsp, double sigma) {
   if (!st.prof) {
     const size_t ns = (size_t)d.nmode * my;
     if ((rc = dalloc(h, &st.prof, (size_t)lmc::NSTAT * my)) || (rc = dalloc(h, &st.erow, (size_t)9 * my)) ||
-        (rc = dalloc(h, &st.uner, (size_t)9)))
+        (rc = dalloc(h, &st.uner, (size_t)9)) || (rc = dalloc(h, &st.xpart, (size_t)9 * my * lmc::XGRP)))
       return rc;
     for (int q = 0; q < 3; q++)
       if ((rc = dalloc(h, &st.dy[q], ns))) return rc;

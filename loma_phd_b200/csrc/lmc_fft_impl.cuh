@@ -47,11 +47,13 @@ struct Geo {
   static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
 };
 
-// z-transform blocks by storage type: twice as many kx lines for FP32
-// storage, so that every strided z row moves the same number of bytes
-template <int N1, int N2, typename ST>
+// z-transform blocks by butterfly type: twice as many kx lines for FP32
+// butterflies (and FP32 storage), so that every strided z row moves the same
+// number of bytes; FP64 butterflies keep the FP64 block, whose shared-memory
+// lines are twice as wide
+template <int N1, int N2, typename CT>
 struct ZGeo {
-  static constexpr int W = sizeof(ST) == sizeof(float2) ? 2 : 1;
+  static constexpr int W = sizeof(CT) == sizeof(float2) ? 2 : 1;
   static constexpr int KB = (64 * W / N1) > 0 ? (64 * W / N1) : 1;
   static constexpr int ZT = round32(KB * N1);
 };
@@ -73,11 +75,11 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // mode 0: the eight transform inputs of the substep; mode 1 (2014 variant,
 // FP64): T before the substep and Delta T, for d(rho) (lomacte/cross.f:1760-1770)
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zinv(Dev d, int ntiles, int mode) {
+__global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
-  constexpr int KB = ZGeo<N1, N2, ST>::KB, LD = G::LD;
+  constexpr int KB = ZGeo<N1, N2, CT>::KB, LD = G::LD;
   constexpr int E = 16 / (int)sizeof(ST);  // stored values per 16-byte unit
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *W = (CT *)smraw;
@@ -162,13 +164,13 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zinv(Dev d, int ntiles
 // mode 0: the substep's outputs (field blockIdx.z in place); mode 1 (2014
 // variant): d(rho) from z-physical buffer 0 into the d(rho) spectral slot
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(ZGeo<N1, N2, ST>::ZT) k_zfwd(Dev d, int mode) {
+__global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zfwd(Dev d, int mode) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *sm = (CT *)smraw;
-  constexpr int KB = ZGeo<N1, N2, ST>::KB;
+  constexpr int KB = ZGeo<N1, N2, CT>::KB;
   const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * KB;
   const int nb = min(KB, d.nkx - i0);
   const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.nkx + i0;
@@ -517,18 +519,20 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xdrho(Dev d) {
 // Statistics of the physical fields on an accumulating substep (phys2,
 // cross.f:1583-1607): per y row the plane sums of u rho u, u rho v,
 // u rho w, v rho v, v rho w, w rho w (u_i = rho u_i T), 1/T, T^sigma and
-// T^(sigma+1).  One block per row inverts rho u, rho v, rho w and T (three
-// complex x transforms per z line, the same packing as k_xphys) before
-// k_xphys overwrites its inputs, and adds its sums in a fixed order.
+// T^(sigma+1).  Block (g, y) inverts rho u, rho v, rho w and T (three
+// complex x transforms per z line, the same packing as k_xphys) on the z
+// tiles g, g + ngrp, ... of row y before k_xphys overwrites its inputs and
+// writes its partial sums to st.xpart; k_xsum adds the ngrp partials of a
+// row in order, so the sums are reproducible.
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xstats(Dev d, Stats st) {
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xstats(Dev d, Stats st, int ngrp) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, NW = G::XT / 32;
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *W = (CT *)smraw;  // 3 groups x ZB lines x LD
   __shared__ double sh[NW * 9];
-  const int y = blockIdx.x, nkx = d.nkx, my = d.my;
+  const int y = blockIdx.y, grp = blockIdx.x, nkx = d.nkx, my = d.my;
   double m0 = 0.0, m1 = 0.0, m2 = 0.0, m5 = 0.0;  // mixed form: FP64 00 profiles
   if constexpr (sizeof(ST) == sizeof(float2)) {
     m0 = d.mi[y];
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xstats(Dev d, Stats st) {
 #pragma unroll
   for (int q = 0; q < 9; q++) a[q] = 0.0;
   const int gap = N - 2 * nkx + 1;
-  for (int z0 = 0; z0 < d.mgalz; z0 += ZB) {
+  for (int z0 = grp * ZB; z0 < d.mgalz; z0 += ngrp * ZB) {
     const int nzb = min(ZB, d.mgalz - z0);
     for (int idx = threadIdx.x; idx < 3 * ZB * gap; idx += blockDim.x) {
       const int ln = idx / gap, g = idx - ln * gap;
@@ -596,9 +600,20 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xstats(Dev d, Stats st) {
     const int q = threadIdx.x;
     double s = 0.0;
     for (int w = 0; w < NW; w++) s += sh[w * 9 + q];
-    const int dst = q < 7 ? ST_RUU + q : ST_MUM + (q - 7);  // ruu..rww, rhom, mum, num
-    st.prof[(size_t)dst * my + y] += s;
+    st.xpart[((size_t)q * my + y) * ngrp + grp] = s;
   }
+}
+
+// the partial sums of k_xstats, group by group, into the profiles
+template <int N1, int N2>
+__global__ void k_xsum(Dev d, Stats st, int ngrp) {
+  const int y = blockIdx.x, q = threadIdx.x;
+  if (q >= 9) return;
+  const double *src = st.xpart + ((size_t)q * d.my + y) * ngrp;
+  double s = 0.0;
+  for (int g = 0; g < ngrp; g++) s += src[g];
+  const int dst = q < 7 ? ST_RUU + q : ST_MUM + (q - 7);  // ruu..rww, rhom, mum, num
+  st.prof[(size_t)dst * d.my + y] += s;
 }
 
 // Plane sums of the mixed form's outputs from the partial sums of k_xphys,
@@ -623,7 +638,7 @@ template <int N1, int N2, typename CT, typename ST>
 struct Launch {
   using G = Geo<N1, N2>;
   static constexpr int E = 16 / (int)sizeof(ST);
-  using ZG = ZGeo<N1, N2, ST>;
+  using ZG = ZGeo<N1, N2, CT>;
   static size_t zsm() { return (size_t)ZG::KB * G::LD * sizeof(CT); }
   static size_t zinv_sm(int mz) {
     return round16(sizeof(CT) * ZG::KB * G::LD) + ((size_t)ZG::KB * mz + 2 * E) * sizeof(ST);
@@ -670,7 +685,9 @@ struct Launch {
   }
   static size_t xstats_sm() { return (size_t)3 * G::ZB * G::LD * sizeof(CT); }
   static void xstats(const Dev &d, const Stats &st, cudaStream_t s) {
-    k_xstats<N1, N2, CT, ST><<<d.my, G::XT, xstats_sm(), s>>>(d, st);
+    const int ntile = (d.mgalz + G::ZB - 1) / G::ZB, ngrp = ntile < XGRP ? ntile : XGRP;
+    k_xstats<N1, N2, CT, ST><<<dim3(ngrp, d.my), G::XT, xstats_sm(), s>>>(d, st, ngrp);
+    k_xsum<N1, N2><<<d.my, 32, 0, s>>>(d, st, ngrp);
   }
   static cudaError_t optin1(const void *fn, int limit) {
     cudaError_t e;

@@ -85,14 +85,16 @@ struct Dev {
 //   uner [9]          sum_j hy_j erow_j (cross.f:2207-2210)
 //   dy   [3]          du/dy, dv/dy, dw/dy of the step ([y][kx][kz])
 //   jsp  [nsp]        0-based rows of the spectra planes
+//   xpart[9][my][XGRP] partial physical-space sums (z-tile groups)
 struct Stats {
-  double *prof, *spec, *erow, *uner;
+  double *prof, *spec, *erow, *uner, *xpart;
   double2 *dy[3];
   const int *jsp;
   int nsp;
   double sigma;  // mu/mu0 = T^sigma (main.f:570)
 };
 constexpr int NSTAT = 33;
+constexpr int XGRP = 32;  // z-tile groups of the physical-space sums
 enum {
   ST_UM = 0, ST_VM, ST_WM, ST_RUM, ST_RVM, ST_RWM, ST_TM, ST_W1M, ST_W2M, ST_W3M, ST_THEM,
   ST_UP, ST_VP, ST_WP, ST_UVR, ST_UWR, ST_VWR, ST_W1P, ST_W2P, ST_W3P, ST_TP, ST_EP,
