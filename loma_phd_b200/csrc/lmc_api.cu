@@ -375,7 +375,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     }
   }
   if (d.tpm)
-    for (int q = 0; q < 4; q++)
+    for (int q = 0; q < 5; q++)
       if ((rc = dalloc(h, &d.ws[q], ns))) { lmc_destroy(h); return rc; }
   if (d.variant &&
       ((rc = dalloc(h, &d.Told, ns)) || (rc = dalloc(h, &d.dTs, ns)) || (rc = dalloc(h, &d.RT, ns)))) {
@@ -493,8 +493,9 @@ namespace {
 // Enqueue the kernels of one RK3 step on the handle's streams (directly, or
 // into a graph being captured) and advance the host-side bookkeeping.
 // Two independent pieces of each substep run on the second stream, beside
-// the main chain: the T derivatives beside Lapvdvhom and the assembly of
-// rho u_i (neither reads what the other writes), and, in the mode-parallel
+// the main chain: the T derivatives and the z transforms of the inputs made
+// from T beside Lapvdvhom, the assembly of rho u_i and its z transforms
+// (neither chain reads what the other writes), and, in the mode-parallel
 // family, the psi solve beside post1 (it reads only d(rho)/dt).  The 2014
 // variant differentiates the T that its assembly saves, and takes d(rho)
 // from a transform round trip after post1, so it runs in one chain.
@@ -521,23 +522,28 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
       d.mo_cur = h->mo[h->mo_flip];
       d.mo_prev = h->mo[1 - h->mo_flip];
     }
+    // the T derivatives and the inverse z transforms of the five inputs
+    // made from T (lap T, dT/dx, dT/dy, dT/dz, T) run beside Lapvdvhom, the
+    // assembly of rho u_i and the z transforms of rho u_i
     if (side_t) {
       if (!fork()) return LMC_ECUDA;
       run(2, s2, [&] { lmc::launch_tder(d, s2); });
+      run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 3, 5); });
       if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
     }
     run(0, s, [&] { lmc::launch_lapv(d, s); });
     run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
     if (side_t) {
+      run(3, s, [&] { lmc::launch_zinv(d, s, 0, 0, 3); });
       if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
     } else {
       run(2, s, [&] { lmc::launch_tder(d, s); });
+      run(3, s, [&] { lmc::launch_zinv(d, s); });
     }
     // statistics of an accumulating step, first substep (cross.f:578-585,
     // 794-812, 1583-1607); id 10 in the profile
     const bool st_now = stats && rk == 0;
     if (st_now) run(10, s, [&] { lmc::launch_stats1(d, h->st, s); });
-    run(3, s, [&] { lmc::launch_zinv(d, s); });
     if (st_now) run(10, s, [&] { lmc::launch_xstats(d, h->st, s); });
     if (rk == 0) {
       LMC_CK(cudaMemsetAsync(d.rhom, 0, (size_t)d.my * sizeof(double), s));
@@ -550,7 +556,7 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
     });
     run(5, s, [&] { lmc::launch_zfwd(d, s); });
     if (st_now) run(10, s, [&] { lmc::launch_stats2(d, h->st, s); });
-    if (side_psi) {
+    if (side_psi) {  // beside post1 and post2, which neither read nor write its data
       if (!fork()) return LMC_ECUDA;
       run(8, s2, [&] { lmc::launch_psi_main(d, rk, s2); });
     }
@@ -560,8 +566,8 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
       run(4, s, [&] { lmc::launch_xdrho(d, s); });
       run(5, s, [&] { lmc::launch_zfwd(d, s, 1); });
     }
-    if (side_psi && !join()) return LMC_ECUDA;
     run(7, s, [&] { lmc::launch_post2(d, rk, s); });
+    if (side_psi && !join()) return LMC_ECUDA;
     if (side_psi) run(8, s, [&] { lmc::launch_psi_tail(d, rk, cfl_step, s); });
     else run(8, s, [&] { lmc::launch_psi(d, rk, cfl_step, 1, s); });
     if (d.prec) {
@@ -769,7 +775,7 @@ int lmc_launches_per_step(lmc_handle *h) {
   // the 2014 variant: 14 kernels per substep (three for the d(rho) round
   // trip, its own 00 tail) and the Deltat kernel in the first substep
   if (h->d.variant) return 3 * 14 + 1;
-  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0);
+  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0) + 1;  // + the split inverse z transform
   return 3 * per;
 }
 
@@ -787,7 +793,7 @@ size_t lmc_footprint(const lmc_params *p) {
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)
   if (p->variant) b += 3 * S * 16;  // T before the substep, Delta T, RHS(T)
   if (p->variant || mode_parallel(g.nmode))
-    b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 4 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
+    b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 5 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
   else
     b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8 + (size_t)g.my * 15 * 8;  // Poisson, d/dy rows
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers

@@ -9,7 +9,7 @@ namespace lmc {
 
 #define LMC_FFT_DECL(SUF)                                                              \
   bool fft_has_##SUF(int n);                                                           \
-  bool fft_zinv_##SUF(const Dev &d, int mode, cudaStream_t s);                         \
+  bool fft_zinv_##SUF(const Dev &d, int mode, int f0, int nf, cudaStream_t s);         \
   bool fft_zfwd_##SUF(const Dev &d, int mode, cudaStream_t s);                         \
   bool fft_xdrho_##SUF(const Dev &d, cudaStream_t s);                                  \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
@@ -24,8 +24,8 @@ cudaError_t ykernels_init(int limit);
 
 bool fft_supported(int n) { return fft_has_a(n) || fft_has_b(n) || fft_has_c(n); }
 
-void launch_zinv(const Dev &d, cudaStream_t s, int mode) {
-  if (!fft_zinv_a(d, mode, s) && !fft_zinv_b(d, mode, s)) fft_zinv_c(d, mode, s);
+void launch_zinv(const Dev &d, cudaStream_t s, int mode, int f0, int nf) {
+  if (!fft_zinv_a(d, mode, f0, nf, s) && !fft_zinv_b(d, mode, f0, nf, s)) fft_zinv_c(d, mode, f0, nf, s);
 }
 void launch_zfwd(const Dev &d, cudaStream_t s, int mode) {
   if (!fft_zfwd_a(d, mode, s) && !fft_zfwd_b(d, mode, s)) fft_zfwd_c(d, mode, s);

@@ -75,7 +75,7 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // mode 0: the eight transform inputs of the substep; mode 1 (2014 variant,
 // FP64): T before the substep and Delta T, for d(rho) (lomacte/cross.f:1760-1770)
 template <int N1, int N2, typename CT, typename ST>
-__global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles, int mode) {
+__global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles, int mode, int f0) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     return (int)((((size_t)y * d.nkx + kb * KB) * d.mz) % E);
   };
   auto issue = [&](int t) {
-    const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
+    const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
     const int nb = min(KB, d.nkx - kb * KB);
     const size_t start = ((size_t)y * d.nkx + kb * KB) * d.mz;
     const int lead = (int)(start % E);
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     __syncthreads();
     if (!s_ok) return;
     ph ^= 1;
-    const int f = t / per_f, r = t - f * per_f, y = r / nkb, kb = r - y * nkb;
+    const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
     const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
     const int lead = lead_of(t);
     const int mult = mode ? 0 : (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
@@ -657,11 +657,16 @@ struct Launch {
     const int g = sms * per;
     return g < ntiles ? g : ntiles;
   }
-  static void zinv(const Dev &d, int mode, cudaStream_t s) {
-    const int ntiles = (mode ? 2 : 8) * d.my * ((d.nkx + ZG::KB - 1) / ZG::KB);
+  // fields f0 .. f0+nf-1 of the eight inputs (nf <= 0: all of them)
+  static void zinv(const Dev &d, int mode, int f0, int nf, cudaStream_t s) {
+    if (nf <= 0) {
+      f0 = 0;
+      nf = mode ? 2 : 8;
+    }
+    const int ntiles = nf * d.my * ((d.nkx + ZG::KB - 1) / ZG::KB);
     const size_t sm = zinv_sm(d.mz);
     const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, ZG::ZT, sm, ntiles);
-    k_zinv<N1, N2, CT, ST><<<g, ZG::ZT, sm, s>>>(d, ntiles, mode);
+    k_zinv<N1, N2, CT, ST><<<g, ZG::ZT, sm, s>>>(d, ntiles, mode, f0);
   }
   static void zfwd(const Dev &d, int mode, cudaStream_t s) {
     dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : 11));
@@ -738,7 +743,8 @@ inline cudaError_t upload_twiddles() {
   case N: LMC_FFT_FORMS(N1, N2, xphys(d, rk, do_cfl, do_diag, s)) return true;
 #define LMC_FFT_CASE_XST(N, N1, N2) \
   case N: LMC_FFT_FORMS(N1, N2, xstats(d, st, s)) return true;
-#define LMC_FFT_CASE_ZI(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zinv)
+#define LMC_FFT_CASE_ZI(N, N1, N2) \
+  case N: LMC_FFT_FORMS(N1, N2, zinv(d, mode, f0, nf, s)) return true;
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
 #define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3);
@@ -754,7 +760,7 @@ inline cudaError_t upload_twiddles() {
   bool fft_has_##SUF(int n) {                                                                     \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_HAS) default: return false; }                         \
   }                                                                                               \
-  bool fft_zinv_##SUF(const Dev &d, int mode, cudaStream_t s) {                                   \
+  bool fft_zinv_##SUF(const Dev &d, int mode, int f0, int nf, cudaStream_t s) {                   \
     switch (d.mgalz) { LMC_FFT_SIZES(LMC_FFT_CASE_ZI) default: return false; }                     \
   }                                                                                               \
   bool fft_zfwd_##SUF(const Dev &d, int mode, cudaStream_t s) {                                   \

@@ -29,8 +29,9 @@ struct Dev {
   const double *PL, *PU, *V12, *AAinv, *k2;
   // Mode-parallel y kernels (tpm = 1, lmc_ytpm.cuh): the same operators in
   // row form ([my][band], one row read by all threads of a warp), per-mode
-  // Poisson tables mode-fastest ([my][band][nmode]), and four FP64
-  // spectral scratch fields for the forward halves of the banded solves.
+  // Poisson tables mode-fastest ([my][band][nmode]), and five FP64
+  // spectral scratch fields for the forward halves of the banded solves
+  // (the fifth is the psi solve's, which runs beside post1 and post2).
   int tpm;
   // 2014 variant (trunk/lomacte): spectral T before this substep's update,
   // its increment Delta T, and the previous substep's spectral RHS(T);
@@ -40,7 +41,7 @@ struct Dev {
   const double2 *tsrc;
   const double *r_dt12, *r_dt11, *r_dt22, *r_dt21, *r_p1L, *r_p1U, *r_p3L, *r_p3U, *r_fmap, *r_ebot, *r_etop;
   const double *PLt, *PUt, *V12t;
-  double2 *ws[4];
+  double2 *ws[5];
   const double *kx, *kz;  // wavenumber per kx plane / kz index
   const double2 *twx, *twz;  // exp(-2 pi i e / N) for the x / z transform lengths
   const float2 *twxf, *twzf;  // the same in FP32 (mixed form)
@@ -132,8 +133,9 @@ bool fft_supported(int n);
 void launch_lapv(const Dev &d, cudaStream_t s);
 void launch_assemble(const Dev &d, int rk, cudaStream_t s);
 void launch_tder(const Dev &d, cudaStream_t s);
-// mode 1 (2014 variant): the d(rho) round trip of T and Delta T
-void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0);
+// mode 1 (2014 variant): the d(rho) round trip of T and Delta T; f0, nf:
+// only inputs f0 .. f0+nf-1 (nf <= 0: all)
+void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0, int f0 = 0, int nf = 0);
 void launch_xdrho(const Dev &d, cudaStream_t s);
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);
 void launch_zfwd(const Dev &d, cudaStream_t s, int mode = 0);

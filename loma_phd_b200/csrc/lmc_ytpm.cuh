@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(TB) t_psi(Dev d, int rk) {
   if (!mode_of(d, M)) return;
   const int my = d.my;
   const size_t ld = d.nmode;
-  double2 *s1 = d.ws[3] + M.m;  // 3: runs beside post1
+  double2 *s1 = d.ws[4] + M.m;  // its own scratch: runs beside post1 and post2
   const double sc = V ? -1.0 / (d.scal_d[0] * (d.gama[rk] + d.xi[rk])) : 1.0;
   {
     Rd<CT, kq<CT>(8)> r;

@@ -114,6 +114,6 @@ def test_automatic_family_choice(gpu, monkeypatch):
     small = Lomacte(*case(32, 32, 33)[:2])
     big = Lomacte(*case(192, 192, 33)[:2])  # 96 x 191 = 18336 modes
     assert small.y_family == "warp" and big.y_family == "mode"
-    assert big.launches_per_step == 33 and small.launches_per_step == 30
+    assert big.launches_per_step == 36 and small.launches_per_step == 33
     small.close()
     big.close()
