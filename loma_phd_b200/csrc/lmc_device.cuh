@@ -534,6 +534,37 @@ struct Four {
       }
     }
     __syncthreads();
+    nat2perm_p2<SIGN, U>(sm, nb, ld);
+  }
+
+  // the first pass of nat2perm with sample n of line b supplied by
+  // load(b, n) instead of read from shared memory (ends with a barrier)
+  template <int SIGN, typename L>
+  __device__ static void nat2perm_in(CT *sm, int nb, int ld, const CT *__restrict__ twN, L &&load) {
+    for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
+      const int b = idx / N1, n1 = idx - b * N1;
+      CT *p = sm + (size_t)b * ld + n1;
+      CT x[N2];
+#pragma unroll
+      for (int j = 0; j < N2; j++) x[j] = load(b, n1 + N1 * j);
+      rdft<N2, SIGN>(x);
+#pragma unroll
+      for (int k = 0; k < N2; k++) {
+        CT v = x[k];
+        if (k > 0 && n1 > 0) {
+          CT w = __ldg(twN + n1 * k);
+          if (SIGN > 0) w = cconj(w);
+          v = cmul(v, w);
+        }
+        p[k * (N1 + 1)] = v;
+      }
+    }
+    __syncthreads();
+  }
+
+  // the second pass of nat2perm (ends with a barrier)
+  template <int SIGN, int U = 1>
+  __device__ static void nat2perm_p2(CT *sm, int nb, int ld) {
     #pragma unroll U
     for (int idx = threadIdx.x; idx < nb * N2; idx += blockDim.x) {
       const int b = idx / N2, k2 = idx - b * N2;

@@ -305,39 +305,38 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         s_est[q] = e;
       }
     }
-    // zero the dealiased gap kx = nkx .. N-nkx of the 4 input lines
-    const int gap = N - 2 * nkx + 1;
-    for (int idx = threadIdx.x; idx < 4 * ZB * gap; idx += blockDim.x) {
-      const int ln = idx / gap, g = idx - ln * gap;
-      W[ln * LD + F::sk(nkx + g)] = cz<CT>();
-    }
-    for (int p = 0; p < 4; p++)
-      for (int l = 0; l < ZB; l++) {
-        CT *line = W + (p * ZB + l) * LD;
-        const ST *A = St + (2 * p) * ZB * nkx + l * nkx, *B = St + (2 * p + 1) * ZB * nkx + l * nkx;
-        for (int k = threadIdx.x; k < nkx; k += blockDim.x) {
-          CT a = cz<CT>(), b = cz<CT>();
-          if (l < nzb) { a = ccvt<CT>(A[k]); b = ccvt<CT>(B[k]); }
-          if (k == 0) {
-            line[F::sk(0)] = cmk<CT>(a.x, b.x);  // Im of mode 0 dropped (rftsingle.f:85-88)
-          } else {
-            line[F::sk(k)] = cmk<CT>(a.x - b.y, a.y + b.x);
-            line[F::sk(N - k)] = cmk<CT>(a.x + b.y, b.x - a.y);
-          }
-        }
-      }
     double rh[PT];
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
       rh[j] = (q < nzb * N && !d.variant) ? Sr[q] : 0.0;
     }
-    __syncthreads();
+    // the first transform pass reads the staged input rows directly: line
+    // p*ZB + l packs fields 2p, 2p+1 of z line l as A + iB of the complex
+    // spectrum, kx = nkx .. N-nkx (the dealiased gap) are zero, and the
+    // imaginary part of mode 0 is dropped (rftsingle.f:85-88)
+    auto load = [&](int b, int n) -> CT {
+      const int p = b / ZB, l = b - p * ZB;
+      if (l >= nzb) return cz<CT>();
+      const ST *A = St + (2 * p) * ZB * nkx + l * nkx, *B = A + ZB * nkx;
+      if (n < nkx) {
+        const CT a = ccvt<CT>(A[n]), c = ccvt<CT>(B[n]);
+        return n == 0 ? cmk<CT>(a.x, c.x) : cmk<CT>(a.x - c.y, a.y + c.x);
+      }
+      const int k = N - n;
+      if (k < nkx) {
+        const CT a = ccvt<CT>(A[k]), c = ccvt<CT>(B[k]);
+        return cmk<CT>(a.x + c.y, c.x - a.y);
+      }
+      return cz<CT>();
+    };
+    F::template nat2perm_in<+1>(W, 4 * ZB, LD, wtwx<CT>(d), load);
+    // the staged rows are consumed: stage the next tile meanwhile
     if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
       fence_proxy_async();
       issue(t + gridDim.x);
     }
-    F::template nat2perm<+1>(W, 4 * ZB, LD, wtwx<CT>(d));
+    F::template nat2perm_p2<+1>(W, 4 * ZB, LD);
 
     // mixed form: s_min / s_est (filled before the transform above) hold the
     // FP64 00 profiles of the inputs at this y and the values subtracted from
