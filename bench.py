@@ -94,6 +94,9 @@ def parse():
                     help="requests of the synthetic serving stream (0: skip)")
     ap.add_argument("--serve-scale", type=float, default=0.05,
                     help="factor on the stream's step counts (log-uniform in [200, 2000])")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="also run an ensemble of this many independent cases of uneven grids (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
@@ -374,6 +377,27 @@ def run_serving(a, dev):
     return out
 
 
+def run_ensemble(a, dev):
+    """An ensemble of independent cases of uneven grids (nx in {64..192},
+    ny in {97, 129, 193}, nz in {64, 96, 128}, seeds 0..n-1), all resident
+    at once and advanced concurrently, in the mixed form and in FP64:
+    makespan, aggregate throughput and per-case completion latency."""
+    import torch
+    from loma_phd_b200.serve import Server, ensemble_requests
+    free, _ = torch.cuda.mem_get_info(dev)
+    cap = int(min(150e9, 0.8 * free))
+    out = {"ensemble": f"{a.ensemble} cases, {a.ensemble_steps} RK3 steps each, all at t=0, "
+                       f"nx in {{64,96,128,192}} x ny in {{97,129,193}} x nz in {{64,96,128}}, "
+                       f"Re~U[100,400], s~U[1,8], seeds 0..{a.ensemble - 1}, {a.ensemble} slots",
+           "unit": "s (latency, makespan, set-up), Mpts*RK3-steps/s (aggregate)"}
+    for name, prec in (("mixed", a.mixed_form), ("fp64", 0)):
+        reqs = ensemble_requests(a.ensemble, a.ensemble_steps, precision=prec)
+        st = Server(cap, max_active=a.ensemble, chunk=10, device=dev).run(reqs)["stats"]
+        out[name] = {k: st[k] for k in ("makespan_s", "aggregate_mpts_steps_per_s", "p50_latency_s",
+                                        "p99_latency_s", "max_concurrent", "peak_device_bytes", "mean_setup_s")}
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -409,6 +433,9 @@ def main():
     serving = None
     if world == 1 and a.serve_requests > 0:
         serving = run_serving(a, dev)
+    ensemble = None
+    if world == 1 and a.ensemble > 0:
+        ensemble = run_ensemble(a, dev)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a, head["p"], head["y"], head["st"])
@@ -431,6 +458,7 @@ def main():
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving, "stats_step": head["stats_step"],
+            "ensemble": ensemble,
         }
         if mixed and 0 in arms:
             f64 = arms[0]

@@ -63,10 +63,14 @@ void drop_graphs(lmc_handle *h);
     }                                                    \
   } while (0)
 
+// Device buffers come from the stream-ordered allocator on the handle's
+// stream and go back with cudaFreeAsync, so creating and destroying a case
+// never waits for the other cases running on the device (cudaFree would
+// synchronise the whole device).
 template <class T>
 int dalloc(lmc_handle *h, T **p, size_t n) {
   void *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 16);
+  cudaError_t e = cudaMallocAsync(&q, n * sizeof(T) + 16, h->s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? LMC_ENOMEM : LMC_ECUDA;
@@ -81,7 +85,8 @@ int dupload(lmc_handle *h, const T **p, const std::vector<T> &v) {
   T *q = nullptr;
   int r = dalloc(h, &q, v.size());
   if (r) return r;
-  LMC_CK(cudaMemcpy(q, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  // pageable source: the call returns once the data is staged
+  LMC_CK(cudaMemcpyAsync(q, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->s));
   *p = q;
   return LMC_OK;
 }
@@ -253,6 +258,13 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   lmc::build_poisson(g, h->ops, kx.data(), kz.data(), h->pt);
 
   if (cudaSetDevice(p->device) != cudaSuccess) { delete h; return LMC_ECUDA; }
+  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    lmc_destroy(h);
+    return LMC_ECUDA;
+  }
   d.my = g.my; d.mgalx = g.mgalx; d.mgalz = g.mgalz; d.nkx = g.nkx; d.mz = g.mz; d.nz1 = g.nz1; d.nmode = g.nmode;
   d.ldy = g.my | 1;
   d.ire = 1.0 / p->Re;
@@ -392,13 +404,6 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     lmc_destroy(h);
     return rc;
   }
-  if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
-    lmc_destroy(h);
-    return LMC_ECUDA;
-  }
   {
     const cudaError_t e = lmc::kernels_init(d);
     if (e != cudaSuccess) {
@@ -407,8 +412,12 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
       return LMC_ECUDA;
     }
   }
-  cudaMemset(d.status, 0, sizeof(int));
-  cudaMemset(d.diag, 0, 16 * sizeof(double));
+  if (cudaMemsetAsync(d.status, 0, sizeof(int), h->s) != cudaSuccess ||
+      cudaMemsetAsync(d.diag, 0, 16 * sizeof(double), h->s) != cudaSuccess ||
+      cudaStreamSynchronize(h->s) != cudaSuccess) {  // buffers and tables in place
+    lmc_destroy(h);
+    return LMC_ECUDA;
+  }
   *out = h;
   return LMC_OK;
 }
@@ -416,9 +425,12 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
 int lmc_destroy(lmc_handle *h) {
   if (!h) return LMC_EINVAL;
   cudaSetDevice(h->p.device);
-  if (h->s) cudaStreamSynchronize(h->s);
+  if (h->s) cudaStreamSynchronize(h->s);  // this case's own work only
   drop_graphs(h);
-  for (void *q : h->allocs) cudaFree(q);
+  for (void *q : h->allocs) {
+    if (h->s) cudaFreeAsync(q, h->s);
+    else cudaFree(q);
+  }
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
@@ -681,7 +693,7 @@ int lmc_stats_reset(lmc_handle *h, int nsp, const int *jsp, double sigma) {
           h->allocs.erase(h->allocs.begin() + i);
           break;
         }
-      cudaFree(q);
+      cudaFreeAsync(q, h->s);
     }
     h->bytes -= h->st_spec_bytes;
     st.spec = nullptr;
@@ -696,7 +708,7 @@ int lmc_stats_reset(lmc_handle *h, int nsp, const int *jsp, double sigma) {
   }
   std::vector<int> rows(nsp > 0 ? nsp : 1, 0);
   for (int i = 0; i < nsp; i++) rows[i] = jsp[i] - 1;
-  LMC_CK(cudaMemcpy((void *)st.jsp, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+  LMC_CK(cudaMemcpyAsync((void *)st.jsp, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice, h->s));
   LMC_CK(cudaMemsetAsync(st.prof, 0, (size_t)lmc::NSTAT * my * sizeof(double), h->s));
   LMC_CK(cudaMemsetAsync(st.spec, 0, (nspec ? nspec : 1) * sizeof(double), h->s));
   LMC_CK(cudaMemsetAsync(st.erow, 0, (size_t)9 * my * sizeof(double), h->s));

@@ -3,6 +3,8 @@
 // per-device set-up of all kernels.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "lmc_kernels.cuh"
 
 namespace lmc {
@@ -53,7 +55,13 @@ size_t z_smem(const Dev &d) {
   return v;
 }
 
+// Checks the grid's shared-memory needs against the device, and once per
+// device (not on every case: the constant-memory twiddles would be
+// rewritten under running kernels) uploads the twiddles and opts the
+// kernels in to the large shared-memory carve-out.
 cudaError_t kernels_init(const Dev &d) {
+  static std::mutex mu;
+  static bool done[64] = {false};
   int dev = 0, limit = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -61,10 +69,14 @@ cudaError_t kernels_init(const Dev &d) {
   const size_t need_y = (size_t)8 * d.ldy * sizeof(double2);
   if ((size_t)limit < xphys_smem(d) + 1024 || (size_t)limit < z_smem(d) + 1024 || (size_t)limit < need_y + 1024)
     return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
   if ((e = fft_init_a(limit)) != cudaSuccess) return e;
   if ((e = fft_init_b(limit)) != cudaSuccess) return e;
   if ((e = fft_init_c(limit)) != cudaSuccess) return e;
-  return ykernels_init(limit);
+  if ((e = ykernels_init(limit)) != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return cudaSuccess;
 }
 
 }  // namespace lmc

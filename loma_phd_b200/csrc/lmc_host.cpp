@@ -422,41 +422,60 @@ extern "C" int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_pa
     }
     std::vector<double> win(my);
     for (int j = 0; j < my; j++) win[j] = std::exp(-(y[j] / ic->swin) * (y[j] / ic->swin));
-    // 1) random velocity per mode (initloma3/src/main.f:128-226)
-    std::vector<cd> uf(ns, 0.0), vf(ns, 0.0), wf(ns, 0.0);
+    // Only the modes with 1 <= |k| <= nkmax (mode-index units) carry noise,
+    // and every step below works on one mode at a time, so every other mode
+    // is zero in all outputs (the 00 mode gets the mean profiles).  The
+    // band's modes are listed in increasing mode order.
+    std::vector<int> band, slot(g.nmode, -1);
+    for (int m = 0; m < g.nmode; m++) {
+      const int i = m / mz, kz = kzi[m % mz];
+      const double nh = std::sqrt((double)(i * i + kz * kz));
+      if (nh >= 1.0 && nh <= (double)ic->nkmax) {
+        slot[m] = (int)band.size();
+        band.push_back(m);
+      }
+    }
+    const int nb = (int)band.size();
+    const size_t nbs = (size_t)nb * my;
+    // 1) random velocity per mode (initloma3/src/main.f:128-226); modes are
+    // independent (counter-based random numbers), so the loops over the band
+    // run in parallel and the result does not depend on the threads
+    std::vector<cd> uf(nbs, 0.0), vf(nbs, 0.0), wf(nbs, 0.0);
     cd *fld[3] = {uf.data(), vf.data(), wf.data()};
     const int nym = ic->nymax > 0 ? ic->nymax : 1;
-    for (int i = 0; i < nkx; i++)
-      for (int k = 0; k < mz; k++) {
-        const int kz = kzi[k];
-        const double nh = std::sqrt((double)(i * i + kz * kz));
-        if (nh < 1.0 || nh > (double)ic->nkmax) continue;
-        if (i == 0 && kz < 0) continue;  // filled by Hermitian symmetry below
-        const double kh = std::sqrt(kxv[i] * kxv[i] + kzv[k] * kzv[k]);
-        for (int c = 0; c < 3; c++) {
-          cd *f = fld[c] + ((size_t)i * mz + k) * my;
-          for (int jj = 1; jj <= nym; jj++) {
-            const double a = 2.0 * (0.5 - urand(ic->seed, i, (uint64_t)(kz + 100000), c, 2 * jj));
-            const double ph = urand(ic->seed, i, (uint64_t)(kz + 100000), c, 2 * jj + 1);
-            const double ky = 2.0 * kh / nym * jj;
-            for (int j = 0; j < my; j++) f[j] += a * std::exp(cd(0.0, ky * y[j] + 2.0 * M_PI * ph)) * win[j];
-          }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; bi++) {
+      const int m = band[bi], i = m / mz, k = m % mz, kz = kzi[k];
+      if (i == 0 && kz < 0) continue;  // filled by Hermitian symmetry below
+      const double kh = std::sqrt(kxv[i] * kxv[i] + kzv[k] * kzv[k]);
+      for (int c = 0; c < 3; c++) {
+        cd *f = fld[c] + (size_t)bi * my;
+        for (int jj = 1; jj <= nym; jj++) {
+          const double a = 2.0 * (0.5 - urand(ic->seed, i, (uint64_t)(kz + 100000), c, 2 * jj));
+          const double ph = urand(ic->seed, i, (uint64_t)(kz + 100000), c, 2 * jj + 1);
+          const double ky = 2.0 * kh / nym * jj;
+          for (int j = 0; j < my; j++) f[j] += a * std::exp(cd(0.0, ky * y[j] + 2.0 * M_PI * ph)) * win[j];
         }
       }
-    for (int k = 0; k < mz; k++)
-      if (kzi[k] < 0)
-        for (int c = 0; c < 3; c++) {
-          const int kp = -kzi[k];
-          const cd *src = fld[c] + (size_t)kp * my;
-          cd *dst = fld[c] + (size_t)k * my;
-          for (int j = 0; j < my; j++) dst[j] = std::conj(src[j]);
-        }
+    }
+    for (int bi = 0; bi < nb; bi++) {
+      const int m = band[bi];
+      if (m / mz != 0 || kzi[m % mz] >= 0) continue;
+      const int src_slot = slot[-kzi[m % mz]];  // kx = 0, kz > 0 partner (same |k|, in the band)
+      for (int c = 0; c < 3; c++) {
+        const cd *src = fld[c] + (size_t)src_slot * my;
+        cd *dst = fld[c] + (size_t)bi * my;
+        for (int j = 0; j < my; j++) dst[j] = std::conj(src[j]);
+      }
+    }
     // 2) solenoidal: curl (initloma3/src/main.f:231-256)
-    std::vector<cd> cu(ns), cv(ns), cw(ns), t1(my), t2(my);
-    for (int m = 0; m < g.nmode; m++) {
-      const int i = m / mz, k = m % mz;
+    std::vector<cd> cu(nbs), cv(nbs), cw(nbs);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; bi++) {
+      std::vector<cd> t1(my), t2(my);
+      const int m = band[bi], i = m / mz, k = m % mz;
       const cd ikx(0.0, kxv[i]), ikz(0.0, kzv[k]);
-      const size_t b = (size_t)m * my;
+      const size_t b = (size_t)bi * my;
       cderiv1(o, &wf[b], t1.data());
       cderiv1(o, &uf[b], t2.data());
       for (int j = 0; j < my; j++) {
@@ -465,49 +484,50 @@ extern "C" int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_pa
         cw[b + j] = ikx * vf[b + j] - t2[j];
       }
     }
-    // 3) scale to rms amp at the mid plane (initloma3/src/main.f:291-356)
+    // 3) scale to rms amp at the mid plane (initloma3/src/main.f:291-356),
+    // summed over the band in mode order (the other modes add zeros)
     int jm = 0;
     for (int j = 1; j < my; j++)
       if (std::fabs(y[j]) < std::fabs(y[jm])) jm = j;
     double e = 0.0;
-    for (int m = 1; m < g.nmode; m++) {
-      const int i = m / mz;
-      e += (i == 0 ? 1.0 : 2.0) * std::norm(cu[(size_t)m * my + jm]);
+    for (int bi = 0; bi < nb; bi++) {
+      const int i = band[bi] / mz;
+      e += (i == 0 ? 1.0 : 2.0) * std::norm(cu[(size_t)bi * my + jm]);
     }
     const double fac = (e > 0.0) ? ic->amp / std::sqrt(e) : 0.0;
     // 4) mean profiles and rho u_i (initloma3/src/main.f:362-374, 572-600)
     std::vector<double> rho00(my);
     for (int j = 0; j < my; j++) rho00[j] = 1.0 + (ic->s - 1.0) / (ic->s + 1.0) * std::tanh(-y[j] / (2.0 * ic->dm0));
-    std::vector<cd> ru(ns), rv(ns), rw(ns);
-    for (int m = 0; m < g.nmode; m++)
-      for (int j = 0; j < my; j++) {
-        const size_t b = (size_t)m * my + j;
-        ru[b] = rho00[j] * fac * cu[b];
-        rv[b] = rho00[j] * fac * cv[b];
-        rw[b] = rho00[j] * fac * cw[b];
-      }
-    for (int j = 0; j < my; j++) { ru[j] = 0.0; rv[j] = 0.0; rw[j] = 0.0; }
-    // 5) psi, Omega_y, phi (initloma3/src/main.f:473-561)
+    // 5) psi, Omega_y, phi (initloma3/src/main.f:473-561); zero outside the band
     cd *VOR = reinterpret_cast<cd *>(vor), *PHI = reinterpret_cast<cd *>(phi);
     cd *PSI = reinterpret_cast<cd *>(psi), *SCA = reinterpret_cast<cd *>(scal);
-    std::vector<cd> dv(my), div(my), ps(my), dps(my), myv(my), d2(my);
-    for (int m = 0; m < g.nmode; m++) {
-      const int i = m / mz, k = m % mz;
+    std::fill(VOR, VOR + ns, cd(0.0));
+    std::fill(PHI, PHI + ns, cd(0.0));
+    std::fill(PSI, PSI + ns, cd(0.0));
+    std::fill(SCA, SCA + ns, cd(0.0));
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int bi = 0; bi < nb; bi++) {
+      std::vector<cd> ru(my), rv(my), rw(my), dv(my), div(my), ps(my), dps(my), myv(my), d2(my);
+      const int m = band[bi], i = m / mz, k = m % mz;
       const cd ikx(0.0, kxv[i]), ikz(0.0, kzv[k]);
       const double k2 = kxv[i] * kxv[i] + kzv[k] * kzv[k];
-      const size_t b = (size_t)m * my;
-      cderiv1(o, &rv[b], dv.data());
-      for (int j = 0; j < my; j++) div[j] = ikx * ru[b + j] + ikz * rw[b + j] + dv[j];
+      const size_t bb = (size_t)bi * my, b = (size_t)m * my;
+      for (int j = 0; j < my; j++) {
+        ru[j] = rho00[j] * fac * cu[bb + j];
+        rv[j] = rho00[j] * fac * cv[bb + j];
+        rw[j] = rho00[j] * fac * cw[bb + j];
+      }
+      cderiv1(o, rv.data(), dv.data());
+      for (int j = 0; j < my; j++) div[j] = ikx * ru[j] + ikz * rw[j] + dv[j];
       if (k2 == 0.0) std::fill(ps.begin(), ps.end(), cd(0.0));
       else cpoisson(o, k2, div.data(), ps.data());
       cderiv1(o, ps.data(), dps.data());
-      for (int j = 0; j < my; j++) myv[j] = rv[b + j] - dps[j];
+      for (int j = 0; j < my; j++) myv[j] = rv[j] - dps[j];
       cderiv2(o, myv.data(), d2.data());
       for (int j = 0; j < my; j++) {
         PSI[b + j] = ps[j];
-        VOR[b + j] = -ikx * rw[b + j] + ikz * ru[b + j];
+        VOR[b + j] = -ikx * rw[j] + ikz * ru[j];
         PHI[b + j] = -k2 * myv[j] + d2[j];
-        SCA[b + j] = 0.0;
       }
     }
     for (int j = 0; j < my; j++) {

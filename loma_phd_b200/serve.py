@@ -77,6 +77,7 @@ class _Active:
     remaining: int
     bytes: int
     inflight: int = 0
+    started: float = 0.0   # set-up done, first steps enqueued
 
 
 def _prepare(req: RunRequest, device: int) -> Lomacte:
@@ -97,7 +98,7 @@ class Server:
     """
 
     def __init__(self, hbm_cap: int, max_active: int = 16, chunk: int = 8, device: int = 0,
-                 keep_state: bool = False, prep_workers: int = 2):
+                 keep_state: bool = False, prep_workers: int = 4):
         self.cap = int(hbm_cap)
         self.max_active = max_active
         self.chunk = max(1, chunk)
@@ -120,6 +121,7 @@ class Server:
         used = 0
         peak_used = 0
         max_conc = 0
+        setup: List[float] = []
         pool = ThreadPoolExecutor(max_workers=self.prep_workers)
         t0 = clock()
         try:
@@ -143,7 +145,8 @@ class Server:
                     if fut.done():
                         case = fut.result()
                         del preparing[rid]
-                        a = _Active(r, case, t_adm, r.steps, fp)
+                        a = _Active(r, case, t_adm, r.steps, fp, started=clock() - t0)
+                        setup.append(a.started - t_adm)
                         active[rid] = a
                         self._enqueue(a)
                         progressed = True
@@ -183,6 +186,7 @@ class Server:
             "aggregate_mpts_steps_per_s": work / makespan if makespan > 0 else None,
             "peak_device_bytes": peak_used,
             "max_concurrent": max_conc,
+            "mean_setup_s": float(np.mean(setup)) if setup else None,
         }
         return {"results": sorted(results, key=lambda r: r.rid), "stats": stats}
 
@@ -215,4 +219,21 @@ def synthetic_stream(n: int, seed: int = 0, rate: float = 2.0, steps_range=(200,
         out.append(RunRequest(rid=i, nx=nx, nz=nx, ny=ny, steps=steps, Re=float(rng.uniform(100, 1000)),
                               s=float(rng.uniform(1.0, 8.0)), amp=float(rng.uniform(5e-3, 2e-2)),
                               seed=int(rng.integers(0, 2**31 - 1)), precision=precision, arrival=t))
+    return out
+
+
+def ensemble_requests(n: int = 48, steps: int = 500, precision: int = 1, seed: int = 0) -> List[RunRequest]:
+    """An ensemble of n independent cases, all present at t = 0, seeds 0 ..
+    n-1: grids drawn uniformly from nx in {64, 96, 128, 192}, ny in {97,
+    129, 193}, nz in {64, 96, 128}; Re ~ U[100, 400], s ~ U[1, 8],
+    amplitude ~ U[5e-3, 2e-2]; the same number of steps each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nx = int(rng.choice((64, 96, 128, 192)))
+        ny = int(rng.choice((97, 129, 193)))
+        nz = int(rng.choice((64, 96, 128)))
+        out.append(RunRequest(rid=i, nx=nx, nz=nz, ny=ny, steps=steps, Re=float(rng.uniform(100, 400)),
+                              s=float(rng.uniform(1.0, 8.0)), amp=float(rng.uniform(5e-3, 2e-2)), seed=i,
+                              precision=precision, arrival=0.0))
     return out

@@ -13,8 +13,16 @@ import numpy as np
 import pytest
 
 from loma_phd_b200 import Lomacte, footprint
-from loma_phd_b200.serve import RunRequest, Server, synthetic_stream
+from loma_phd_b200.serve import RunRequest, Server, ensemble_requests, synthetic_stream
 from tests.helpers import FIELDS, case, rel_l2
+
+
+def test_ensemble_requests():
+    e = ensemble_requests(48, 500, precision=0)
+    assert [r.seed for r in e] == list(range(48)) and all(r.arrival == 0.0 and r.steps == 500 for r in e)
+    assert all(r.nx in (64, 96, 128, 192) and r.ny in (97, 129, 193) and r.nz in (64, 96, 128) for r in e)
+    assert len({(r.nx, r.ny, r.nz) for r in e}) > 10  # uneven grids
+    assert all(footprint(r.params()) > 0 for r in e)
 
 
 def test_stream_generator_and_footprint():
