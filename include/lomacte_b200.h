@@ -48,7 +48,11 @@ typedef struct lmc_params {
                            1: mixed: FP32 work buffers and FP32 FFTs; FP64
                               state, RK3 accumulators, y solves, 00 modes
                               and pointwise EOS / d(rho)/dt math
-                           2: as 1 with FP64 FFT arithmetic (FP32 storage) */
+                           2: as 1 with FP64 FFT arithmetic (FP32 storage)
+                           With precision 1, LMC_FFT64=<mask> in the
+                           environment at lmc_create gives chosen stages FP64
+                           butterflies (1 inverse z, 2 x stage, 4 direct z),
+                           for attributing the mixed form's error. */
   int device;           /* CUDA device ordinal */
   int variant;          /* 0: trunk/lomacte3 (2017); 1: the 2014 code
                            trunk/lomacte (spectral T, d(rho) by a transform

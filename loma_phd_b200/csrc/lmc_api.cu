@@ -240,6 +240,10 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   lmc::Dev &d = h->d;
   std::memset(&d, 0, sizeof(d));
   d.prec = p->precision;
+  if (d.prec == 1) {
+    const char *e = std::getenv("LMC_FFT64");
+    d.fft64 = e ? (std::atoi(e) & 7) : 0;
+  }
   const lmc::Grid &g = h->g;
   int rc = LMC_OK;
   if (g.nkx < 1 || g.mz < 1 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) rc = LMC_EINVAL;

@@ -734,16 +734,26 @@ inline cudaError_t upload_twiddles() {
     case 2: Launch<N1, N2, double2, float2>::CALL; break;             \
     default: Launch<N1, N2, double2, double2>::CALL; break;           \
   }
+// precision 1 with bit BIT of d.fft64 set: FP64 butterflies for this stage
+#define LMC_FFT_FORMS_M(N1, N2, BIT, CALL)                                \
+  switch (d.prec) {                                                       \
+    case 1:                                                               \
+      if (d.fft64 & (BIT)) Launch<N1, N2, double2, float2>::CALL;         \
+      else Launch<N1, N2, float2, float2>::CALL;                          \
+      break;                                                              \
+    case 2: Launch<N1, N2, double2, float2>::CALL; break;                 \
+    default: Launch<N1, N2, double2, double2>::CALL; break;               \
+  }
 #define LMC_FFT_CASE_Z(N, N1, N2, WHAT) \
-  case N: LMC_FFT_FORMS(N1, N2, WHAT(d, mode, s)) return true;
+  case N: LMC_FFT_FORMS_M(N1, N2, 4, WHAT(d, mode, s)) return true;
 #define LMC_FFT_CASE_XD(N, N1, N2) \
   case N: Launch<N1, N2, double2, double2>::xdrho(d, s); return true;
 #define LMC_FFT_CASE_X(N, N1, N2) \
-  case N: LMC_FFT_FORMS(N1, N2, xphys(d, rk, do_cfl, do_diag, s)) return true;
+  case N: LMC_FFT_FORMS_M(N1, N2, 2, xphys(d, rk, do_cfl, do_diag, s)) return true;
 #define LMC_FFT_CASE_XST(N, N1, N2) \
   case N: LMC_FFT_FORMS(N1, N2, xstats(d, st, s)) return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) \
-  case N: LMC_FFT_FORMS(N1, N2, zinv(d, mode, f0, nf, s)) return true;
+  case N: LMC_FFT_FORMS_M(N1, N2, 1, zinv(d, mode, f0, nf, s)) return true;
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
 #define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3);

@@ -15,6 +15,8 @@ namespace lmc {
 struct Dev {
   int prec;  // 0: FP64; 1: mixed (FP32 work buffers and transforms);
              // 2: mixed with FP64 transform arithmetic (FP32 work buffers)
+  int fft64;  // precision 1: FP64 butterflies for the stages set here
+              // (1 inverse z, 2 x stage, 4 direct z)
   int my, mgalx, mgalz, nkx, mz, nz1, nmode;
   int lpm, base, extra, C;  // y-chunking of a pencil over the lanes of a warp
   int ldy;                  // staging stride of a pencil (odd, >= my)

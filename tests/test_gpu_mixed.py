@@ -80,3 +80,18 @@ def test_mixed_thousand_steps_vs_fp64(gpu, prec, grid):
     b = np.array([h["dm"] for h in h64])
     assert np.abs(a - b).max() <= DM_TOL * np.abs(b).max(), (a, b)
     assert np.isfinite(dm["dm"]) and dm["time"] == pytest.approx(d64["time"])
+
+
+def test_fft64_stage_mask(gpu, monkeypatch):
+    """LMC_FFT64 gives chosen transform stages of the mixed form FP64
+    butterflies: with the x stage and the direct z transforms in FP64 the
+    result is closer to the FP64 path than the plain mixed form."""
+    p, y, st = case(64, 64, 129, precision=1)
+    p64, _, _ = case(64, 64, 129)
+    s64, _, _ = _run(p64, y, st, 20)
+    errs = {}
+    for mask in ("0", "6"):
+        monkeypatch.setenv("LMC_FFT64", mask)
+        sm, _, _ = _run(p, y, st, 20)
+        errs[mask] = rel_l2(sm["phi"], s64["phi"])
+    assert errs["6"] < 0.5 * errs["0"], errs
