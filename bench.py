@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from loma_phd_b200.replicas import case_seed, job_throughput, max_over_ranks  # noqa: E402
+
 # Algorithmic HBM bytes per launch, in units of the spectral (S = nplanes *
 # mz * ny complex), z-padded (Z = nplanes * mgalz * ny complex) and physical
 # (P = mgalx * mgalz * ny real) counts.  State fields (Omega_y, phi, psi, T,
@@ -238,7 +240,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
 
     p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec)
     y = stretched_mesh(p.my)
-    st = make_ic(p, y, ICParams(s=4.0, seed=rank))
+    st = make_ic(p, y, ICParams(s=4.0, seed=case_seed(rank)))
     g = Lomacte(p, y)
     g.load_state(st)
     g_launches = g.launches_per_step
@@ -266,12 +268,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     barrier()
     prof = g.profile_read()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = mpts(a) * a.steps * world / (ms / 1e3)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
+    value = job_throughput(mpts(a), a.steps, world, ms / 1e3)
     diag = g.diag()
     if not np.isfinite(diag["dm"]):
         raise RuntimeError("non-finite diagnostics after the timed steps")
@@ -300,11 +298,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
             g.load_state_ptrs(*ptrs)
             g.step(1)
             g.get_state_ptrs(*ptrs)
-        el = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([el], device=f"cuda:{dev}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{dev}")
         nbytes = 4 * S * 16 + 3 * p.my * 8
         e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
