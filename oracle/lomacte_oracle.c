@@ -444,8 +444,16 @@ struct lmo {
   fftplan px, pz;
   /* work buffers: spectral [kx][kz][y] (size nmode*my) */
   cplx *w_mx, *w_my, *w_mz, *w_nx, *w_ny, *w_nz, *w_t12, *w_t13, *w_t23, *w_drho, *w_chwk, *w_chwk2;
-  /* line buffers [line][kx] complex, line = z + mgalz*y */
-  cplx *ln[11];
+  /* line buffers [line][kx] complex, line = z + mgalz*y: 8 inputs and 11
+   * outputs of the transforms, 12 and 12 with the passive scalar */
+  cplx *ln[12];
+  /* passive scalar Z (the extension restated in lomacte_oracle.h): state,
+   * spectral work (lap Z, dZ/dx, dZ/dy, dZ/dz, Delta Z), physical RHS(Z) of
+   * the previous substep, wall values of its 00 mode, Re*Sc */
+  int scalar;
+  double pez, zbot, ztop;
+  cplx *zsc, *w_zlap, *w_zx, *w_zy, *w_zz, *w_dz;
+  double *rhsz;
   /* statistics (cross.f:578-585, 794-812, 1583-1607; escru.f:276-580):
    * st[LMO_NSTAT][my] raw accumulators in the order of the .sta record,
    * sp[nkx][12][nsp][nz1+1] spectra, uner[9] energies of the last
@@ -520,7 +528,7 @@ lmo *lmo_create(int mgalx, int mgalz, int my, const double *y, double Re,
                    &o->w_t12, &o->w_t13, &o->w_t23, &o->w_drho, &o->w_chwk, &o->w_chwk2, &o->rts};
   for (size_t b = 0; b < sizeof(bufs) / sizeof(bufs[0]); b++) *bufs[b] = xcalloc(ns, sizeof(cplx));
   size_t nl = (size_t)mgalz * my;
-  for (int f = 0; f < 11; f++) o->ln[f] = xcalloc(nl * o->nkx, sizeof(cplx));
+  for (int f = 0; f < 12; f++) o->ln[f] = xcalloc(nl * o->nkx, sizeof(cplx));
   o->rhst = xcalloc(nl * mgalx, 8);
   o->u00wk = xcalloc(my, 8); o->v00wk = xcalloc(my, 8); o->w00wk = xcalloc(my, 8);
   o->rf0u = xcalloc(my, 8); o->rf0w = xcalloc(my, 8); o->rf0v = xcalloc(my, 8);
@@ -538,8 +546,9 @@ void lmo_destroy(lmo *o) {
                o->w_nx, o->w_ny, o->w_nz, o->w_t12, o->w_t13, o->w_t23, o->w_drho, o->w_chwk, o->w_chwk2,
                o->rts};
   for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
-  for (int f = 0; f < 11; f++) free(o->ln[f]);
+  for (int f = 0; f < 12; f++) free(o->ln[f]);
   free(o->jsp); free(o->st); free(o->sp);
+  free(o->zsc); free(o->w_zlap); free(o->w_zx); free(o->w_zy); free(o->w_zz); free(o->w_dz); free(o->rhsz);
   plan_free(&o->px); plan_free(&o->pz);
   free(o);
 }
@@ -555,6 +564,7 @@ int lmo_set_state(lmo *o, const double *vor, const double *phi, const double *ps
   memset(o->ten12p, 0, ns * sizeof(cplx)); memset(o->ten13p, 0, ns * sizeof(cplx));
   memset(o->rts, 0, ns * sizeof(cplx));
   memset(o->rhst, 0, (size_t)o->mgalz * o->my * o->mgalx * 8);
+  if (o->rhsz) memset(o->rhsz, 0, (size_t)o->mgalz * o->my * o->mgalx * 8);
   /* cross.f:276-280 (first step copies the 00 modes to the work vectors) */
   memcpy(o->u00wk, u00, o->my * 8); memcpy(o->v00wk, v00, o->my * 8); memcpy(o->w00wk, w00, o->my * 8);
   memset(o->rf0u, 0, o->my * 8); memset(o->rf0w, 0, o->my * 8); memset(o->rf0v, 0, o->my * 8);
@@ -840,24 +850,22 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
   double ab = o->alpha[rk] / o->beta[rk];
 #pragma omp parallel num_threads(o->nthreads)
   {
-    double *ph = malloc(sizeof(double) * mgalx * 8), *out = malloc(sizeof(double) * mgalx * 12);
+    double *ph = malloc(sizeof(double) * mgalx * 12), *out = malloc(sizeof(double) * mgalx * 12);
     cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
     cplx *spec = malloc(sizeof(cplx) * nkx * 12);
 #pragma omp for schedule(static)
     for (long L = 0; L < (long)nlines; L++) {
       int jj = (int)(L / mgalz); /* y index (cross.f:1583) */
-      cplx *sp[8];
-      for (int f = 0; f < 8; f++) sp[f] = o->ln[f] + (size_t)L * nkx;
-      double *p[8];
-      for (int f = 0; f < 8; f++) p[f] = ph + (size_t)f * mgalx;
-      xinv2(o, sp[0], sp[1], p[0], p[1], buf, fo);
-      xinv2(o, sp[2], sp[3], p[2], p[3], buf, fo);
-      xinv2(o, sp[4], sp[5], p[4], p[5], buf, fo);
-      xinv2(o, sp[6], sp[7], p[6], p[7], buf, fo);
+      const int nin = o->scalar ? 12 : 8, nout = o->scalar ? 12 : 11;
+      cplx *sp[12];
+      for (int f = 0; f < nin; f++) sp[f] = o->ln[f] + (size_t)L * nkx;
+      double *p[12];
+      for (int f = 0; f < nin; f++) p[f] = ph + (size_t)f * mgalx;
+      for (int f = 0; f < nin; f += 2) xinv2(o, sp[f], sp[f + 1], p[f], p[f + 1], buf, fo);
       double *ru = p[0], *rv = p[1], *rw = p[2], *lapT = p[3], *tx = p[4], *ty = p[5], *tz = p[6], *T = p[7];
       double *rh = o->rhst + (size_t)L * mgalx;
-      double *q[11];
-      for (int f = 0; f < 11; f++) q[f] = out + (size_t)f * mgalx;
+      double *q[12];
+      for (int f = 0; f < nout; f++) q[f] = out + (size_t)f * mgalx;
       double lmx = 0, lmy = 0, lmz = 0, Tmax = 0, rsum = 0;
       for (int x = 0; x < mgalx; x++) {
         double u = ru[x] * T[x], v = rv[x] * T[x], w = rw[x] * T[x]; /* cross.f:1613-1622 */
@@ -868,6 +876,14 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         tnext = tnext + dtgamma * rhs; /* cross.f:1640-1643 */
         d8 = d8 + dtgamma * rhs;
         q[10][x] = d8;                     /* DT (cross.f:1645-1647) */
+        if (o->scalar) { /* the passive scalar, advanced as T is */
+          const double *zl = p[8], *zx = p[9], *zy = p[10], *zz = p[11];
+          double *rz = o->rhsz + (size_t)L * mgalx;
+          double dz = dtxi * rz[x];
+          double rzs = -u * zx[x] - v * zy[x] - w * zz[x] + T[x] * zl[x] / o->pez;
+          rz[x] = rzs;
+          q[11][x] = dz + dtgamma * rzs;
+        }
         q[0][x] = u; q[1][x] = v; q[2][x] = w;
         q[3][x] = ru[x] * u; q[4][x] = rv[x] * v; q[5][x] = rw[x] * w; /* cross.f:1655-1659 */
         q[6][x] = ru[x] * v; q[7][x] = ru[x] * w; q[8][x] = rv[x] * w; /* cross.f:1662-1666 */
@@ -898,7 +914,7 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         }
       }
       if (do_cfl) { /* cross.f:1690-1708 */
-        double DD = 1.0 / o->peclet * Tmax;
+        double DD = (o->scalar ? fmax(1.0 / o->peclet, 1.0 / o->pez) : 1.0 / o->peclet) * Tmax;
         double c0 = lmy / o->hy[jj];
         double cT = 2 * DD * ((hxalp / 2) * (hxalp / 2) + (hzbet / 2) * (hzbet / 2) + (1 / o->hy[jj]) * (1 / o->hy[jj]));
 #pragma omp critical
@@ -910,11 +926,12 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
 #pragma omp atomic
         rhom[jj] += rsum;
       }
-      cplx *so[11];
-      for (int f = 0; f < 11; f++) so[f] = spec + (size_t)f * nkx;
+      cplx *so[12];
+      for (int f = 0; f < nout; f++) so[f] = spec + (size_t)f * nkx;
       for (int f = 0; f < 10; f += 2) xfwd2(o, q[f], q[f + 1], so[f], so[f + 1], buf, fo);
-      xfwd2(o, q[10], NULL, so[10], NULL, buf, fo);
-      for (int f = 0; f < 11; f++) memcpy(o->ln[f] + (size_t)L * nkx, so[f], sizeof(cplx) * nkx);
+      if (o->scalar) xfwd2(o, q[10], q[11], so[10], so[11], buf, fo);  /* (DT, DZ) */
+      else xfwd2(o, q[10], NULL, so[10], NULL, buf, fo);
+      for (int f = 0; f < nout; f++) memcpy(o->ln[f] + (size_t)L * nkx, so[f], sizeof(cplx) * nkx);
     }
     free(ph); free(out); free(buf); free(fo); free(spec);
   }
@@ -932,13 +949,14 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
 
 /* foup2: cross.f:1282-1430 */
 static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, int do_cfl, int do_diag,
-                  cplx *in8[8], cplx *out11[11]) {
+                  cplx *in8[12], cplx *out11[12]) {
+  const int nin = o->scalar ? 12 : 8, nout = o->scalar ? 12 : 11;
   int nkx = o->nkx, mgalz = o->mgalz;
 #pragma omp parallel num_threads(o->nthreads)
   {
     cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
 #pragma omp for collapse(2) schedule(static)
-    for (int f = 0; f < 8; f++)
+    for (int f = 0; f < nin; f++)
       for (int i = 0; i < nkx; i++) zinv_plane(o, i, in8[f], o->ln[f], buf, out);
     free(buf); free(out);
   }
@@ -949,7 +967,7 @@ static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
   {
     cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
 #pragma omp for collapse(2) schedule(static)
-    for (int f = 0; f < 11; f++)
+    for (int f = 0; f < nout; f++)
       for (int i = 0; i < nkx; i++) zfwd_plane(o, i, o->ln[f], out11[f], buf, out);
     free(buf); free(out);
   }
@@ -1110,6 +1128,14 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
   }
   o->scal[0] = 1.0 / o->rhobot;
   o->scal[my - 1] = 1.0 / o->rhotop;
+  if (o->scalar) { /* Z: zero at the walls, its mean held at the wall values */
+    for (int m = 0; m < o->nmode; m++) {
+      cplx *zz = o->zsc + (size_t)m * my;
+      zz[0] = 0; zz[my - 1] = 0;
+    }
+    o->zsc[0] = o->zbot;
+    o->zsc[my - 1] = o->ztop;
+  }
 
   cplx *mxw = o->w_mx, *myw = o->w_my, *mzw = o->w_mz, *nxw = o->w_nx, *nyw = o->w_ny, *nzw = o->w_nz;
   cplx *t12 = o->w_t12, *t13 = o->w_t13, *t23 = o->w_t23, *drho = o->w_drho, *chwk = o->w_chwk, *chwk2 = o->w_chwk2;
@@ -1156,6 +1182,16 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
         t23[b + j] = I * kz * drho[b + j];
         t12[b + j] = I * kx * drho[b + j];
       }
+      if (o->scalar) { /* the same derivatives of Z */
+        const cplx *z = o->zsc + b;
+        deryr2_c(o, z, o->w_zy + b, w1, w2, tt1, tt2);
+        deryyr2_c(o, z, o->w_zlap + b, w1, w2, tt1, tt2);
+        for (int j = 0; j < my; j++) {
+          o->w_zlap[b + j] = o->w_zlap[b + j] - rK * z[j];
+          o->w_zx[b + j] = I * kx * z[j];
+          o->w_zz[b + j] = I * kz * z[j];
+        }
+      }
     }
     free(s);
   }
@@ -1173,8 +1209,8 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
   if (do_st) addstats1(o, mxw, myw, mzw, drho); /* cross.f:578-585 */
   /* (5) foup2 */
   int do_cfl = (r == 0 && o->icfl == 1 && o->dtmode == 0);
-  cplx *in8[8] = {mxw, myw, mzw, nyw, t12, t13, t23, drho};
-  cplx *out11[11] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, drho, chwk2};
+  cplx *in8[12] = {mxw, myw, mzw, nyw, t12, t13, t23, drho, o->w_zlap, o->w_zx, o->w_zy, o->w_zz};
+  cplx *out11[12] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, drho, chwk2, o->w_dz};
   foup2(o, r, dtxi, dtgamma, dtbeta, do_cfl, ihist && r == 0, in8, out11);
   if (do_st) { /* cross.f:796-812 (u, v, w are not changed in between) */
     o->nacum++;
@@ -1193,6 +1229,8 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
       size_t b = (size_t)m * my;
       /* (6a) T update: cross.f:619-627 */
       for (int j = 0; j < my; j++) o->scal[b + j] = o->scal[b + j] + chwk2[b + j];
+      if (o->scalar)
+        for (int j = 0; j < my; j++) o->zsc[b + j] = o->zsc[b + j] + o->w_dz[b + j];
       /* (6b) Nx, Ny, Nz: cross.f:652-682 */
       deryr2_c(o, nyw + b, nyw + b, w1, w2, tt1, tt2);
       for (int j = 0; j < my; j++) nyw[b + j] = -I * kx * t12[b + j] - nyw[b + j] - I * kz * t23[b + j];
@@ -1673,6 +1711,35 @@ int lmo_step(lmo *o, int nsteps) {
 int lmo_set_variant(lmo *o, int variant) {
   if (!o || variant < 0 || variant > 1) return -1;
   o->variant = variant;
+  return 0;
+}
+
+int lmo_set_scalar(lmo *o, int on, double schmidt) {
+  if (!o || o->variant || (on && !(schmidt > 0))) return -1;
+  size_t ns = (size_t)o->nmode * o->my, np = (size_t)o->mgalz * o->my * o->mgalx;
+  o->scalar = on != 0;
+  if (!on) return 0;
+  o->pez = o->Re * schmidt;
+  cplx **b[] = {&o->zsc, &o->w_zlap, &o->w_zx, &o->w_zy, &o->w_zz, &o->w_dz};
+  for (size_t i = 0; i < sizeof(b) / sizeof(b[0]); i++)
+    if (!*b[i]) *b[i] = xcalloc(ns, sizeof(cplx));
+  if (!o->rhsz) o->rhsz = xcalloc(np, 8);
+  return 0;
+}
+
+int lmo_set_scalar_state(lmo *o, const double *z) {
+  if (!o || !o->scalar || !z) return -1;
+  size_t ns = (size_t)o->nmode * o->my;
+  memcpy(o->zsc, z, ns * sizeof(cplx));
+  memset(o->rhsz, 0, (size_t)o->mgalz * o->my * o->mgalx * 8);
+  o->zbot = creal(o->zsc[SIDX(o, 0, 0, 0)]);
+  o->ztop = creal(o->zsc[SIDX(o, 0, 0, o->my - 1)]);
+  return 0;
+}
+
+int lmo_get_scalar_state(const lmo *o, double *z) {
+  if (!o || !o->scalar || !z) return -1;
+  memcpy(z, o->zsc, (size_t)o->nmode * o->my * sizeof(cplx));
   return 0;
 }
 

@@ -81,6 +81,19 @@ int lmo_stats_reset(lmo *o, int nsp, const int *jsp, double sigma);
 int lmo_stats_step(lmo *o, int nsteps);
 int lmo_stats_read(lmo *o, double *prof, double *spec, double *uner, int *counts, int clear_spectra);
 
+/* Passive scalar Z (an extension: no lomacte code carries one).  Z is
+ * advanced exactly as the lomacte3 substep advances T (cross.f:336-349,
+ * 521-554, 619-627, 1625-1647): zero at the walls except its mean, held at
+ * the wall values it was loaded with; its derivatives go through the same
+ * transforms; in physical space RHS(Z) = -u.grad Z + T lap Z / (Re Sc) with
+ * the FP64 RK3 accumulator; the increment Delta Z is transformed back and
+ * added to the spectral Z.  The diffusive CFL limit takes the larger of
+ * 1/Pe and 1/(Re Sc).  Not for the 2014 variant.  set_scalar allocates;
+ * set_scalar_state loads Z (reference layout) and clears its RK3 memory. */
+int lmo_set_scalar(lmo *o, int on, double schmidt);
+int lmo_set_scalar_state(lmo *o, const double *z);
+int lmo_get_scalar_state(const lmo *o, double *z);
+
 /* Coefficient access for tests (band storage row-major [row][band]). */
 void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12,
                    double *prem3_lu, double *dt21, double *dt22, double *fmap);

@@ -64,6 +64,9 @@ def lib():
                                       ctypes.c_double]
         L.lmo_stats_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.lmo_stats_read.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.lmo_set_scalar.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.lmo_set_scalar_state.argtypes = [ctypes.c_void_p, _dp]
+        L.lmo_get_scalar_state.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_cft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         L.lmo_rft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         _lib = L
@@ -132,6 +135,18 @@ class Oracle:
 
     def substep(self, r=0):
         lib().lmo_substep(self.h, r)
+
+    # passive scalar Z, advanced as T (lomacte_oracle.h)
+    def set_scalar(self, z, schmidt):
+        if lib().lmo_set_scalar(self.h, 1, float(schmidt)) != 0:
+            raise ValueError("lmo_set_scalar rejected its arguments")
+        a = np.ascontiguousarray(np.asarray(z, dtype=np.complex128).reshape(self.shape)).view(np.float64)
+        lib().lmo_set_scalar_state(self.h, _p(a.ravel()))
+
+    def get_scalar(self):
+        a = np.zeros(self.shape, dtype=np.complex128)
+        lib().lmo_get_scalar_state(self.h, _p(a.view(np.float64).ravel()))
+        return a
 
     # statistics: addstats1/2 and the phys2 sums (cross.f:578-585, 794-812,
     # 1583-1607), resetstats (escru.f:485-580)
