@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also run an ensemble of this many independent cases of uneven grids (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--scalar", action="store_true",
+                    help="carry the passive scalar Z (extension; e2e loads the flow state only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
@@ -238,11 +240,18 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     from loma_phd_b200 import ICParams, Lomacte, Params, make_ic, stretched_mesh
     from loma_phd_b200.lomacte import KERNEL_NAMES
 
-    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec)
+    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec,
+                          scalar=1 if a.scalar else 0)
     y = stretched_mesh(p.my)
     st = make_ic(p, y, ICParams(s=4.0, seed=case_seed(rank)))
     g = Lomacte(p, y)
     g.load_state(st)
+    if a.scalar:  # Z = (T - T_bot)/(T_top - T_bot), Sc = Pr
+        T = st["scal"]
+        tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
+        z = T / (tt - tb)
+        z[0, 0, :] -= tb / (tt - tb)
+        g.load_scalar(z)
     g_launches = g.launches_per_step
     y_family = g.y_family
     stream = torch.cuda.ExternalStream(g.stream, device=dev)
@@ -443,7 +452,8 @@ def main():
             "dtype": "mixed f32/f64" if mixed else "f64",
             "precision_form": a.mixed_form if mixed else 0,
             "data": "synthetic (seeded initial condition)",
-            "config": {"workload": f"lomacte {MIXED_NAMES[a.mixed_form] if mixed else 'FP64 plain path'} "
+            "config": {"workload": f"lomacte {MIXED_NAMES[a.mixed_form] if mixed else 'FP64 plain path'}"
+                                   f"{' + passive scalar' if a.scalar else ''} "
                                    f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
                        "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},

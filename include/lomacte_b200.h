@@ -57,6 +57,10 @@ typedef struct lmc_params {
   int variant;          /* 0: trunk/lomacte3 (2017); 1: the 2014 code
                            trunk/lomacte (spectral T, d(rho) by a transform
                            round trip, Dirichlet psi; FP64 only) */
+  int scalar;           /* 1: carry a passive scalar Z (an extension with no
+                           counterpart in the lomacte codes, see
+                           lmc_load_scalar_f64); not with variant 1 */
+  double schmidt;       /* Schmidt number Sc of Z; <= 0: Sc = Pr = 0.7f */
 } lmc_params;
 
 /* Per-step diagnostics (the .cf record of cross.f:1172-1176 without the
@@ -103,6 +107,19 @@ int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi,
 int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi,
                       float *scal, double *u00, double *v00, double *w00,
                       double *time);
+
+/* Passive scalar Z (lmc_params.scalar = 1).  No lomacte code carries a
+ * scalar; Z is advanced exactly as the lomacte3 substep advances T
+ * (cross.f:336-349, 521-554, 619-627, 1625-1647): zero at the walls except
+ * its 00 mode, held at the wall values it was loaded with; dZ/dy and lap Z
+ * by the compact schemes; in physical space RHS(Z) = -u.grad Z +
+ * T lap Z / (Re Sc) with its own FP64 RK3 accumulator; Delta Z transformed
+ * back and added to the spectral Z.  The diffusive CFL limit takes the
+ * larger of 1/Pe and 1/(Re Sc).  Load Z after lmc_load_state_*: the layout
+ * is that of the other fields (reference layout, complex*16); loading
+ * clears Z's RK3 memory.  LMC_EINVAL without the scalar. */
+int lmc_load_scalar_f64(lmc_handle *h, const double *z);
+int lmc_get_scalar_f64(lmc_handle *h, double *z);
 
 /* Advance nsteps full RK3 steps (the body of cross.f:225-1226, 3
  * substeps of cross.f:307-1141 each).  Asynchronous on the handle's

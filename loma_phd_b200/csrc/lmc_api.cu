@@ -194,8 +194,9 @@ int do_load(lmc_handle *h, const double *vor, const double *phi, const double *p
   // Densities at the walls from the 00 mode of T (cross.f:211-213).
   const double tb = scal[0], tt = scal[2 * (size_t)(d.my - 1)];
   if (!(tb > 0.0) || !(tt > 0.0)) return LMC_EINVAL;
-  double sc[8] = {h->p.dt, h->p.dt, time, 1.0 / tb, 1.0 / tt, 0, 0, 0};
+  double sc[5] = {h->p.dt, h->p.dt, time, 1.0 / tb, 1.0 / tt};  // [5], [6]: the scalar's wall values
   LMC_CK(cudaMemcpyAsync(d.scal_d, sc, sizeof(sc), cudaMemcpyHostToDevice, h->s));
+  if (d.scalar) LMC_CK(cudaMemsetAsync(d.rhsz, 0, (size_t)d.my * d.mgalz * d.mgalx * sizeof(double), h->s));
   LMC_CK(cudaMemsetAsync(d.diag, 0, 16 * sizeof(double), h->s));
   LMC_CK(cudaMemsetAsync(d.status, 0, sizeof(int), h->s));
   LMC_CK(cudaStreamSynchronize(h->s));
@@ -233,6 +234,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   if (p->device < 0 || p->device >= ndev) return LMC_EINVAL;
   if (p->precision < 0 || p->precision > 2) return LMC_EINVAL;
   if (p->variant < 0 || p->variant > 1 || (p->variant == 1 && p->precision != 0)) return LMC_EINVAL;
+  if (p->scalar < 0 || p->scalar > 1 || (p->scalar && p->variant)) return LMC_EINVAL;
   lmc_handle *h = new (std::nothrow) lmc_handle();
   if (!h) return LMC_ENOMEM;
   h->p = *p;
@@ -273,6 +275,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   d.ldy = g.my | 1;
   d.ire = 1.0 / p->Re;
   d.variant = p->variant;
+  d.scalar = p->scalar;
+  // Re*Sc; Sc <= 0 takes Sc = Pr, the Schmidt number of the reference's Pe = Re*0.7f
+  d.pez = p->Re * (p->schmidt > 0 ? p->schmidt : (double)0.7f);
   // Pe = Re*0.7f (main.f:569); the 2014 code uses Pe = Re (lomacte/cross.f:1301)
   d.peclet = p->peclet > 0 ? p->peclet : (d.variant ? p->Re : p->Re * (double)0.7f);
   d.cfl = (double)(float)p->cfl;
@@ -285,7 +290,8 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   // y-operator tables go to the device chunk-major (see lmcd::tab)
   const int C = d.C, lpm = d.lpm, base = d.base, extra = d.extra, my = g.my;
   auto cm = [&](const std::vector<double> &T, int W) { return lmc::chunk_major(T, my, W, C, lpm, base, extra); };
-  d.tpm = d.variant ? 1 : mode_parallel(g.nmode);  // the 2014 variant runs the mode-parallel kernels
+  // the 2014 variant and the passive scalar run the mode-parallel kernels
+  d.tpm = (d.variant || p->scalar) ? 1 : mode_parallel(g.nmode);
   const size_t pm2 = (size_t)C * 2 * 32, pm3 = (size_t)C * 3 * 32;
   const size_t nm = d.tpm ? 0 : (size_t)g.nmode;  // chunk-major per-mode tables: warp kernels only
   std::vector<double> PLc(nm * pm2), PUc(nm * pm3), V12c(nm * pm2);
@@ -371,7 +377,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     if ((rc = dalloc(h, q, ns))) { lmc_destroy(h); return rc; }
   // work buffers: FP64 in the plain form; FP32 in the mixed form, which
   // keeps three FP64 spectral buffers for the ABI transposes and lmc_op_y
-  for (int f = 0; f < 11; f++) {
+  for (int f = 0; f < (p->scalar ? 12 : 11); f++) {
     if (!d.prec || (f >= 7 && f <= 9))
       if ((rc = dalloc(h, &d.sb[f], ns))) { lmc_destroy(h); return rc; }
     if (!d.prec) {
@@ -383,9 +389,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   if (d.prec) {
     // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
     d.mpart_ld = 4 * g.mgalz;
-    if ((rc = dalloc(h, &d.mi, (size_t)6 * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)11 * g.my)) ||
-        (rc = dalloc(h, &h->mo[1], (size_t)11 * g.my)) ||
-        (rc = dalloc(h, &d.mpart, (size_t)11 * g.my * d.mpart_ld))) {
+    if ((rc = dalloc(h, &d.mi, (size_t)8 * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
+        (rc = dalloc(h, &h->mo[1], (size_t)12 * g.my)) ||
+        (rc = dalloc(h, &d.mpart, (size_t)12 * g.my * d.mpart_ld))) {
       lmc_destroy(h);
       return rc;
     }
@@ -399,6 +405,11 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     return rc;
   }
   d.tsrc = d.variant ? d.Told : d.scal;
+  if (d.scalar &&
+      ((rc = dalloc(h, &d.zsc, ns)) || (rc = dalloc(h, &d.rhsz, (size_t)g.my * g.mgalz * g.mgalx)))) {
+    lmc_destroy(h);
+    return rc;
+  }
   double **vec[] = {&d.u00, &d.v00, &d.w00, &d.rf0u, &d.rf0w, &d.rf0v, &d.rhom};
   for (auto q : vec)
     if ((rc = dalloc(h, q, (size_t)g.my))) { lmc_destroy(h); return rc; }
@@ -485,6 +496,33 @@ int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi, doub
   return h->err;
 }
 
+int lmc_load_scalar_f64(lmc_handle *h, const double *z) {
+  if (!h || !z || !h->d.scalar) return LMC_EINVAL;
+  if (h->err) return h->err;
+  const lmc::Dev &d = h->d;
+  const size_t ns = (size_t)d.nmode * d.my * sizeof(double2);
+  LMC_CK(cudaSetDevice(h->p.device));
+  LMC_CK(cudaMemcpyAsync(d.sb[7], z, ns, cudaMemcpyHostToDevice, h->s));
+  lmc::launch_ref2dev(d, d.sb[7], d.zsc, h->s);
+  LMC_CK(cudaMemsetAsync(d.rhsz, 0, (size_t)d.my * d.mgalz * d.mgalx * sizeof(double), h->s));
+  // wall values of the 00 mode, held by the boundary condition
+  const double zw[2] = {z[0], z[2 * (size_t)(d.my - 1)]};
+  LMC_CK(cudaMemcpyAsync(d.scal_d + 5, zw, sizeof(zw), cudaMemcpyHostToDevice, h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return LMC_OK;
+}
+
+int lmc_get_scalar_f64(lmc_handle *h, double *z) {
+  if (!h || !z || !h->d.scalar) return LMC_EINVAL;
+  const lmc::Dev &d = h->d;
+  const size_t ns = (size_t)d.nmode * d.my * sizeof(double2);
+  LMC_CK(cudaSetDevice(h->p.device));
+  lmc::launch_dev2ref(d, d.zsc, d.sb[7], h->s);
+  LMC_CK(cudaMemcpyAsync(z, d.sb[7], ns, cudaMemcpyDeviceToHost, h->s));
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return h->err;
+}
+
 int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi, float *scal, double *u00, double *v00,
                       double *w00, double *time) {
   if (!h) return LMC_EINVAL;
@@ -544,7 +582,9 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
     if (side_t) {
       if (!fork()) return LMC_ECUDA;
       run(2, s2, [&] { lmc::launch_tder(d, s2); });
+      if (d.scalar) run(2, s2, [&] { lmc::launch_zder(d, s2); });
       run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 3, 5); });
+      if (d.scalar) run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 8, 4); });
       if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
     }
     run(0, s, [&] { lmc::launch_lapv(d, s); });
@@ -574,6 +614,7 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
     if (st_now) run(10, s, [&] { lmc::launch_stats2(d, h->st, s); });
     if (side_psi) {  // beside post1 and post2, which neither read nor write its data
       if (!fork()) return LMC_ECUDA;
+      if (d.scalar) run(5, s2, [&] { lmc::launch_zupd(d, s2); });  // Z += Delta Z
       run(8, s2, [&] { lmc::launch_psi_main(d, rk, s2); });
     }
     run(6, s, [&] { lmc::launch_post1(d, rk, do_cfl, 1, s); });
@@ -791,7 +832,9 @@ int lmc_launches_per_step(lmc_handle *h) {
   // the 2014 variant: 14 kernels per substep (three for the d(rho) round
   // trip, its own 00 tail) and the Deltat kernel in the first substep
   if (h->d.variant) return 3 * 14 + 1;
-  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0) + 1;  // + the split inverse z transform
+  // the split inverse z transform adds one; the passive scalar three (its
+  // derivatives, its inverse z transforms, its update)
+  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0) + 1 + (h->d.scalar ? 3 : 0);
   return 3 * per;
 }
 
@@ -808,10 +851,14 @@ size_t lmc_footprint(const lmc_params *p) {
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)
   if (p->variant) b += 3 * S * 16;  // T before the substep, Delta T, RHS(T)
-  if (p->variant || mode_parallel(g.nmode))
+  if (p->variant || p->scalar || mode_parallel(g.nmode))
     b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 5 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
   else
     b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8 + (size_t)g.my * 15 * 8;  // Poisson, d/dy rows
+  if (p->scalar) {  // Z, RHS(Z), one more spectral and z-physical work buffer
+    b += S * 16 + P * 8 + (p->precision == 0 ? S * 16 + Z * 16 : S * 8 + Z * 8);
+    b += 2 * (size_t)g.my * 8 + (size_t)g.my * 8 * 4 * g.mgalz;  // mixed sums of the 12th output
+  }
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
   else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;
   b += (size_t)C * 32 * 64 * 8 + 6 * 5 * 32 * 16 * 8 + (size_t)(g.mgalx + g.mgalz) * 24;  // y tables, twiddles

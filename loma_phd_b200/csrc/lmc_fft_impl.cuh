@@ -96,6 +96,12 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
       case 2: return wsb<ST>(d, SB_RW);
       case 3: return wsb<ST>(d, SB_LAPT);
       case 5: return wsb<ST>(d, SB_DTDY);
+      case 8: return wsb<ST>(d, SB_LAPZ);   // passive scalar: lap Z,
+      case 10: return wsb<ST>(d, SB_DZDY);  // dZ/dy,
+      case 9:
+      case 11:                              // and Z for dZ/dx, dZ/dz
+        if constexpr (sizeof(ST) == sizeof(double2)) return d.zsc;
+        else return wsb<ST>(d, SB_Z32);
       default:
         if constexpr (sizeof(ST) == sizeof(double2)) return d.tsrc;
         else return wsb<ST>(d, SB_T32);
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
     const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
     const int lead = lead_of(t);
-    const int mult = mode ? 0 : (f == 4) ? 1 : (f == 6) ? 2 : 0;  // i kx T, i kz T
+    const int mult = mode ? 0 : (f == 4 || f == 9) ? 1 : (f == 6 || f == 11) ? 2 : 0;  // i kx, i kz of T, Z
     for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
       const int il = idx / gap, g = idx - il * gap;
       W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
@@ -229,8 +235,10 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 // Persistent: each block walks tiles (y, z block of ZB lines).  The next
 // tile's eight input rows (each ZB*nkx contiguous complex values in the
 // [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
-// current tile is transformed.
-template <int N1, int N2, typename CT, typename ST>
+// current tile is transformed.  ZS: the passive scalar's four more input
+// rows (lap Z, dZ/dx, dZ/dy, dZ/dz), its RHS(Z) row and Delta Z as a
+// twelfth output, packed beside Delta T.
+template <int N1, int N2, typename CT, typename ST, bool ZS>
 // FP32 butterflies: at most about 128 registers, so that eight 64-thread
 // blocks (or the same thread count in larger blocks) share an SM
 __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) ? 512 / Geo<N1, N2>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
@@ -238,25 +246,28 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
+  constexpr int NI = ZS ? 12 : 8, NL = NI / 2, NO = ZS ? 12 : 11, NM = ZS ? 8 : 6;
   static_assert(G::XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nkx = d.nkx;  // a multiple of 8 for every supported length
-  CT *W = (CT *)smraw;                                       // 4 buffers x ZB lines x LD
-  ST *St = (ST *)(smraw + round16(sizeof(CT) * 4 * ZB * LD));  // 8 rows of ZB*nkx inputs
-  double *Sr = (double *)(St + 8 * ZB * nkx);  // ZB*N RHS(T)
+  CT *W = (CT *)smraw;                                        // NL buffers x ZB lines x LD
+  ST *St = (ST *)(smraw + round16(sizeof(CT) * NL * ZB * LD));  // NI rows of ZB*nkx inputs
+  double *Sr = (double *)(St + NI * ZB * nkx);  // ZB*N RHS(T)
+  double *Srz = Sr + ZB * N;                    // ZB*N RHS(Z) (ZS)
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
   __shared__ unsigned long long s_tmax[ZB], s_vmax;
   __shared__ double s_red[3][8];
-  __shared__ double s_min[6], s_est[11];  // mixed form, per tile
+  __shared__ double s_min[NM], s_est[NO];  // mixed form, per tile
   const int nzk = (d.mgalz + ZB - 1) / ZB;
   auto issue = [&](int t) {
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
     const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = d.variant ? 0u : (uint32_t)nzb * N * sizeof(double);
-    mbar_expect_tx(&bar, 8 * rb + hb);
+    mbar_expect_tx(&bar, NI * rb + (ZS ? 2 : 1) * hb);
     const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
-    for (int f = 0; f < 8; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
+    for (int f = 0; f < NI; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
     if (hb) bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
+    if (ZS && hb) bulk_g2s(Srz, d.rhsz + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
   };
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -280,8 +291,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
     if constexpr (sizeof(ST) == sizeof(float2)) {  // mixed form: see s_min / s_est below
       const int q = threadIdx.x;
-      if (q < 6) s_min[q] = d.mi[(size_t)q * d.my + y];
-      if (q < 11) {
+      if (q < NM) s_min[q] = d.mi[(size_t)q * d.my + y];
+      if (q < NO) {
         double e;
         if (d.mean_ok) {
           e = d.mo_prev[(size_t)q * d.my + y] / ((double)d.mgalx * (double)d.mgalz);
@@ -305,11 +316,12 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         s_est[q] = e;
       }
     }
-    double rh[PT];
+    double rh[PT], rz[ZS ? PT : 1];
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
       rh[j] = (q < nzb * N && !d.variant) ? Sr[q] : 0.0;
+      if constexpr (ZS) rz[j] = (q < nzb * N) ? Srz[q] : 0.0;
     }
     // the first transform pass reads the staged input rows directly: line
     // p*ZB + l packs fields 2p, 2p+1 of z line l as A + iB of the complex
@@ -330,30 +342,31 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
       }
       return cz<CT>();
     };
-    F::template nat2perm_in<+1>(W, 4 * ZB, LD, wtwx<CT>(d), load);
+    F::template nat2perm_in<+1>(W, NL * ZB, LD, wtwx<CT>(d), load);
     // the staged rows are consumed: stage the next tile meanwhile
     if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
       fence_proxy_async();
       issue(t + gridDim.x);
     }
-    F::template nat2perm_p2<+1>(W, 4 * ZB, LD);
+    F::template nat2perm_p2<+1>(W, NL * ZB, LD);
 
     // mixed form: s_min / s_est (filled before the transform above) hold the
     // FP64 00 profiles of the inputs at this y and the values subtracted from
     // the outputs before they are rounded to FP32
     constexpr bool MX = sizeof(ST) == sizeof(float2);
-    double acc[11];
+    double acc[NO];
     if constexpr (MX) {
 #pragma unroll
-      for (int o = 0; o < 11; o++) acc[o] = 0.0;
+      for (int o = 0; o < NO; o++) acc[o] = 0.0;
     }
 
-    Re r0[PT], r1[PT], r2[PT];
+    Re r0[PT], r1[PT], r2[PT], r3[ZS ? PT : 1];
     double rs = 0.0, mv = 0.0;
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
       r0[j] = r1[j] = r2[j] = 0.0;
+      if constexpr (ZS) r3[j] = 0.0;
       if (q < nzb * N) {
         const int l = q / N, pos = q - l * N;
         CT *c0 = W + (size_t)l * LD + F::sk(pos);
@@ -374,7 +387,19 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
           tn = tn + dtg * rhs;                                           // cross.f:1641
           d8 = d8 + dtg * rhs;                                           // cross.f:1642
         }
-        double o[11];
+        double o[NO];
+        if constexpr (ZS) {  // the passive scalar, advanced as T is
+          CT *c4 = c3 + (size_t)ZB * LD, *c5 = c4 + (size_t)ZB * LD;
+          double2 p4 = to_d2(*c4), p5 = to_d2(*c5);
+          if constexpr (MX) {
+            p4.x += s_min[6];
+            p5.x += s_min[7];
+          }
+          const double lapZ = p4.x, zx = p4.y, zy = p5.x, zz = p5.y;
+          const double rzs = -u * zx - v * zy - w * zz + T * lapZ / d.pez;
+          d.rhsz[((size_t)y * d.mgalz + z0 + l) * N + pos] = rzs;
+          o[ODZ] = dtxi * rz[j] + dtg * rzs;
+        }
         o[OU] = u; o[OV] = v; o[OW] = w;
         o[ORUU] = ru * u; o[ORVV] = rv * v; o[ORWW] = rw * w;              // cross.f:1655-1666
         o[ORUV] = ru * v; o[ORUW] = ru * w; o[ORVW] = rv * w;
@@ -382,7 +407,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         o[ODT] = d8;                                                     // cross.f:1645-1647
         if constexpr (MX) {
 #pragma unroll
-          for (int q = 0; q < 11; q++) {
+          for (int q = 0; q < NO; q++) {
             acc[q] += o[q];
             o[q] -= s_est[q];
           }
@@ -394,6 +419,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         r0[j] = (Re)o[ORVW];
         r1[j] = (Re)o[ODRHO];
         r2[j] = (Re)o[ODT];
+        if constexpr (ZS) r3[j] = (Re)o[ODZ];
         if (do_cfl) {
           mu = fmax(mu, fabs(u));
           mv = fmax(mv, fabs(v));
@@ -410,7 +436,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
     if constexpr (MX) {  // FP64 partial plane sums, one slot per (tile, warp)
       const int slot = (z0 / ZB) * (G::XT / 32) + (threadIdx.x >> 5);
 #pragma unroll
-      for (int q = 0; q < 11; q++) {
+      for (int q = 0; q < NO; q++) {
         const double v = warp_sum(acc[q]);
         if ((threadIdx.x & 31) == 0) d.mpart[((size_t)q * d.my + y) * d.mpart_ld + slot] = v;
       }
@@ -424,7 +450,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
       const double hy = d.hy[y];
       cfy = fmax(cfy, __longlong_as_double((long long)s_vmax) / hy);
       for (int l = 0; l < nzb; l++) {
-        const double DD = ipe * __longlong_as_double((long long)s_tmax[l]);  // cross.f:1704
+        // cross.f:1704; with the scalar the larger of the two diffusivities
+        const double DD = (ZS ? fmax(ipe, 1.0 / d.pez) : ipe) * __longlong_as_double((long long)s_tmax[l]);
         cft = fmax(cft, 2.0 * DD * ((d.hxalp / 2) * (d.hxalp / 2) + (d.hzbet / 2) * (d.hzbet / 2) + (1.0 / hy) * (1.0 / hy)));
         s_tmax[l] = 0ull;
       }
@@ -443,13 +470,14 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         const int l = q / N, pos = q - l * N;
         CT *c0 = W + (size_t)l * LD + F::sk(pos);
         c0[0] = cmk<CT>(r0[j], r1[j]);
-        c0[(size_t)ZB * LD] = cmk<CT>(r2[j], 0);
+        if constexpr (ZS) c0[(size_t)ZB * LD] = cmk<CT>(r2[j], r3[j]);  // (Delta T, Delta Z)
+        else c0[(size_t)ZB * LD] = cmk<CT>(r2[j], 0);
       }
     }
     __syncthreads();
     F::template perm2nat<-1>(W, 2 * ZB, LD, wtwx<CT>(d));
     x_extract<N1, N2, CT, ST>(d, W, 0, ORVW, ODRHO, y, z0, nzb);
-    if (!d.variant) x_extract<N1, N2, CT, ST>(d, W, 1, ODT, -1, y, z0, nzb);
+    if (!d.variant) x_extract<N1, N2, CT, ST>(d, W, 1, ODT, ZS ? ODZ : -1, y, z0, nzb);
     __syncthreads();
   }
   if (do_cfl) {
@@ -642,9 +670,9 @@ struct Launch {
   static size_t zinv_sm(int mz) {
     return round16(sizeof(CT) * ZG::KB * G::LD) + ((size_t)ZG::KB * mz + 2 * E) * sizeof(ST);
   }
-  static size_t xsm() { return round16(sizeof(CT) * 4 * G::ZB * G::LD); }
-  static size_t xphys_sm(int nkx) {
-    return xsm() + (size_t)8 * G::ZB * nkx * sizeof(ST) + (size_t)G::ZB * G::N * sizeof(double);
+  static size_t xsm(bool zs) { return round16(sizeof(CT) * (zs ? 6 : 4) * G::ZB * G::LD); }
+  static size_t xphys_sm(int nkx, bool zs = false) {
+    return xsm(zs) + (size_t)(zs ? 12 : 8) * G::ZB * nkx * sizeof(ST) + (size_t)(zs ? 2 : 1) * G::ZB * G::N * sizeof(double);
   }
   // resident blocks per SM x SMs, for the persistent kernels
   static int grid_for(const void *fn, int threads, size_t smem, int ntiles) {
@@ -668,7 +696,7 @@ struct Launch {
     k_zinv<N1, N2, CT, ST><<<g, ZG::ZT, sm, s>>>(d, ntiles, mode, f0);
   }
   static void zfwd(const Dev &d, int mode, cudaStream_t s) {
-    dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : 11));
+    dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : n_out(d)));
     k_zfwd<N1, N2, CT, ST><<<g, ZG::ZT, zsm(), s>>>(d, mode);
   }
   static void xdrho(const Dev &d, cudaStream_t s) {
@@ -677,15 +705,20 @@ struct Launch {
       k_xdrho<N1, N2><<<g, G::XT, (size_t)G::ZB * G::LD * sizeof(double2), s>>>(d);
     }
   }
-  static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+  template <bool ZS>
+  static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
-    const size_t sm = xphys_sm(d.nkx);
-    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST>, G::XT, sm, ntiles);
-    k_xphys<N1, N2, CT, ST><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    const size_t sm = xphys_sm(d.nkx, ZS);
+    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS>, G::XT, sm, ntiles);
+    k_xphys<N1, N2, CT, ST, ZS><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
     if constexpr (sizeof(ST) == sizeof(float2)) {
       const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (G::XT / 32);
-      k_msum<N1, N2><<<dim3(d.my, 11), 128, 0, s>>>(d, nslot);
+      k_msum<N1, N2><<<dim3(d.my, n_out(d)), 128, 0, s>>>(d, nslot);
     }
+  }
+  static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
+    if (d.scalar) xphys_zs<true>(d, rk, do_cfl, do_diag, s);
+    else xphys_zs<false>(d, rk, do_cfl, do_diag, s);
   }
   static size_t xstats_sm() { return (size_t)3 * G::ZB * G::LD * sizeof(CT); }
   static void xstats(const Dev &d, const Stats &st, cudaStream_t s) {
@@ -704,7 +737,8 @@ struct Launch {
     if ((e = optin1((const void *)k_zinv<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_zfwd<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xstats<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
-    return optin1((const void *)k_xphys<N1, N2, CT, ST>, limit);
+    if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true>, limit)) != cudaSuccess) return e;
+    return optin1((const void *)k_xphys<N1, N2, CT, ST, false>, limit);
   }
 };
 
@@ -756,7 +790,7 @@ inline cudaError_t upload_twiddles() {
   case N: LMC_FFT_FORMS_M(N1, N2, 1, zinv(d, mode, f0, nf, s)) return true;
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
-#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3);
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3, zs);
 #define LMC_FFT_CASE_OPT(N, N1, N2)                                                         \
   if ((e = Launch<N1, N2, double2, double2>::optin(limit)) != cudaSuccess) return e;        \
   if ((e = Launch<N1, N2, float2, float2>::optin(limit)) != cudaSuccess) return e;          \
@@ -787,7 +821,7 @@ inline cudaError_t upload_twiddles() {
   size_t fft_zsm_##SUF(int n) {                                                                   \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_ZS) default: return 0; }                             \
   }                                                                                               \
-  size_t fft_xsm_##SUF(int n) {                                                                   \
+  size_t fft_xsm_##SUF(int n, bool zs) {                                                          \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_XS) default: return 0; }                              \
   }                                                                                               \
   cudaError_t fft_init_##SUF(int limit) {                                                         \

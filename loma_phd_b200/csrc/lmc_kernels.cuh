@@ -50,20 +50,30 @@ struct Dev {
   // state
   double2 *vor, *phi, *psi, *scal, *Rom, *Rphi;
   double *u00, *v00, *w00, *rf0u, *rf0w, *rf0v;
-  double2 *sb[11];  // spectral work buffers (FP64 form; [7..9] also staging)
-  double2 *zb[11];  // z-physical work buffers (FP64 form)
-  float2 *sbf[11];  // spectral work buffers (mixed form)
-  float2 *zbf[11];  // z-physical work buffers (mixed form)
+  double2 *sb[12];  // spectral work buffers (FP64 form; [7..9] also staging)
+  double2 *zb[12];  // z-physical work buffers (FP64 form)
+  float2 *sbf[12];  // spectral work buffers (mixed form)
+  float2 *zbf[12];  // z-physical work buffers (mixed form)
+  // [11] and the Z slots below exist only with the passive scalar
+  // Passive scalar Z (scalar = 1): the spectral state, the physical RHS(Z)
+  // of the previous substep, and Re*Sc; its wall values live in scal_d[5],
+  // scal_d[6].  Z is advanced as T is: derivatives, transforms, physical
+  // RK3 accumulator, increment transformed back.
+  int scalar;
+  double pez;
+  double2 *zsc;
+  double *rhsz;
   double *rhst;
   // device scalars: [0] Deltat, [1] dtr, [2] time, [3] rhobot, [4] rhotop
   double *scal_d;
   unsigned long long *cflmax;  // [4] max|u|, max|v|/hy, max|w|, max cflT (ordered bits)
   double *rhom;                // [my] plane sums of 1/T
   // Mixed form: the kx = kz = 0 (00) modes bypass the FP32 transforms.
-  //   mi     [6][my]  00 profiles of the transform inputs rho u, rho v,
-  //                   rho w, lap T, dT/dy, T (FP64); zinv drops the 00
-  //                   coefficient and xphys adds the profile back per point
-  //   mo_cur [11][my] FP64 plane sums of the 11 transform outputs (their
+  //   mi     [8][my]  00 profiles of the transform inputs rho u, rho v,
+  //                   rho w, lap T, dT/dy, T, and with the scalar lap Z,
+  //                   dZ/dy (FP64); zinv drops the 00 coefficient and
+  //                   xphys adds the profile back per point
+  //   mo_cur [12][my] FP64 plane sums of the 11 (12) transform outputs (their
   //                   exact 00 modes times mgalx*mgalz), read by post1/psi
   //   mo_prev[11][my] the sums of the previous substep: xphys subtracts
   //                   prev/(mgalx*mgalz) before rounding an output to FP32,
@@ -105,9 +115,13 @@ enum {
 };
 
 // Spectral work-buffer roles before / after the transforms.
-// SB_T32 holds an FP32 copy of T for the z transforms of the mixed form.
-enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32 };
-enum { OU = 0, OV, OW, ORUU, ORVV, ORWW, ORUV, ORUW, ORVW, ODRHO, ODT };
+// SB_T32 holds an FP32 copy of T for the z transforms of the mixed form;
+// SB_LAPZ, SB_DZDY and SB_Z32 (the same for Z) are used with the scalar.
+enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32, SB_LAPZ, SB_DZDY, SB_Z32 };
+enum { OU = 0, OV, OW, ORUU, ORVV, ORWW, ORUV, ORUW, ORVW, ODRHO, ODT, ODZ };
+// transform inputs (8, 12 with the scalar) and outputs (11, 12)
+__host__ __device__ inline int n_in(const Dev &d) { return d.scalar ? 12 : 8; }
+__host__ __device__ inline int n_out(const Dev &d) { return d.scalar ? 12 : 11; }
 
 // work-buffer views of the two precisions
 template <typename CT>
@@ -135,6 +149,9 @@ bool fft_supported(int n);
 void launch_lapv(const Dev &d, cudaStream_t s);
 void launch_assemble(const Dev &d, int rk, cudaStream_t s);
 void launch_tder(const Dev &d, cudaStream_t s);
+// passive scalar: Z wall values, dZ/dy, lap Z; and Z += Delta Z
+void launch_zder(const Dev &d, cudaStream_t s);
+void launch_zupd(const Dev &d, cudaStream_t s);
 // mode 1 (2014 variant): the d(rho) round trip of T and Delta T; f0, nf:
 // only inputs f0 .. f0+nf-1 (nf <= 0: all)
 void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0, int f0 = 0, int nf = 0);

@@ -33,6 +33,8 @@ void tpm_psi(const Dev &d, int rk, cudaStream_t s) { LMC_TPMV(t_psi, d, rk); }
 void tpm_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *out2, cudaStream_t s) {
   tpm::t_op_y<<<tgrid(d), tpm::TB, 0, s>>>(d, op, in, out, out2);
 }
+void launch_zder(const Dev &d, cudaStream_t s) { LMC_TPM(t_zder, d); }
+void launch_zupd(const Dev &d, cudaStream_t s) { LMC_TPM(t_zupd, d); }
 void tpm_cfl14(const Dev &d, int do_cfl, cudaStream_t s) { tpm::k_cfl14<<<1, 32, 0, s>>>(d, do_cfl); }
 void tpm_psi00_14(const Dev &d, int rk, cudaStream_t s) { tpm::k_psi00_14<<<1, 32, 0, s>>>(d, rk); }
 

@@ -491,6 +491,90 @@ __global__ void __launch_bounds__(TB) t_tder(Dev d) {
 }
 
 // ----------------------------------------------------------------------
+// Passive scalar Z, treated as t_tder treats T: zero at the walls except
+// the 00 mode (held at scal_d[5], scal_d[6]), dZ/dy and lap Z for the
+// transforms, an FP32 copy of Z in the mixed forms (the z transforms form
+// dZ/dx, dZ/dz from it) and its 00 profiles (mi rows 6, 7).  Runs after
+// t_tder on the second stream and shares its scratch fields.
+// ----------------------------------------------------------------------
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_zder(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool m00 = M.m == 0;
+  double2 *s1 = d.ws[2] + M.m, *s2 = d.ws[3] + M.m;
+  {
+    Rd<double2, 8> r;
+    r.start(d.zsc + M.m, ld, my, 1, 0);
+    r.pop();
+    const double2 wb = m00 ? make_double2(d.scal_d[5], 0.0) : czero();
+    const double2 wt_bc = m00 ? make_double2(d.scal_d[6], 0.0) : czero();
+    Win w;
+    w.clear();
+    Hist h1, h2;
+    h1.clear();
+    h2.clear();
+    w.push(wb);
+    for (int t = 1; t < 3; t++) w.push(r.pop());
+    #pragma unroll 4
+    for (int j = 0; j < my; j++) {
+      const double2 v = r.pop();
+      w.push(j + 3 == my - 1 ? wt_bc : v);
+      const double2 Z = w.c();
+      put(d.zsc + M.m, ld, j, Z);
+      if constexpr (mixed<CT>()) put(wsb<CT>(d, SB_Z32) + M.m, ld, j, Z);
+      s1[(size_t)j * ld] = d1f(d, j, w, h1);
+      s2[(size_t)j * ld] = d2f(d, j, w, h2);
+    }
+  }
+  {
+    Rd<double2, 4> r1, r2, rZ;
+    r1.start(s1, ld, my, -1, my - 1);
+    r2.start(s2, ld, my, -1, my - 1);
+    rZ.start(d.zsc + M.m, ld, my, -1, my - 1);
+    CT *DY = wsb<CT>(d, SB_DZDY) + M.m, *LZ = wsb<CT>(d, SB_LAPZ) + M.m;
+    Hist h1, h2;
+    h1.clear();
+    h2.clear();
+    #pragma unroll 4
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 dZ = d1b(d, j, r1.pop(), h1);
+      const double2 lZ = csub(d2b(d, j, r2.pop(), h2), cscale(M.k2, rZ.pop()));
+      if constexpr (mixed<CT>())
+        if (m00) {
+          d.mi[(size_t)7 * my + j] = dZ.x;
+          d.mi[(size_t)6 * my + j] = lZ.x;
+        }
+      put(DY, ld, j, dZ);
+      put(LZ, ld, j, lZ);
+    }
+  }
+}
+
+// Z += Delta Z (the scalar's counterpart of cross.f:619-627); the mixed
+// forms take the exact FP64 00 mode of Delta Z from the plane sums
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_zupd(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  Rd<double2, 4> rz;
+  Rd<CT, kq<CT>(4)> rd;
+  rz.start(d.zsc + M.m, ld, my, 1, 0);
+  rd.start(wsb<CT>(d, ODZ) + M.m, ld, my, 1, 0);
+  #pragma unroll 4
+  for (int j = 0; j < my; j++) {
+    double2 dz = rd.pop();
+    if constexpr (mixed<CT>())
+      if (M.m == 0) dz = mo00_row(d, ODZ, j);
+    put(d.zsc + M.m, ld, j, cadd(rz.pop(), dz));
+  }
+}
+
+// ----------------------------------------------------------------------
 // (6a)-(6b) T update and N_i (cross.f:619-682); rf0u / rf0w get the 00
 // pencils of d(rho uv)/dy and d(rho vw)/dy for the 00 tail.
 // ----------------------------------------------------------------------

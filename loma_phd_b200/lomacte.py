@@ -32,7 +32,7 @@ SYMBOLS = (
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
     "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
-    "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read",
+    "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read", "lmc_load_scalar_f64", "lmc_get_scalar_f64",
 )
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset", "stats")
@@ -50,7 +50,8 @@ class lmc_params(ctypes.Structure):
                 ("Re", ctypes.c_double), ("alp", ctypes.c_double), ("bet", ctypes.c_double),
                 ("peclet", ctypes.c_double), ("cfl", ctypes.c_double), ("ncfl", ctypes.c_int),
                 ("dt_mode", ctypes.c_int), ("dt", ctypes.c_double), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int), ("variant", ctypes.c_int)]
+                ("device", ctypes.c_int), ("variant", ctypes.c_int), ("scalar", ctypes.c_int),
+                ("schmidt", ctypes.c_double)]
 
 
 class lmc_diag(ctypes.Structure):
@@ -112,6 +113,8 @@ def _lib():
         L.lmc_stats_reset.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_double]
         L.lmc_stats_step.argtypes = [vp, ctypes.c_int]
         L.lmc_stats_read.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.lmc_load_scalar_f64.argtypes = [vp, _dp]
+        L.lmc_get_scalar_f64.argtypes = [vp, _dp]
         L.lmc_footprint.argtypes = [ctypes.POINTER(lmc_params)]
         L.lmc_footprint.restype = ctypes.c_size_t
         _LIB = L
@@ -154,6 +157,8 @@ class Params:
     precision: int = 0
     device: int = 0
     variant: int = 0          # 0 trunk/lomacte3 (2017), 1 trunk/lomacte (2014)
+    scalar: int = 0           # 1: carry a passive scalar Z (lmc_load_scalar_f64)
+    schmidt: float = 0.0      # Sc of Z; <= 0: Sc = Pr = 0.7f
 
     def c(self) -> lmc_params:
         return lmc_params(*[getattr(self, f.name) for f in dataclasses.fields(self)])
@@ -307,6 +312,16 @@ class Lomacte:
 
     def step(self, n: int = 1):
         _check(_lib().lmc_step(self._h, int(n)), "lmc_step")
+
+    # passive scalar Z (Params.scalar = 1): reference layout, complex
+    def load_scalar(self, z):
+        a = np.ascontiguousarray(np.asarray(z, dtype=np.complex128).reshape(self.shape))
+        _check(_lib().lmc_load_scalar_f64(self._h, _ptr(a.view(np.float64))), "lmc_load_scalar_f64")
+
+    def get_scalar(self) -> np.ndarray:
+        a = np.zeros(self.shape, dtype=np.complex128)
+        _check(_lib().lmc_get_scalar_f64(self._h, _ptr(a.view(np.float64))), "lmc_get_scalar_f64")
+        return a
 
     def sync(self):
         _check(_lib().lmc_sync(self._h), "lmc_sync")
