@@ -91,7 +91,10 @@ def write_restart(path: str, state: Dict[str, np.ndarray], y: np.ndarray, fmap: 
                   Re: float, alp: float, bet: float, a0: float = 0.0) -> None:
     """Write a state dict (vor, phi, psi, scal complex [nkx][mz][my]; u00,
     v00, w00 [my]) as the reference writes its images (escru.f:121-139).
-    Values are stored in real*4 like the reference; y and fmap in real*8."""
+    Values are stored in real*4 like the reference; y and fmap in real*8.
+    With a passive scalar under "mfz" the plane records carry it as a fifth
+    interleaved field, as the scalar-carrying branch reads them
+    (branches/lomaHZ/src/main.f:432-433: ntotr = 5*2*my*mz)."""
     vor = np.asarray(state["vor"])
     nkx, mz, my = vor.shape
     y = np.asarray(y, dtype=np.float64)
@@ -106,11 +109,12 @@ def write_restart(path: str, state: Dict[str, np.ndarray], y: np.ndarray, fmap: 
     w00[:, 0] = state["u00"]
     w00[:, 1] = state["v00"]
     w00[:, 2] = state["w00"]
+    names = _FIELDS + (("mfz",) if "mfz" in state else ())
     with open(path, "wb") as f:
         _write_record(f, head + yf.tobytes() + w00.tobytes())
-        plane = np.empty((mz, 2 * my, 4), dtype="<f4")
+        plane = np.empty((mz, 2 * my, len(names)), dtype="<f4")
         for i in range(nkx):
-            for q, name in enumerate(_FIELDS):
+            for q, name in enumerate(names):
                 a = np.ascontiguousarray(state[name][i], dtype=np.complex64)  # [mz][my]
                 plane[:, :, q] = a.view(np.float32).reshape(mz, 2 * my)
             _write_record(f, plane.tobytes())
@@ -132,7 +136,8 @@ def _assign_kz(a: np.ndarray, mz: int) -> np.ndarray:
 def read_restart(path: str, mz: Optional[int] = None) -> Dict[str, object]:
     """Read a restart / image file.  Returns a dict with the header
     (RestartHeader under "header") and the state: vor, phi, psi, scal as
-    complex128 [nplanes][mz][my] (real*4 values widened), u00, v00, w00.
+    complex128 [nplanes][mz][my] (real*4 values widened), u00, v00, w00, and
+    "mfz" when the plane records carry a fifth field (the passive scalar).
     With mz given, the kz modes are re-mapped as the reference does."""
     with open(path, "rb") as f:
         r1 = _read_record(f)
@@ -145,20 +150,23 @@ def read_restart(path: str, mz: Optional[int] = None) -> Dict[str, object]:
         yf = np.frombuffer(r1, dtype="<f8", count=2 * my, offset=32).reshape(my, 2)
         w00 = np.frombuffer(r1, dtype="<f4", count=3 * my, offset=32 + 16 * my).reshape(my, 3)
         planes: List[np.ndarray] = []
+        nf = 4
         while True:
             rec = _read_record(f)
             if rec is None:
                 break
-            if len(rec) != 4 * 8 * my * mze:
+            if not planes and len(rec) == 5 * 8 * my * mze:
+                nf = 5
+            if len(rec) != nf * 8 * my * mze:
                 raise ValueError("plane record of unexpected length")
-            planes.append(np.frombuffer(rec, dtype="<f4").reshape(mze, 2 * my, 4))
-    data = np.stack(planes) if planes else np.zeros((0, mze, 2 * my, 4), dtype=np.float32)
+            planes.append(np.frombuffer(rec, dtype="<f4").reshape(mze, 2 * my, nf))
+    data = np.stack(planes) if planes else np.zeros((0, mze, 2 * my, nf), dtype=np.float32)
     out: Dict[str, object] = {
         "header": RestartHeader(time, Re, alp, bet, a0, mx, my, mze, yf[:, 0].copy(), yf[:, 1].copy()),
         "u00": w00[:, 0].astype(np.float64), "v00": w00[:, 1].astype(np.float64),
         "w00": w00[:, 2].astype(np.float64), "time": float(time),
     }
-    for q, name in enumerate(_FIELDS):
+    for q, name in enumerate(_FIELDS + (("mfz",) if nf == 5 else ())):
         re_im = np.ascontiguousarray(data[:, :, :, q]).reshape(data.shape[0], mze, my, 2)
         c = (re_im[..., 0].astype(np.float64) + 1j * re_im[..., 1].astype(np.float64))
         out[name] = _assign_kz(c, mz) if mz is not None else c

@@ -45,6 +45,21 @@ def test_restart_round_trip_and_layout(tmp_path):
     assert len(raw) == 8 + n1 + p.nplanes * (8 + n2)
 
 
+def test_restart_with_scalar_field(tmp_path):
+    p, y, st = case(16, 16, 33)
+    fm = y_metrics(y)["fmap"]
+    st = dict(st)
+    st["mfz"] = 0.5 * np.asarray(st["scal"])
+    path = str(tmp_path / "case_z.001")
+    write_restart(path, st, y, fm, time=0.5, Re=p.Re, alp=p.alp, bet=p.bet)
+    r = read_restart(path)
+    assert np.array_equal(r["mfz"], np.asarray(st["mfz"]).astype(np.complex64).astype(np.complex128))
+    assert np.array_equal(r["vor"], _f32(st)["vor"])
+    raw = open(path, "rb").read()
+    n1 = struct.unpack("<i", raw[:4])[0]
+    assert struct.unpack("<i", raw[8 + n1:12 + n1])[0] == 5 * 8 * p.my * p.mz
+
+
 def test_restart_kz_remapping(tmp_path):
     p, y, st = case(16, 16, 33)
     path = str(tmp_path / "case.002")
