@@ -369,13 +369,14 @@ def run_serving(a, dev):
     from loma_phd_b200.serve import Server, synthetic_stream
     free, _ = torch.cuda.mem_get_info(dev)
     cap = int(min(150e9, 0.8 * free))
-    out = {"stream": f"{a.serve_requests} requests, Poisson arrivals at 4/s, nx=nz in {{64..256}}, "
-                     f"ny in {{129,193,257}}, Re~U[100,1000], s~U[1,8], steps log-uniform [200,2000] x "
+    out = {"stream": f"{a.serve_requests} requests, Poisson arrivals at 4/s, half 2-D (nz=1, nx in "
+                     f"{{256..1024}}, ny=257), half 3-D (nx=nz in {{64..256}}, ny in {{129,193,257}}), "
+                     f"Re~U[100,1000], s~U[1,8], steps log-uniform [200,2000] x "
                      f"{a.serve_scale:g}, HBM cap {cap / 1e9:.0f} GB, 16 slots",
            "unit": "s (latency), Mpts*RK3-steps/s (aggregate)"}
     for name, prec in (("mixed", a.mixed_form), ("fp64", 0)):
         reqs = synthetic_stream(a.serve_requests, seed=7, rate=4.0, steps_scale=a.serve_scale,
-                                nx_range=(64, 256), precision=prec)
+                                nx_range=(64, 256), precision=prec, frac_2d=0.5)
         out[name] = Server(cap, max_active=16, chunk=8, device=dev).run(reqs)["stats"]
     return out
 

@@ -248,7 +248,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   }
   const lmc::Grid &g = h->g;
   int rc = LMC_OK;
-  if (g.nkx < 1 || g.mz < 1 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) rc = LMC_EINVAL;
+  // x lengths from 24 up; z also 3 (mz = 1: a 2-D run, one kz mode)
+  if (g.nkx < 1 || g.mz < 1 || g.mgalx < 24 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz))
+    rc = LMC_EINVAL;
   if (!rc) rc = pick_chunks(g.my, d.C, d.lpm, d.base, d.extra);
   if (rc) { delete h; return rc; }
   try {
@@ -846,7 +848,7 @@ size_t lmc_footprint(const lmc_params *p) {
   g.set(p->mgalx, p->mgalz, p->my);
   int C, lpm, base, extra;
   if (g.nkx < 1 || g.mz < 1 || pick_chunks(g.my, C, lpm, base, extra) != LMC_OK) return 0;
-  if (!lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) return 0;
+  if (g.mgalx < 24 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) return 0;
   const size_t S = (size_t)g.nmode * g.my, Z = (size_t)g.nkx * g.my * g.mgalz;
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)

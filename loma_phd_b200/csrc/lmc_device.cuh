@@ -426,12 +426,12 @@ __device__ __forceinline__ double warp_max(double v) {
 // Twiddles exp(-2 pi i e/R) come from a constant table (c_tw), one block
 // per size, filled by the host at initialisation.
 // ---------------------------------------------------------------------
-constexpr int TW_SIZES[] = {4, 6, 8, 9, 12, 16, 18, 24, 32, 36};
+constexpr int TW_SIZES[] = {4, 6, 8, 9, 12, 16, 18, 24, 32, 36, 48};
 __host__ __device__ constexpr int tw_off(int R) {
   return R == 4 ? 0 : R == 6 ? 4 : R == 8 ? 10 : R == 9 ? 18 : R == 12 ? 27 : R == 16 ? 39 : R == 18 ? 55
-       : R == 24 ? 73 : R == 32 ? 97 : R == 36 ? 129 : -1;
+       : R == 24 ? 73 : R == 32 ? 97 : R == 36 ? 129 : R == 48 ? 165 : -1;
 }
-constexpr int TW_TOTAL = 4 + 6 + 8 + 9 + 12 + 16 + 18 + 24 + 32 + 36;
+constexpr int TW_TOTAL = 4 + 6 + 8 + 9 + 12 + 16 + 18 + 24 + 32 + 36 + 48;
 
 static __constant__ double2 c_tw[TW_TOTAL];  // one copy per translation unit
 static __constant__ float2 c_twf[TW_TOTAL];  // the same, rounded to FP32

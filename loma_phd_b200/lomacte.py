@@ -177,8 +177,9 @@ class Params:
 
     @staticmethod
     def from_modes(nx: int, nz: int, ny: int, **kw) -> "Params":
-        """Grid from nominal Fourier-mode counts (nx = mx, nz = mz+1)."""
-        return Params(mgalx=3 * nx // 2, mgalz=3 * nz // 2, my=ny, **kw)
+        """Grid from nominal Fourier-mode counts (nx = mx, nz = mz+1); nz = 1
+        is a 2-D run (mz = 1, mgalz = 3)."""
+        return Params(mgalx=3 * nx // 2, mgalz=3 if nz == 1 else 3 * nz // 2, my=ny, **kw)
 
 
 @dataclasses.dataclass

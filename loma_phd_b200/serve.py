@@ -201,22 +201,34 @@ class Server:
 _MODES = (64, 96, 128, 192, 256, 384)
 
 
+# x mode counts of 2-D requests (nx = 2/3 mgalx, mgalx from 384 to 1536)
+_MODES_2D = (256, 384, 512, 768, 1024)
+
+
 def synthetic_stream(n: int, seed: int = 0, rate: float = 2.0, steps_range=(200, 2000), steps_scale: float = 1.0,
-                     nx_range=(64, 384), ny_choices=(129, 193, 257), precision: int = 1) -> List[RunRequest]:
-    """Poisson arrivals of 3-D runs: nx = nz drawn from the supported sizes
-    in nx_range, ny from ny_choices, Re ~ U[100, 1000], s ~ U[1, 8], steps
-    log-uniform in steps_range (times steps_scale), amplitude ~ U[5e-3, 2e-2]."""
+                     nx_range=(64, 384), ny_choices=(129, 193, 257), precision: int = 1,
+                     frac_2d: float = 0.0, nx2d_range=(256, 1024)) -> List[RunRequest]:
+    """Poisson arrivals of runs: 3-D with nx = nz drawn from the supported
+    sizes in nx_range and ny from ny_choices, or, with probability frac_2d,
+    2-D (nz = 1) with nx from nx2d_range and ny = 257; Re ~ U[100, 1000],
+    s ~ U[1, 8], steps log-uniform in steps_range (times steps_scale),
+    amplitude ~ U[5e-3, 2e-2]."""
     rng = np.random.default_rng(seed)
     modes = [m for m in _MODES if nx_range[0] <= m <= nx_range[1]]
+    modes2 = [m for m in _MODES_2D if nx2d_range[0] <= m <= nx2d_range[1]]
     t = 0.0
     out = []
     for i in range(n):
         t += rng.exponential(1.0 / rate)
-        nx = int(rng.choice(modes))
-        ny = int(rng.choice(ny_choices))
+        two_d = frac_2d > 0 and rng.uniform() < frac_2d
+        if two_d:
+            nx, nz, ny = int(rng.choice(modes2)), 1, 257
+        else:
+            nx = int(rng.choice(modes))
+            nz, ny = nx, int(rng.choice(ny_choices))
         lo, hi = math.log(steps_range[0]), math.log(steps_range[1])
         steps = max(1, int(round(math.exp(rng.uniform(lo, hi)) * steps_scale)))
-        out.append(RunRequest(rid=i, nx=nx, nz=nx, ny=ny, steps=steps, Re=float(rng.uniform(100, 1000)),
+        out.append(RunRequest(rid=i, nx=nx, nz=nz, ny=ny, steps=steps, Re=float(rng.uniform(100, 1000)),
                               s=float(rng.uniform(1.0, 8.0)), amp=float(rng.uniform(5e-3, 2e-2)),
                               seed=int(rng.integers(0, 2**31 - 1)), precision=precision, arrival=t))
     return out

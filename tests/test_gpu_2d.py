@@ -1,0 +1,74 @@
+"""2-D runs (one kz mode: nz = 1, mz = 1, mgalz = 3) and the longest x
+transform (1536 points, nx = 1024), the request shapes of BASELINE's
+serving config, against the FP64 oracle through the C ABI.
+
+Bars as in test_gpu_parity.py: FP64 1 RK3 step <= 1e-10 relative L2 per
+field, 20 steps <= 1e-9 with the momentum thickness to 1e-9; mixed forms 1
+step <= 1e-6: form 1 (FP32 butterflies) at nx = 256, form 2 (FP64
+butterflies, FP32 storage) at nx = 1024, where form 1's round-off, carried
+to phi with the k^3 weight of its equation, reaches 9e-5 after one step.
+"""
+import numpy as np
+import pytest
+
+from loma_phd_b200 import Lomacte
+from tests.helpers import FIELDS, case, oracle_for, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _steps(p, y, st, n):
+    g = Lomacte(p, y)
+    g.load_state(st)
+    o = oracle_for(p, y, st)
+    dg, do = [], []
+    for _ in range(n):
+        g.step(1)
+        o.step(1)
+        dg.append(g.diag()["dm"])
+        do.append(o.diag()["dm"])
+    out = g.get_state(), o.get_state(), np.array(dg), np.array(do)
+    g.close()
+    return out
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 65), (256, 65), (1024, 65)])
+def test_2d_one_step(gpu, nx, ny):
+    p, y, st = case(nx, 1, ny)
+    assert (p.mgalz, p.mz) == (3, 1)
+    sg, so, _, _ = _steps(p, y, st, 1)
+    for k in FIELDS:
+        assert rel_l2(sg[k], so[k]) < 1e-10, (k, rel_l2(sg[k], so[k]))
+
+
+def test_2d_twenty_steps(gpu):
+    p, y, st = case(256, 1, 129)
+    sg, so, dg, do = _steps(p, y, st, 20)
+    for k in FIELDS:
+        assert rel_l2(sg[k], so[k]) < 1e-9, k
+    assert np.abs(dg - do).max() < 1e-9
+
+
+def test_1536_3d_one_step(gpu):
+    p, y, st = case(1024, 32, 33)
+    assert p.mgalx == 1536
+    sg, so, _, _ = _steps(p, y, st, 1)
+    for k in FIELDS:
+        assert rel_l2(sg[k], so[k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("nx,prec", [(256, 1), (1024, 2)])
+def test_2d_mixed_one_step(gpu, nx, prec):
+    tol = 1e-6
+    p, y, st = case(nx, 1, 65, precision=prec)
+    p64, _, _ = case(nx, 1, 65)
+    g = Lomacte(p, y)
+    g.load_state(st)
+    g.step(1)
+    sm = g.get_state()
+    g.close()
+    o = oracle_for(p64, y, st)
+    o.step(1)
+    so = o.get_state()
+    for k in FIELDS:
+        assert rel_l2(sm[k], so[k]) < tol, (k, rel_l2(sm[k], so[k]))

@@ -17,6 +17,15 @@ from loma_phd_b200.serve import RunRequest, Server, ensemble_requests, synthetic
 from tests.helpers import FIELDS, case, rel_l2
 
 
+def test_stream_with_2d_requests():
+    a = synthetic_stream(40, seed=5, frac_2d=0.5)
+    two = [r for r in a if r.nz == 1]
+    assert 5 < len(two) < 35
+    assert all(r.ny == 257 and r.nx in (256, 384, 512, 768, 1024) for r in two)
+    assert all(footprint(r.params()) > 0 for r in a)
+    assert all(r.params().mgalz == 3 for r in two)
+
+
 def test_ensemble_requests():
     e = ensemble_requests(48, 500, precision=0)
     assert [r.seed for r in e] == list(range(48)) and all(r.arrival == 0.0 and r.steps == 500 for r in e)
