@@ -41,7 +41,7 @@ from loma_phd_b200.replicas import case_seed, job_throughput, max_over_ranks  # 
 # (P = mgalx * mgalz * ny real) counts.  State fields (Omega_y, phi, psi, T,
 # R_Omega, R_phi) are FP64 complex (16 B) in both forms; transform work
 # buffers take w bytes per complex value (16 in the FP64 form, 8 in the mixed
-# form).  Compulsory reads + writes of each kernel:
+# form).  Compulsory reads + writes of each kernel group (one profile id):
 #   zinv : 6 spectral inputs read (rho u, rho v, rho w, lap T, dT/dy, T), 8 Z written
 #   xphys: 8 Z read, 11 Z written, RHS(T) physical accumulator (FP64) read + written
 #   zfwd : 11 Z read, 11 S written
@@ -52,16 +52,23 @@ from loma_phd_b200.replicas import case_seed, job_throughput, max_over_ranks  # 
 #   post2: u, v, w, N_x, N_y, N_z, vor, phi read; R_om, R_phi, vor, phi written
 #          (two launches, post2a and post2b, counted together as one stage)
 #   psi  : drho read, psi written (+ 7 doubles/point mode tables read)
+# The passive scalar (sc) adds to zinv lap Z, dZ/dy, Z read and 4 Z
+# written; to xphys 4 Z read, 1 Z written (the twelfth output) and its
+# physical accumulator; to zfwd the twelfth output; to tder (t_zder) Z read
+# and written, dZ/dy, lap Z written; to zfwd's profile id (t_zupd) Z read
+# and written, Delta Z read.  The variable viscosity (vs) adds to zinv the
+# four strain-rate sums read and 6 Z written; to xphys 6 Z read; to the
+# assemble id (t_sgrad) rho u, rho v, rho w read and the four sums written.
 ALGO = {
-    "zinv": lambda S, Z, P, w: 6 * S * w + 8 * Z * w,
-    "xphys": lambda S, Z, P, w: 19 * Z * w + 2 * P * 8,
-    "zfwd": lambda S, Z, P, w: 11 * Z * w + 11 * S * w,
-    "lapv": lambda S, Z, P, w: S * 16 + 2 * S * w + S * 7 * 8 // 2,
-    "assemble": lambda S, Z, P, w: 7 * S * 16 + 5 * S * w,
-    "tder": lambda S, Z, P, w: 2 * S * 16 + 2 * S * w,
-    "post1": lambda S, Z, P, w: 2 * S * 16 + 10 * S * w,
-    "post2": lambda S, Z, P, w: 6 * S * 16 + 6 * S * w,
-    "psi": lambda S, Z, P, w: S * 16 + S * w + S * 7 * 8 // 2,
+    "zinv": lambda S, Z, P, w, sc, vs: (6 + 3 * sc + 4 * vs) * S * w + (8 + 4 * sc + 6 * vs) * Z * w,
+    "xphys": lambda S, Z, P, w, sc, vs: (19 + 5 * sc + 6 * vs) * Z * w + 2 * (1 + sc) * P * 8,
+    "zfwd": lambda S, Z, P, w, sc, vs: (11 + sc) * (Z + S) * w + sc * (2 * S * 16 + S * w),
+    "lapv": lambda S, Z, P, w, sc, vs: S * 16 + 2 * S * w + S * 7 * 8 // 2,
+    "assemble": lambda S, Z, P, w, sc, vs: 7 * S * 16 + 5 * S * w + vs * 7 * S * w,
+    "tder": lambda S, Z, P, w, sc, vs: (1 + sc) * (2 * S * 16 + 2 * S * w),
+    "post1": lambda S, Z, P, w, sc, vs: 2 * S * 16 + 10 * S * w,
+    "post2": lambda S, Z, P, w, sc, vs: 6 * S * 16 + 6 * S * w,
+    "psi": lambda S, Z, P, w, sc, vs: S * 16 + S * w + S * 7 * 8 // 2,
 }
 
 # DRAM bytes (read + write) per launch measured by ncu (full-set capture of
@@ -101,6 +108,8 @@ def parse():
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--scalar", action="store_true",
                     help="carry the passive scalar Z (extension; e2e loads the flow state only)")
+    ap.add_argument("--sigma", type=float, default=None,
+                    help="variable viscosity mu = k = rho D = T^sigma (extension; default: constant)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
@@ -182,13 +191,37 @@ def sizes(p):
     return S, Z, P
 
 
+def scalar_ic(st):
+    """Z = (T - T_bot)/(T_top - T_bot): the passive scalar of the workload."""
+    T = st["scal"]
+    tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
+    z = T / (tt - tb)
+    z[0, 0, :] -= tb / (tt - tb)
+    return z
+
+
+def oracle_case(a, p, y, st, nth):
+    """The oracle set up with the workload's extensions (Sc = Pr = 0.7f)."""
+    from oracle.oracle import Oracle
+    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=p.dt_mode, dt0=p.dt, nthreads=nth)
+    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    if a.scalar:
+        o.set_scalar(scalar_ic(st), float(np.float32(0.7)))
+    if a.sigma is not None:
+        o.set_viscosity(a.sigma)
+    return o
+
+
+def extensions(a):
+    e = (" + passive scalar" if a.scalar else "") + (f" + mu = T^{a.sigma:g}" if a.sigma is not None else "")
+    return e
+
+
 def cpu_baseline(a, p, y, st):
     """The FP64 CPU restatement (oracle) on the host cores: a bounded sample
     of the same workload (one RK3 substep), scaled to steps."""
-    from oracle.oracle import Oracle
     nth = os.cpu_count() or 1
-    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=p.dt_mode, dt0=p.dt, nthreads=nth)
-    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    o = oracle_case(a, p, y, st, nth)
     t0 = time.perf_counter()
     o.substep(0)
     dt = time.perf_counter() - t0
@@ -203,13 +236,11 @@ def run_reference(a):
     if rank != 0:
         return
     from loma_phd_b200 import ICParams, Params, make_ic, stretched_mesh
-    from oracle.oracle import Oracle
     p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01)
     y = stretched_mesh(p.my)
     st = make_ic(p, y, ICParams(s=4.0, seed=0))
     nth = os.cpu_count() or 1
-    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=1, dt0=0.01, nthreads=nth)
-    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    o = oracle_case(a, p, y, st, nth)
     for _ in range(a.warmup):
         o.substep(0)
     t0 = time.perf_counter()
@@ -223,7 +254,8 @@ def run_reference(a):
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded initial condition)",
-        "config": {"workload": f"lomacte FP64 {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
+        "config": {"workload": f"lomacte FP64{extensions(a)} {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), "
+                               f"s=4, Re=160, dt=0.01",
                    "sample": "each step = one RK3 substep", "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": val, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port",
                          "sample": f"{a.steps} RK3 substeps of the workload, FP64 CPU restatement "
@@ -241,17 +273,14 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     from loma_phd_b200.lomacte import KERNEL_NAMES
 
     p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec,
-                          scalar=1 if a.scalar else 0)
+                          scalar=1 if a.scalar else 0, visc=0 if a.sigma is None else 1,
+                          sigma=a.sigma or 0.0)
     y = stretched_mesh(p.my)
     st = make_ic(p, y, ICParams(s=4.0, seed=case_seed(rank)))
     g = Lomacte(p, y)
     g.load_state(st)
     if a.scalar:  # Z = (T - T_bot)/(T_top - T_bot), Sc = Pr
-        T = st["scal"]
-        tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
-        z = T / (tt - tb)
-        z[0, 0, :] -= tb / (tt - tb)
-        g.load_scalar(z)
+        g.load_scalar(scalar_ic(st))
     g_launches = g.launches_per_step
     y_family = g.y_family
     stream = torch.cuda.ExternalStream(g.stream, device=dev)
@@ -336,7 +365,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     top = max((k for k in KERNEL_NAMES if k in ALGO), key=lambda k: prof[k][0])
     tot_ms, cnt = prof[top]
     avg_s = tot_ms / max(cnt, 1) / 1e3
-    algo = ALGO[top](S, Z, P, w)
+    sc, vs = int(a.scalar), int(a.sigma is not None)
+    algo = ALGO[top](S, Z, P, w, sc, vs)
     peak, kind = peaks()
     achieved = algo / avg_s / 1e9
     # fraction of the timed region during which each kernel group runs; the
@@ -345,7 +375,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES if prof[k][1]}
     traffic = None
     table = NCU_TRAFFIC_256x65 if prec == 0 else NCU_TRAFFIC_MIXED_256x65
-    if a.nx == 256 and a.nz == 256 and top in table:
+    if a.nx == 256 and a.nz == 256 and top in table and not sc and not vs:
         traffic = table[top] * a.ny / 65.0
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
@@ -353,7 +383,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
                                   "256x65x256, scaled by ny/65" if traffic else None,
                 "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
     launches = g_launches
-    step_bytes = 3 * sum(f(S, Z, P, w) for f in ALGO.values())
+    step_bytes = 3 * sum(f(S, Z, P, w, sc, vs) for f in ALGO.values())
     return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
             "kernel_share": share, "e2e": e2e, "state": state, "diag": diag, "step_bytes": step_bytes,
             "stats_step": stats_step,
@@ -454,7 +484,7 @@ def main():
             "precision_form": a.mixed_form if mixed else 0,
             "data": "synthetic (seeded initial condition)",
             "config": {"workload": f"lomacte {MIXED_NAMES[a.mixed_form] if mixed else 'FP64 plain path'}"
-                                   f"{' + passive scalar' if a.scalar else ''} "
+                                   f"{extensions(a)} "
                                    f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
                        "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},

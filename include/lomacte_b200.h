@@ -61,6 +61,15 @@ typedef struct lmc_params {
                            counterpart in the lomacte codes, see
                            lmc_load_scalar_f64); not with variant 1 */
   double schmidt;       /* Schmidt number Sc of Z; <= 0: Sc = Pr = 0.7f */
+  int visc;             /* 1: variable viscosity mu = k = rho D = T^sigma (an
+                           extension after branches/loma/src/cross.f:
+                           1591-1596, 2177-2196); 0: the constant viscosity
+                           of lomacte3.  Not with variant 1; the x stage
+                           then needs mgalx <= 768 (1152 without the
+                           scalar) for its shared memory */
+  double sigma;         /* exponent sigma in [0, 4] (0.7 for air;
+                           branches/loma reads it as hre.dat's fourth
+                           value, main.f:543) */
 } lmc_params;
 
 /* Per-step diagnostics (the .cf record of cross.f:1172-1176 without the
@@ -120,6 +129,20 @@ int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi,
  * clears Z's RK3 memory.  LMC_EINVAL without the scalar. */
 int lmc_load_scalar_f64(lmc_handle *h, const double *z);
 int lmc_get_scalar_f64(lmc_handle *h, double *z);
+
+/* Variable viscosity (lmc_params.visc = 1): mu = k = rho D = T^sigma.  The
+ * lomacte3 substep keeps its constant-viscosity terms; in physical space
+ *   RHS(T) = -u.grad T + T^sigma (T lap T + sigma |grad T|^2) / Pe
+ *   RHS(Z) = -u.grad Z + T^sigma (T lap Z + sigma grad T.grad Z) / (Re Sc)
+ * (branches/loma/src/cross.f:1591-1596), and the products rho u_i u_j that
+ * the substep differentiates lose 2 (T^sigma - 1) S_ij / Re, with S_ij from
+ * d(u_i)/dx_j = T d(rho u_i)/dx_j + rho u_i dT/dx_j (six more transform
+ * inputs).  The total viscous force is then the divergence of
+ * 2 T^sigma S_ij / Re up to a gradient, which the Omega_y and phi
+ * equations do not see, as branches/loma/src/cross.f:2177-2196 forms it
+ * (tau_ij = 2 T^sigma S_ij, the isotropic part left in the pressure).  The
+ * diffusive CFL limit takes T_max^(1+sigma).  sigma = 0 reproduces the
+ * constant-viscosity substep. */
 
 /* Advance nsteps full RK3 steps (the body of cross.f:225-1226, 3
  * substeps of cross.f:307-1141 each).  Asynchronous on the handle's

@@ -235,6 +235,8 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   if (p->precision < 0 || p->precision > 2) return LMC_EINVAL;
   if (p->variant < 0 || p->variant > 1 || (p->variant == 1 && p->precision != 0)) return LMC_EINVAL;
   if (p->scalar < 0 || p->scalar > 1 || (p->scalar && p->variant)) return LMC_EINVAL;
+  if (p->visc < 0 || p->visc > 1 || (p->visc && (p->variant || !(p->sigma >= 0.0 && p->sigma <= 4.0))))
+    return LMC_EINVAL;
   lmc_handle *h = new (std::nothrow) lmc_handle();
   if (!h) return LMC_ENOMEM;
   h->p = *p;
@@ -278,6 +280,8 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   d.ire = 1.0 / p->Re;
   d.variant = p->variant;
   d.scalar = p->scalar;
+  d.visc = p->visc;
+  d.sigma = p->visc ? p->sigma : 0.0;
   // Re*Sc; Sc <= 0 takes Sc = Pr, the Schmidt number of the reference's Pe = Re*0.7f
   d.pez = p->Re * (p->schmidt > 0 ? p->schmidt : (double)0.7f);
   // Pe = Re*0.7f (main.f:569); the 2014 code uses Pe = Re (lomacte/cross.f:1301)
@@ -292,8 +296,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   // y-operator tables go to the device chunk-major (see lmcd::tab)
   const int C = d.C, lpm = d.lpm, base = d.base, extra = d.extra, my = g.my;
   auto cm = [&](const std::vector<double> &T, int W) { return lmc::chunk_major(T, my, W, C, lpm, base, extra); };
-  // the 2014 variant and the passive scalar run the mode-parallel kernels
-  d.tpm = (d.variant || p->scalar) ? 1 : mode_parallel(g.nmode);
+  // the 2014 variant, the passive scalar and the variable viscosity run
+  // the mode-parallel kernels
+  d.tpm = (d.variant || p->scalar || p->visc) ? 1 : mode_parallel(g.nmode);
   const size_t pm2 = (size_t)C * 2 * 32, pm3 = (size_t)C * 3 * 32;
   const size_t nm = d.tpm ? 0 : (size_t)g.nmode;  // chunk-major per-mode tables: warp kernels only
   std::vector<double> PLc(nm * pm2), PUc(nm * pm3), V12c(nm * pm2);
@@ -379,19 +384,22 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     if ((rc = dalloc(h, q, ns))) { lmc_destroy(h); return rc; }
   // work buffers: FP64 in the plain form; FP32 in the mixed form, which
   // keeps three FP64 spectral buffers for the ABI transposes and lmc_op_y
-  for (int f = 0; f < (p->scalar ? 12 : 11); f++) {
-    if (!d.prec || (f >= 7 && f <= 9))
+  const int nsb = lmc::n_sbuf(d), nzb = lmc::n_zbuf(d);
+  for (int f = 0; f < (nsb > nzb ? nsb : nzb); f++) {
+    if (f < nsb && (!d.prec || (f >= 7 && f <= 9)))
       if ((rc = dalloc(h, &d.sb[f], ns))) { lmc_destroy(h); return rc; }
-    if (!d.prec) {
-      if ((rc = dalloc(h, &d.zb[f], nzp))) { lmc_destroy(h); return rc; }
-    } else {
-      if ((rc = dalloc(h, &d.sbf[f], ns)) || (rc = dalloc(h, &d.zbf[f], nzp))) { lmc_destroy(h); return rc; }
+    if (f < nsb && d.prec)
+      if ((rc = dalloc(h, &d.sbf[f], ns))) { lmc_destroy(h); return rc; }
+    if (f < nzb) {
+      if (!d.prec) rc = dalloc(h, &d.zb[f], nzp);
+      else rc = dalloc(h, &d.zbf[f], nzp);
+      if (rc) { lmc_destroy(h); return rc; }
     }
   }
   if (d.prec) {
     // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
     d.mpart_ld = 4 * g.mgalz;
-    if ((rc = dalloc(h, &d.mi, (size_t)8 * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
+    if ((rc = dalloc(h, &d.mi, (size_t)lmc::NMI * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &h->mo[1], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &d.mpart, (size_t)12 * g.my * d.mpart_ld))) {
       lmc_destroy(h);
@@ -591,8 +599,10 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
     }
     run(0, s, [&] { lmc::launch_lapv(d, s); });
     run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
+    if (d.visc) run(1, s, [&] { lmc::launch_sgrad(d, s); });  // the strain-rate inputs
     if (side_t) {
       run(3, s, [&] { lmc::launch_zinv(d, s, 0, 0, 3); });
+      if (d.visc) run(3, s, [&] { lmc::launch_zinv(d, s, 0, lmc::vbase(d), 6); });
       if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
     } else {
       run(2, s, [&] { lmc::launch_tder(d, s); });
@@ -835,8 +845,9 @@ int lmc_launches_per_step(lmc_handle *h) {
   // trip, its own 00 tail) and the Deltat kernel in the first substep
   if (h->d.variant) return 3 * 14 + 1;
   // the split inverse z transform adds one; the passive scalar three (its
-  // derivatives, its inverse z transforms, its update)
-  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0) + 1 + (h->d.scalar ? 3 : 0);
+  // derivatives, its inverse z transforms, its update); the variable
+  // viscosity two (the strain-rate inputs and their inverse z transforms)
+  const int per = (h->d.tpm ? 11 : 10) + (h->d.prec ? 1 : 0) + 1 + (h->d.scalar ? 3 : 0) + (h->d.visc ? 2 : 0);
   return 3 * per;
 }
 
@@ -853,13 +864,18 @@ size_t lmc_footprint(const lmc_params *p) {
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)
   if (p->variant) b += 3 * S * 16;  // T before the substep, Delta T, RHS(T)
-  if (p->variant || p->scalar || mode_parallel(g.nmode))
+  if (p->variant || p->scalar || p->visc || mode_parallel(g.nmode))
     b += S * 7 * 8 + (size_t)g.nmode * 5 * 8 + 5 * S * 16 + (size_t)g.my * 40 * 8;  // tables, scratch
   else
     b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8 + (size_t)g.my * 15 * 8;  // Poisson, d/dy rows
   if (p->scalar) {  // Z, RHS(Z), one more spectral and z-physical work buffer
     b += S * 16 + P * 8 + (p->precision == 0 ? S * 16 + Z * 16 : S * 8 + Z * 8);
     b += 2 * (size_t)g.my * 8 + (size_t)g.my * 8 * 4 * g.mgalz;  // mixed sums of the 12th output
+  }
+  if (p->visc) {  // spectral buffers up to 15, z-physical ones up to 14 (18 with the scalar)
+    const size_t have = p->scalar ? 12 : 11, xs = 15 - have, xz = (p->scalar ? 18 : 14) - have;
+    const size_t e = p->precision == 0 ? 16 : 8;
+    b += xs * S * e + xz * Z * e + 3 * (size_t)g.my * 8;
   }
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
   else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;

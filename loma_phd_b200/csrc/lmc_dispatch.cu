@@ -17,7 +17,7 @@ namespace lmc {
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
   bool fft_xstats_##SUF(const Dev &d, const Stats &st, cudaStream_t s);                \
   size_t fft_zsm_##SUF(int n);                                                         \
-  size_t fft_xsm_##SUF(int n, bool zs);                                                \
+  size_t fft_xsm_##SUF(int n, bool zs, bool vs);                                       \
   cudaError_t fft_init_##SUF(int limit);
 LMC_FFT_DECL(a)
 LMC_FFT_DECL(b)
@@ -43,10 +43,10 @@ void launch_xstats(const Dev &d, const Stats &st, cudaStream_t s) {
   if (!fft_xstats_a(d, st, s) && !fft_xstats_b(d, st, s)) fft_xstats_c(d, st, s);
 }
 size_t xphys_smem(const Dev &d) {
-  const bool zs = d.scalar != 0;
-  size_t v = fft_xsm_a(d.mgalx, zs);
-  if (!v) v = fft_xsm_b(d.mgalx, zs);
-  if (!v) v = fft_xsm_c(d.mgalx, zs);
+  const bool zs = d.scalar != 0, vs = d.visc != 0;
+  size_t v = fft_xsm_a(d.mgalx, zs, vs);
+  if (!v) v = fft_xsm_b(d.mgalx, zs, vs);
+  if (!v) v = fft_xsm_c(d.mgalx, zs, vs);
   return v;
 }
 size_t z_smem(const Dev &d) {

@@ -72,8 +72,9 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // current tile is transformed.  A bulk copy moves whole 16-byte units, so
 // for FP32 values the run is widened to an even start and length and the
 // tile is read from offset `lead` in the staging buffer.
-// mode 0: the eight transform inputs of the substep; mode 1 (2014 variant,
-// FP64): T before the substep and Delta T, for d(rho) (lomacte/cross.f:1760-1770)
+// mode 0: the transform inputs of the substep (vbase); mode 1 (2014
+// variant, FP64): T before the substep and Delta T, for d(rho)
+// (lomacte/cross.f:1760-1770)
 template <int N1, int N2, typename CT, typename ST>
 __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles, int mode, int f0) {
   using F = Four<N1, N2, CT>;
@@ -86,10 +87,20 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
   ST *St = (ST *)(smraw + round16(sizeof(CT) * KB * LD));
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
-  const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb;
+  const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb, vb = vbase(d);
   auto src_of = [&](int f) -> const ST * {
     if constexpr (sizeof(ST) == sizeof(double2))
       if (mode == 1) return f == 0 ? d.Told : d.dTs;
+    if (f >= vb) {  // variable viscosity: rho u (for d/dx), the sums, rho w (for d/dz)
+      switch (f - vb) {
+        case 0: return wsb<ST>(d, SB_RU);
+        case 1: return wsb<ST>(d, SB_GYY);
+        case 2: return wsb<ST>(d, SB_RW);
+        case 3: return wsb<ST>(d, SB_G12);
+        case 4: return wsb<ST>(d, SB_G13);
+        default: return wsb<ST>(d, SB_G23);
+      }
+    }
     switch (f) {
       case 0: return wsb<ST>(d, SB_RU);
       case 1: return wsb<ST>(d, SB_RV);
@@ -135,7 +146,9 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
     const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
     const int lead = lead_of(t);
-    const int mult = mode ? 0 : (f == 4 || f == 9) ? 1 : (f == 6 || f == 11) ? 2 : 0;  // i kx, i kz of T, Z
+    // i kx, i kz: of T, Z, and with the variable viscosity of rho u, rho w
+    const int mult = mode ? 0 : f >= vb ? (f == vb ? 1 : f == vb + 2 ? 2 : 0)
+                                        : (f == 4 || f == 9) ? 1 : (f == 6 || f == 11) ? 2 : 0;
     for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
       const int il = idx / gap, g = idx - il * gap;
       W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
@@ -237,8 +250,10 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 // [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
 // current tile is transformed.  ZS: the passive scalar's four more input
 // rows (lap Z, dZ/dx, dZ/dy, dZ/dz), its RHS(Z) row and Delta Z as a
-// twelfth output, packed beside Delta T.
-template <int N1, int N2, typename CT, typename ST, bool ZS>
+// twelfth output, packed beside Delta T.  VS: the variable viscosity's six
+// more input rows (vbase), with T^sigma in the diffusion of T and Z and
+// the variable part of the stress taken off the products rho u_i u_j.
+template <int N1, int N2, typename CT, typename ST, bool ZS, bool VS>
 // FP32 butterflies: at most about 128 registers, so that eight 64-thread
 // blocks (or the same thread count in larger blocks) share an SM
 __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) ? 512 / Geo<N1, N2>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
@@ -246,7 +261,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
-  constexpr int NI = ZS ? 12 : 8, NL = NI / 2, NO = ZS ? 12 : 11, NM = ZS ? 8 : 6;
+  constexpr int VB = ZS ? 12 : 8;  // first viscosity input
+  constexpr int NI = VB + (VS ? 6 : 0), NL = NI / 2, NO = ZS ? 12 : 11, NM = VS ? NMI : ZS ? 8 : 6;
   static_assert(G::XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nkx = d.nkx;  // a multiple of 8 for every supported length
@@ -381,7 +397,14 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
         double tn = T + dtxi * rhp;                                      // cross.f:1626
         double d8 = dtxi * rhp;                                          // cross.f:1627
-        const double rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;   // cross.f:1632-1634
+        double mu = 1.0;                                                 // mu = k = rho D = T^sigma
+        double rhs;
+        if constexpr (VS) {  // branches/loma/src/cross.f:1591-1596
+          mu = pow(T, d.sigma);
+          rhs = -u * tx - v * ty - w * tz + mu * (T * lapT + d.sigma * (tx * tx + ty * ty + tz * tz)) * ipe;
+        } else {
+          rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;              // cross.f:1632-1634
+        }
         if (!d.variant) {  // the 2014 variant keeps RHS(T) spectral (lomacte/cross.f:1452-1456)
           d.rhst[((size_t)y * d.mgalz + z0 + l) * N + pos] = rhs;
           tn = tn + dtg * rhs;                                           // cross.f:1641
@@ -396,13 +419,31 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
             p5.x += s_min[7];
           }
           const double lapZ = p4.x, zx = p4.y, zy = p5.x, zz = p5.y;
-          const double rzs = -u * zx - v * zy - w * zz + T * lapZ / d.pez;
+          double rzs;
+          if constexpr (VS) rzs = -u * zx - v * zy - w * zz + mu * (T * lapZ + d.sigma * (tx * zx + ty * zy + tz * zz)) / d.pez;
+          else rzs = -u * zx - v * zy - w * zz + T * lapZ / d.pez;
           d.rhsz[((size_t)y * d.mgalz + z0 + l) * N + pos] = rzs;
           o[ODZ] = dtxi * rz[j] + dtg * rzs;
         }
         o[OU] = u; o[OV] = v; o[OW] = w;
         o[ORUU] = ru * u; o[ORVV] = rv * v; o[ORWW] = rw * w;              // cross.f:1655-1666
         o[ORUV] = ru * v; o[ORUW] = ru * w; o[ORVW] = rv * w;
+        if constexpr (VS) {  // minus the variable part of the stress, 2 (T^sigma - 1) S_ij / Re
+          const CT *cv = c0 + (size_t)(VB / 2) * ZB * LD;
+          double2 g0 = to_d2(cv[0]), g1 = to_d2(cv[(size_t)ZB * LD]), g2 = to_d2(cv[(size_t)2 * ZB * LD]);
+          if constexpr (MX) {
+            g0.y += s_min[8];
+            g1.y += s_min[9];
+            g2.y += s_min[10];
+          }
+          const double c = d.ire * (mu - 1.0);
+          o[ORUU] -= 2.0 * c * (T * g0.x + ru * tx);
+          o[ORVV] -= 2.0 * c * (T * g0.y + rv * ty);
+          o[ORWW] -= 2.0 * c * (T * g1.x + rw * tz);
+          o[ORUV] -= c * (T * g1.y + ru * ty + rv * tx);
+          o[ORUW] -= c * (T * g2.x + ru * tz + rw * tx);
+          o[ORVW] -= c * (T * g2.y + rv * tz + rw * ty);
+        }
         o[ODRHO] = d.variant ? rhs : (d8 / (T * tn)) / dtb - ab * rhs / (T * T);  // cross.f:1670-1671
         o[ODT] = d8;                                                     // cross.f:1645-1647
         if constexpr (MX) {
@@ -451,7 +492,8 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
       cfy = fmax(cfy, __longlong_as_double((long long)s_vmax) / hy);
       for (int l = 0; l < nzb; l++) {
         // cross.f:1704; with the scalar the larger of the two diffusivities
-        const double DD = (ZS ? fmax(ipe, 1.0 / d.pez) : ipe) * __longlong_as_double((long long)s_tmax[l]);
+        const double tm = __longlong_as_double((long long)s_tmax[l]);
+        const double DD = (ZS ? fmax(ipe, 1.0 / d.pez) : ipe) * (VS ? pow(tm, 1.0 + d.sigma) : tm);
         cft = fmax(cft, 2.0 * DD * ((d.hxalp / 2) * (d.hxalp / 2) + (d.hzbet / 2) * (d.hzbet / 2) + (1.0 / hy) * (1.0 / hy)));
         s_tmax[l] = 0ull;
       }
@@ -670,9 +712,10 @@ struct Launch {
   static size_t zinv_sm(int mz) {
     return round16(sizeof(CT) * ZG::KB * G::LD) + ((size_t)ZG::KB * mz + 2 * E) * sizeof(ST);
   }
-  static size_t xsm(bool zs) { return round16(sizeof(CT) * (zs ? 6 : 4) * G::ZB * G::LD); }
-  static size_t xphys_sm(int nkx, bool zs = false) {
-    return xsm(zs) + (size_t)(zs ? 12 : 8) * G::ZB * nkx * sizeof(ST) + (size_t)(zs ? 2 : 1) * G::ZB * G::N * sizeof(double);
+  static constexpr int nin(bool zs, bool vs) { return (zs ? 12 : 8) + (vs ? 6 : 0); }
+  static size_t xsm(bool zs, bool vs) { return round16(sizeof(CT) * (nin(zs, vs) / 2) * G::ZB * G::LD); }
+  static size_t xphys_sm(int nkx, bool zs = false, bool vs = false) {
+    return xsm(zs, vs) + (size_t)nin(zs, vs) * G::ZB * nkx * sizeof(ST) + (size_t)(zs ? 2 : 1) * G::ZB * G::N * sizeof(double);
   }
   // resident blocks per SM x SMs, for the persistent kernels
   static int grid_for(const void *fn, int threads, size_t smem, int ntiles) {
@@ -705,20 +748,25 @@ struct Launch {
       k_xdrho<N1, N2><<<g, G::XT, (size_t)G::ZB * G::LD * sizeof(double2), s>>>(d);
     }
   }
-  template <bool ZS>
+  template <bool ZS, bool VS>
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
-    const size_t sm = xphys_sm(d.nkx, ZS);
-    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS>, G::XT, sm, ntiles);
-    k_xphys<N1, N2, CT, ST, ZS><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    const size_t sm = xphys_sm(d.nkx, ZS, VS);
+    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS, VS>, G::XT, sm, ntiles);
+    k_xphys<N1, N2, CT, ST, ZS, VS><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
     if constexpr (sizeof(ST) == sizeof(float2)) {
       const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (G::XT / 32);
       k_msum<N1, N2><<<dim3(d.my, n_out(d)), 128, 0, s>>>(d, nslot);
     }
   }
   static void xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
-    if (d.scalar) xphys_zs<true>(d, rk, do_cfl, do_diag, s);
-    else xphys_zs<false>(d, rk, do_cfl, do_diag, s);
+    if (d.visc) {
+      if (d.scalar) xphys_zs<true, true>(d, rk, do_cfl, do_diag, s);
+      else xphys_zs<false, true>(d, rk, do_cfl, do_diag, s);
+    } else {
+      if (d.scalar) xphys_zs<true, false>(d, rk, do_cfl, do_diag, s);
+      else xphys_zs<false, false>(d, rk, do_cfl, do_diag, s);
+    }
   }
   static size_t xstats_sm() { return (size_t)3 * G::ZB * G::LD * sizeof(CT); }
   static void xstats(const Dev &d, const Stats &st, cudaStream_t s) {
@@ -737,8 +785,10 @@ struct Launch {
     if ((e = optin1((const void *)k_zinv<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_zfwd<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xstats<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
-    if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true>, limit)) != cudaSuccess) return e;
-    return optin1((const void *)k_xphys<N1, N2, CT, ST, false>, limit);
+    if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true, true>, limit)) != cudaSuccess) return e;
+    if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, false, true>, limit)) != cudaSuccess) return e;
+    if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true, false>, limit)) != cudaSuccess) return e;
+    return optin1((const void *)k_xphys<N1, N2, CT, ST, false, false>, limit);
   }
 };
 
@@ -790,7 +840,7 @@ inline cudaError_t upload_twiddles() {
   case N: LMC_FFT_FORMS_M(N1, N2, 1, zinv(d, mode, f0, nf, s)) return true;
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
-#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3, zs);
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3, zs, vs);
 #define LMC_FFT_CASE_OPT(N, N1, N2)                                                         \
   if ((e = Launch<N1, N2, double2, double2>::optin(limit)) != cudaSuccess) return e;        \
   if ((e = Launch<N1, N2, float2, float2>::optin(limit)) != cudaSuccess) return e;          \
@@ -821,7 +871,7 @@ inline cudaError_t upload_twiddles() {
   size_t fft_zsm_##SUF(int n) {                                                                   \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_ZS) default: return 0; }                             \
   }                                                                                               \
-  size_t fft_xsm_##SUF(int n, bool zs) {                                                          \
+  size_t fft_xsm_##SUF(int n, bool zs, bool vs) {                                                \
     switch (n) { LMC_FFT_SIZES(LMC_FFT_CASE_XS) default: return 0; }                              \
   }                                                                                               \
   cudaError_t fft_init_##SUF(int limit) {                                                         \

@@ -6,6 +6,8 @@
 
 namespace lmc {
 
+constexpr int NWB = 18;  // work-buffer slots: 12 + 6 transform inputs at most
+
 // Device-side view of one case.
 //   spectral fields   complex [y][kx][kz]            (kz fastest)
 //   z-physical fields complex [y][z][kx]             (kx fastest, z permuted)
@@ -50,11 +52,12 @@ struct Dev {
   // state
   double2 *vor, *phi, *psi, *scal, *Rom, *Rphi;
   double *u00, *v00, *w00, *rf0u, *rf0w, *rf0v;
-  double2 *sb[12];  // spectral work buffers (FP64 form; [7..9] also staging)
-  double2 *zb[12];  // z-physical work buffers (FP64 form)
-  float2 *sbf[12];  // spectral work buffers (mixed form)
-  float2 *zbf[12];  // z-physical work buffers (mixed form)
-  // [11] and the Z slots below exist only with the passive scalar
+  double2 *sb[NWB];  // spectral work buffers (FP64 form; [7..9] also staging)
+  double2 *zb[NWB];  // z-physical work buffers (FP64 form)
+  float2 *sbf[NWB];  // spectral work buffers (mixed form)
+  float2 *zbf[NWB];  // z-physical work buffers (mixed form)
+  // buffers beyond the 11th exist only with the passive scalar or the
+  // variable viscosity
   // Passive scalar Z (scalar = 1): the spectral state, the physical RHS(Z)
   // of the previous substep, and Re*Sc; its wall values live in scal_d[5],
   // scal_d[6].  Z is advanced as T is: derivatives, transforms, physical
@@ -63,16 +66,23 @@ struct Dev {
   double pez;
   double2 *zsc;
   double *rhsz;
+  // Variable viscosity (visc = 1): mu = k = rho D = T^sigma.  The products
+  // rho u_i u_j lose the variable part of the stress 2 (T^sigma - 1) S_ij /
+  // Re, formed per point from six more transform inputs (the symmetric sums
+  // of d(rho u_i)/dx_j, see vbase); T's and Z's diffusion take T^sigma.
+  int visc;
+  double sigma;
   double *rhst;
   // device scalars: [0] Deltat, [1] dtr, [2] time, [3] rhobot, [4] rhotop
   double *scal_d;
   unsigned long long *cflmax;  // [4] max|u|, max|v|/hy, max|w|, max cflT (ordered bits)
   double *rhom;                // [my] plane sums of 1/T
   // Mixed form: the kx = kz = 0 (00) modes bypass the FP32 transforms.
-  //   mi     [8][my]  00 profiles of the transform inputs rho u, rho v,
-  //                   rho w, lap T, dT/dy, T, and with the scalar lap Z,
-  //                   dZ/dy (FP64); zinv drops the 00 coefficient and
-  //                   xphys adds the profile back per point
+  //   mi     [11][my] 00 profiles of the transform inputs rho u, rho v,
+  //                   rho w, lap T, dT/dy, T, with the scalar lap Z,
+  //                   dZ/dy, and with the variable viscosity d(rho v)/dy,
+  //                   d(rho u)/dy, d(rho w)/dy (FP64); zinv drops the 00
+  //                   coefficient and xphys adds the profile back per point
   //   mo_cur [12][my] FP64 plane sums of the 11 (12) transform outputs (their
   //                   exact 00 modes times mgalx*mgalz), read by post1/psi
   //   mo_prev[11][my] the sums of the previous substep: xphys subtracts
@@ -116,12 +126,26 @@ enum {
 
 // Spectral work-buffer roles before / after the transforms.
 // SB_T32 holds an FP32 copy of T for the z transforms of the mixed form;
-// SB_LAPZ, SB_DZDY and SB_Z32 (the same for Z) are used with the scalar.
-enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32, SB_LAPZ, SB_DZDY, SB_Z32 };
+// SB_LAPZ, SB_DZDY and SB_Z32 (the same for Z) are used with the scalar;
+// SB_GYY .. SB_G23 with the variable viscosity: d(rho v)/dy and the sums
+// d(rho u)/dy + d(rho v)/dx, d(rho u)/dz + d(rho w)/dx, d(rho v)/dz +
+// d(rho w)/dy (written by t_sgrad, read by the inverse z transforms).
+enum { SB_RU = 0, SB_RV, SB_RW, SB_LAPT, SB_DTDY, SB_MY, SB_DMY, SB_T32, SB_LAPZ, SB_DZDY, SB_Z32,
+       SB_GYY, SB_G12, SB_G13, SB_G23 };
 enum { OU = 0, OV, OW, ORUU, ORVV, ORWW, ORUV, ORUW, ORVW, ODRHO, ODT, ODZ };
-// transform inputs (8, 12 with the scalar) and outputs (11, 12)
-__host__ __device__ inline int n_in(const Dev &d) { return d.scalar ? 12 : 8; }
+// Transform inputs: 8 (rho u, rho v, rho w, lap T, dT/dx, dT/dy, dT/dz,
+// T), 4 more with the scalar (lap Z, dZ/dx, dZ/dy, dZ/dz), and from vbase
+// 6 more with the variable viscosity (d(rho u)/dx, d(rho v)/dy,
+// d(rho w)/dz, and the SB_G12, SB_G13, SB_G23 sums); outputs 11, 12 with
+// the scalar.
+__host__ __device__ inline int vbase(const Dev &d) { return d.scalar ? 12 : 8; }
+__host__ __device__ inline int n_in(const Dev &d) { return vbase(d) + (d.visc ? 6 : 0); }
 __host__ __device__ inline int n_out(const Dev &d) { return d.scalar ? 12 : 11; }
+// spectral and z-physical work buffers a case allocates
+__host__ __device__ inline int n_sbuf(const Dev &d) { return d.visc ? SB_G23 + 1 : n_out(d); }
+__host__ __device__ inline int n_zbuf(const Dev &d) { return n_in(d) > n_out(d) ? n_in(d) : n_out(d); }
+// 00 profiles held for the mixed form's transform inputs
+constexpr int NMI = 11;
 
 // work-buffer views of the two precisions
 template <typename CT>
@@ -152,6 +176,9 @@ void launch_tder(const Dev &d, cudaStream_t s);
 // passive scalar: Z wall values, dZ/dy, lap Z; and Z += Delta Z
 void launch_zder(const Dev &d, cudaStream_t s);
 void launch_zupd(const Dev &d, cudaStream_t s);
+// variable viscosity: the SB_GYY .. SB_G23 inputs from rho u_i (after
+// launch_assemble)
+void launch_sgrad(const Dev &d, cudaStream_t s);
 // mode 1 (2014 variant): the d(rho) round trip of T and Delta T; f0, nf:
 // only inputs f0 .. f0+nf-1 (nf <= 0: all)
 void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0, int f0 = 0, int nf = 0);

@@ -575,6 +575,110 @@ __global__ void __launch_bounds__(TB) t_zupd(Dev d) {
 }
 
 // ----------------------------------------------------------------------
+// Variable viscosity: the spectral inputs of the strain rates.  In
+// physical space d(u_i)/dx_j = T d(rho u_i)/dx_j + rho u_i dT/dx_j, and the
+// stress needs d(rho u_i)/dx_j only in the symmetric sums; this kernel
+// writes d(rho v)/dy and the three off-diagonal sums (d(rho u)/dx and
+// d(rho w)/dz are formed by the inverse z transforms from rho u and rho w).
+// The y derivatives are deryr2's (cfdiff.f:518-601), as every first y
+// derivative of the substep.  Runs after t_assemble on the same stream;
+// scratch fields 0, 1 and 4 hold the forward halves (2 and 3 belong to
+// t_tder / t_zder on the second stream, 4 is free until the psi solve).
+// The mixed forms take the 00 pencils from the exact FP64 profiles (mi rows
+// 0..2) and leave the 00 profiles of the results in mi rows 8..10.
+// ----------------------------------------------------------------------
+// a pencil of CT values, or (the mixed forms' 00 mode) an FP64 profile
+template <typename CT, int K>
+struct RdP {
+  Rd<CT, K> r;
+  const double *prof;
+  int my, dir, nxt;
+  __device__ __forceinline__ void start(const CT *base, size_t ld, int my_, int dir_, int first, const double *pr) {
+    prof = pr;
+    my = my_;
+    dir = dir_;
+    nxt = first;
+    if (!pr) r.start(base, ld, my_, dir_, first);
+  }
+  __device__ __forceinline__ double2 pop() {
+    if (!prof) return r.pop();
+    const double v = (nxt >= 0 && nxt < my) ? prof[nxt] : 0.0;
+    nxt += dir;
+    return make_double2(v, 0.0);
+  }
+};
+
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool x00 = mixed<CT>() && M.m == 0;
+  double2 *s0 = d.ws[0] + M.m, *s1 = d.ws[1] + M.m, *s2 = d.ws[4] + M.m;
+  const CT *RU = wsb<CT>(d, SB_RU) + M.m, *RV = wsb<CT>(d, SB_RV) + M.m, *RW = wsb<CT>(d, SB_RW) + M.m;
+  const double *pu = x00 ? d.mi : nullptr, *pv = x00 ? d.mi + my : nullptr, *pw = x00 ? d.mi + 2 * my : nullptr;
+  {  // forward halves of d/dy of rho u, rho v, rho w
+    RdP<CT, kq<CT>(4)> ru, rv, rw;
+    ru.start(RU, ld, my, 1, 0, pu);
+    rv.start(RV, ld, my, 1, 0, pv);
+    rw.start(RW, ld, my, 1, 0, pw);
+    Win wu, wv, ww;
+    wu.clear();
+    wv.clear();
+    ww.clear();
+    Hist hu, hv, hw;
+    hu.clear();
+    hv.clear();
+    hw.clear();
+    for (int t = 0; t < 3; t++) {
+      wu.push(ru.pop());
+      wv.push(rv.pop());
+      ww.push(rw.pop());
+    }
+    #pragma unroll 2
+    for (int j = 0; j < my; j++) {
+      wu.push(ru.pop());
+      wv.push(rv.pop());
+      ww.push(rw.pop());
+      s0[(size_t)j * ld] = d1f(d, j, wu, hu);
+      s1[(size_t)j * ld] = d1f(d, j, wv, hv);
+      s2[(size_t)j * ld] = d1f(d, j, ww, hw);
+    }
+  }
+  {  // backward halves, then the sums
+    Rd<double2, 4> r0, r1, r2;
+    r0.start(s0, ld, my, -1, my - 1);
+    r1.start(s1, ld, my, -1, my - 1);
+    r2.start(s2, ld, my, -1, my - 1);
+    RdP<CT, kq<CT>(4)> ru, rv, rw;
+    ru.start(RU, ld, my, -1, my - 1, pu);
+    rv.start(RV, ld, my, -1, my - 1, pv);
+    rw.start(RW, ld, my, -1, my - 1, pw);
+    CT *GYY = wsb<CT>(d, SB_GYY) + M.m, *G12 = wsb<CT>(d, SB_G12) + M.m;
+    CT *G13 = wsb<CT>(d, SB_G13) + M.m, *G23 = wsb<CT>(d, SB_G23) + M.m;
+    Hist hu, hv, hw;
+    hu.clear();
+    hv.clear();
+    hw.clear();
+    #pragma unroll 2
+    for (int j = my - 1; j >= 0; j--) {
+      const double2 du = d1b(d, j, r0.pop(), hu), dv = d1b(d, j, r1.pop(), hv), dw = d1b(d, j, r2.pop(), hw);
+      const double2 u = ru.pop(), v = rv.pop(), w = rw.pop();
+      if (x00) {
+        d.mi[(size_t)8 * my + j] = dv.x;
+        d.mi[(size_t)9 * my + j] = du.x;
+        d.mi[(size_t)10 * my + j] = dw.x;
+      }
+      put(GYY, ld, j, dv);
+      put(G12, ld, j, cadd(du, cik(M.kx, v)));
+      put(G13, ld, j, cadd(cik(M.kz, u), cik(M.kx, w)));
+      put(G23, ld, j, cadd(cik(M.kz, v), dw));
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
 // (6a)-(6b) T update and N_i (cross.f:619-682); rf0u / rf0w get the 00
 // pencils of d(rho uv)/dy and d(rho vw)/dy for the 00 tail.
 // ----------------------------------------------------------------------

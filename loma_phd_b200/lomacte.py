@@ -51,7 +51,7 @@ class lmc_params(ctypes.Structure):
                 ("peclet", ctypes.c_double), ("cfl", ctypes.c_double), ("ncfl", ctypes.c_int),
                 ("dt_mode", ctypes.c_int), ("dt", ctypes.c_double), ("precision", ctypes.c_int),
                 ("device", ctypes.c_int), ("variant", ctypes.c_int), ("scalar", ctypes.c_int),
-                ("schmidt", ctypes.c_double)]
+                ("schmidt", ctypes.c_double), ("visc", ctypes.c_int), ("sigma", ctypes.c_double)]
 
 
 class lmc_diag(ctypes.Structure):
@@ -159,6 +159,8 @@ class Params:
     variant: int = 0          # 0 trunk/lomacte3 (2017), 1 trunk/lomacte (2014)
     scalar: int = 0           # 1: carry a passive scalar Z (lmc_load_scalar_f64)
     schmidt: float = 0.0      # Sc of Z; <= 0: Sc = Pr = 0.7f
+    visc: int = 0             # 1: mu = k = rho D = T^sigma (0: constant viscosity)
+    sigma: float = 0.0        # the exponent, in [0, 4]
 
     def c(self) -> lmc_params:
         return lmc_params(*[getattr(self, f.name) for f in dataclasses.fields(self)])

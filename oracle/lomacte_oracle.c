@@ -446,7 +446,7 @@ struct lmo {
   cplx *w_mx, *w_my, *w_mz, *w_nx, *w_ny, *w_nz, *w_t12, *w_t13, *w_t23, *w_drho, *w_chwk, *w_chwk2;
   /* line buffers [line][kx] complex, line = z + mgalz*y: 8 inputs and 11
    * outputs of the transforms, 12 and 12 with the passive scalar */
-  cplx *ln[12];
+  cplx *ln[18];
   /* passive scalar Z (the extension restated in lomacte_oracle.h): state,
    * spectral work (lap Z, dZ/dx, dZ/dy, dZ/dz, Delta Z), physical RHS(Z) of
    * the previous substep, wall values of its 00 mode, Re*Sc */
@@ -454,6 +454,14 @@ struct lmo {
   double pez, zbot, ztop;
   cplx *zsc, *w_zlap, *w_zx, *w_zy, *w_zz, *w_dz;
   double *rhsz;
+  /* variable viscosity mu = k = rho D = T^vsig (the extension restated in
+   * lomacte_oracle.h): on/off, the exponent, and the six spectral inputs
+   * d(rho u)/dx, d(rho v)/dy, d(rho w)/dz, and the symmetric sums
+   * d(rho u)/dy + d(rho v)/dx, d(rho u)/dz + d(rho w)/dx,
+   * d(rho v)/dz + d(rho w)/dy */
+  int vs;
+  double vsig;
+  cplx *w_g[6];
   /* statistics (cross.f:578-585, 794-812, 1583-1607; escru.f:276-580):
    * st[LMO_NSTAT][my] raw accumulators in the order of the .sta record,
    * sp[nkx][12][nsp][nz1+1] spectra, uner[9] energies of the last
@@ -546,7 +554,8 @@ void lmo_destroy(lmo *o) {
                o->w_nx, o->w_ny, o->w_nz, o->w_t12, o->w_t13, o->w_t23, o->w_drho, o->w_chwk, o->w_chwk2,
                o->rts};
   for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
-  for (int f = 0; f < 12; f++) free(o->ln[f]);
+  for (int f = 0; f < 18; f++) free(o->ln[f]);
+  for (int f = 0; f < 6; f++) free(o->w_g[f]);
   free(o->jsp); free(o->st); free(o->sp);
   free(o->zsc); free(o->w_zlap); free(o->w_zx); free(o->w_zy); free(o->w_zz); free(o->w_dz); free(o->rhsz);
   plan_free(&o->px); plan_free(&o->pz);
@@ -850,16 +859,16 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
   double ab = o->alpha[rk] / o->beta[rk];
 #pragma omp parallel num_threads(o->nthreads)
   {
-    double *ph = malloc(sizeof(double) * mgalx * 12), *out = malloc(sizeof(double) * mgalx * 12);
+    double *ph = malloc(sizeof(double) * mgalx * 18), *out = malloc(sizeof(double) * mgalx * 12);
     cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
     cplx *spec = malloc(sizeof(cplx) * nkx * 12);
 #pragma omp for schedule(static)
     for (long L = 0; L < (long)nlines; L++) {
       int jj = (int)(L / mgalz); /* y index (cross.f:1583) */
-      const int nin = o->scalar ? 12 : 8, nout = o->scalar ? 12 : 11;
-      cplx *sp[12];
+      const int vb = o->scalar ? 12 : 8, nin = vb + (o->vs ? 6 : 0), nout = o->scalar ? 12 : 11;
+      cplx *sp[18];
       for (int f = 0; f < nin; f++) sp[f] = o->ln[f] + (size_t)L * nkx;
-      double *p[12];
+      double *p[18];
       for (int f = 0; f < nin; f++) p[f] = ph + (size_t)f * mgalx;
       for (int f = 0; f < nin; f += 2) xinv2(o, sp[f], sp[f + 1], p[f], p[f + 1], buf, fo);
       double *ru = p[0], *rv = p[1], *rw = p[2], *lapT = p[3], *tx = p[4], *ty = p[5], *tz = p[6], *T = p[7];
@@ -872,6 +881,12 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         double tnext = T[x] + dtxi * rh[x];                            /* cross.f:1625-1629 */
         double d8 = dtxi * rh[x];
         double rhs = -u * tx[x] - v * ty[x] - w * tz[x] + T[x] * lapT[x] / o->peclet; /* cross.f:1631-1637 */
+        double mu = 1.0;
+        if (o->vs) { /* k = T^sigma: branches/loma/src/cross.f:1591-1596 */
+          mu = pow(T[x], o->vsig);
+          const double g2 = tx[x] * tx[x] + ty[x] * ty[x] + tz[x] * tz[x];
+          rhs = -u * tx[x] - v * ty[x] - w * tz[x] + mu * (T[x] * lapT[x] + o->vsig * g2) / o->peclet;
+        }
         rh[x] = rhs;
         tnext = tnext + dtgamma * rhs; /* cross.f:1640-1643 */
         d8 = d8 + dtgamma * rhs;
@@ -881,12 +896,26 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
           double *rz = o->rhsz + (size_t)L * mgalx;
           double dz = dtxi * rz[x];
           double rzs = -u * zx[x] - v * zy[x] - w * zz[x] + T[x] * zl[x] / o->pez;
+          if (o->vs) /* rho D = T^sigma */
+            rzs = -u * zx[x] - v * zy[x] - w * zz[x] +
+                  mu * (T[x] * zl[x] + o->vsig * (tx[x] * zx[x] + ty[x] * zy[x] + tz[x] * zz[x])) / o->pez;
           rz[x] = rzs;
           q[11][x] = dz + dtgamma * rzs;
         }
         q[0][x] = u; q[1][x] = v; q[2][x] = w;
         q[3][x] = ru[x] * u; q[4][x] = rv[x] * v; q[5][x] = rw[x] * w; /* cross.f:1655-1659 */
         q[6][x] = ru[x] * v; q[7][x] = ru[x] * w; q[8][x] = rv[x] * w; /* cross.f:1662-1666 */
+        if (o->vs) { /* minus the variable part of the stress, 2 (T^sigma - 1) S_ij / Re */
+          const double *g0 = p[vb], *g1 = p[vb + 1], *g2 = p[vb + 2], *g3 = p[vb + 3], *g4 = p[vb + 4],
+                       *g5 = p[vb + 5];
+          const double c = o->ire * (mu - 1.0), Tx = T[x];
+          q[3][x] -= 2.0 * c * (Tx * g0[x] + ru[x] * tx[x]);
+          q[4][x] -= 2.0 * c * (Tx * g1[x] + rv[x] * ty[x]);
+          q[5][x] -= 2.0 * c * (Tx * g2[x] + rw[x] * tz[x]);
+          q[6][x] -= c * (Tx * g3[x] + ru[x] * ty[x] + rv[x] * tx[x]);
+          q[7][x] -= c * (Tx * g4[x] + ru[x] * tz[x] + rw[x] * tx[x]);
+          q[8][x] -= c * (Tx * g5[x] + rv[x] * tz[x] + rw[x] * ty[x]);
+        }
         q[9][x] = (d8 / (T[x] * tnext)) / dtbeta - ab * rhs / (T[x] * T[x]); /* cross.f:1669-1673 */
         if (do_cfl) {
           lmx = fmax(lmx, fabs(u)); lmy = fmax(lmy, fabs(v)); lmz = fmax(lmz, fabs(w)); Tmax = fmax(Tmax, T[x]);
@@ -914,7 +943,8 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         }
       }
       if (do_cfl) { /* cross.f:1690-1708 */
-        double DD = (o->scalar ? fmax(1.0 / o->peclet, 1.0 / o->pez) : 1.0 / o->peclet) * Tmax;
+        double DD = (o->scalar ? fmax(1.0 / o->peclet, 1.0 / o->pez) : 1.0 / o->peclet) *
+                    (o->vs ? pow(Tmax, 1.0 + o->vsig) : Tmax);
         double c0 = lmy / o->hy[jj];
         double cT = 2 * DD * ((hxalp / 2) * (hxalp / 2) + (hzbet / 2) * (hzbet / 2) + (1 / o->hy[jj]) * (1 / o->hy[jj]));
 #pragma omp critical
@@ -949,8 +979,8 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
 
 /* foup2: cross.f:1282-1430 */
 static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, int do_cfl, int do_diag,
-                  cplx *in8[12], cplx *out11[12]) {
-  const int nin = o->scalar ? 12 : 8, nout = o->scalar ? 12 : 11;
+                  cplx *in8[18], cplx *out11[12]) {
+  const int nin = (o->scalar ? 12 : 8) + (o->vs ? 6 : 0), nout = o->scalar ? 12 : 11;
   int nkx = o->nkx, mgalz = o->mgalz;
 #pragma omp parallel num_threads(o->nthreads)
   {
@@ -1112,6 +1142,41 @@ static void addstats2(lmo *o, const cplx *u1, const cplx *u2, const cplx *u3) {
 }
 
 /* ------------------------------------------------------------------ */
+/* Variable viscosity (extension): the spectral inputs of the strain   */
+/* rates.  In physical space d(u_i)/dx_j = T d(rho u_i)/dx_j +         */
+/* rho u_i dT/dx_j, so S_ij needs d(rho u_i)/dx_j only in the sums     */
+/* d(rho u_i)/dx_j + d(rho u_j)/dx_i: g[0..2] the diagonal ones        */
+/* (halved), g[3..5] the pairs 12, 13, 23.  y derivatives by deryr2    */
+/* (cfdiff.f:518-601), as every first y derivative of the substep.     */
+/* ------------------------------------------------------------------ */
+static void strain_inputs(lmo *o, const cplx *ru, const cplx *rv, const cplx *rw) {
+  int my = o->my, mz = o->mz;
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 4 * my);
+    cplx *dy = malloc(sizeof(cplx) * 3 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      double kx = o->kxv[m / mz], kz = o->kzv[m % mz];
+      size_t b = (size_t)m * my;
+      deryr2_c(o, ru + b, dy, w1, w2, tt1, tt2);
+      deryr2_c(o, rv + b, dy + my, w1, w2, tt1, tt2);
+      deryr2_c(o, rw + b, dy + 2 * my, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        o->w_g[0][b + j] = I * kx * ru[b + j];
+        o->w_g[1][b + j] = dy[my + j];
+        o->w_g[2][b + j] = I * kz * rw[b + j];
+        o->w_g[3][b + j] = dy[j] + I * kx * rv[b + j];
+        o->w_g[4][b + j] = I * kz * ru[b + j] + I * kx * rw[b + j];
+        o->w_g[5][b + j] = I * kz * rv[b + j] + dy[2 * my + j];
+      }
+    }
+    free(s); free(dy);
+  }
+}
+
+/* ------------------------------------------------------------------ */
 /* One RK3 substep: cross.f:307-1141                                   */
 /* ------------------------------------------------------------------ */
 static void substep(lmo *o, int r /*0..2*/, int ihist) {
@@ -1205,11 +1270,16 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     o->u00wk[j] += dtxi * o->rf0u[j];
     o->w00wk[j] += dtxi * o->rf0w[j];
   }
+  if (o->vs) strain_inputs(o, mxw, myw, mzw);
   const int do_st = o->istati && r == 0 && o->st;
   if (do_st) addstats1(o, mxw, myw, mzw, drho); /* cross.f:578-585 */
   /* (5) foup2 */
   int do_cfl = (r == 0 && o->icfl == 1 && o->dtmode == 0);
-  cplx *in8[12] = {mxw, myw, mzw, nyw, t12, t13, t23, drho, o->w_zlap, o->w_zx, o->w_zy, o->w_zz};
+  cplx *in8[18] = {mxw, myw, mzw, nyw, t12, t13, t23, drho, o->w_zlap, o->w_zx, o->w_zy, o->w_zz};
+  if (o->vs) {
+    const int vb = o->scalar ? 12 : 8;
+    for (int f = 0; f < 6; f++) in8[vb + f] = o->w_g[f];
+  }
   cplx *out11[12] = {mxw, myw, mzw, nxw, nyw, nzw, t12, t13, t23, drho, chwk2, o->w_dz};
   foup2(o, r, dtxi, dtgamma, dtbeta, do_cfl, ihist && r == 0, in8, out11);
   if (do_st) { /* cross.f:796-812 (u, v, w are not changed in between) */
@@ -1709,7 +1779,7 @@ int lmo_step(lmo *o, int nsteps) {
 }
 
 int lmo_set_variant(lmo *o, int variant) {
-  if (!o || variant < 0 || variant > 1) return -1;
+  if (!o || variant < 0 || variant > 1 || (variant && (o->scalar || o->vs))) return -1;
   o->variant = variant;
   return 0;
 }
@@ -1724,6 +1794,19 @@ int lmo_set_scalar(lmo *o, int on, double schmidt) {
   for (size_t i = 0; i < sizeof(b) / sizeof(b[0]); i++)
     if (!*b[i]) *b[i] = xcalloc(ns, sizeof(cplx));
   if (!o->rhsz) o->rhsz = xcalloc(np, 8);
+  return 0;
+}
+
+int lmo_set_viscosity(lmo *o, int on, double sigma) {
+  if (!o || o->variant || (on && !(sigma >= 0.0 && sigma <= 4.0))) return -1;
+  o->vs = on != 0;
+  o->vsig = on ? sigma : 0.0;
+  if (!on) return 0;
+  size_t ns = (size_t)o->nmode * o->my, nl = (size_t)o->mgalz * o->my * o->nkx;
+  for (int f = 0; f < 6; f++)
+    if (!o->w_g[f]) o->w_g[f] = xcalloc(ns, sizeof(cplx));
+  for (int f = 12; f < 18; f++)
+    if (!o->ln[f]) o->ln[f] = xcalloc(nl, sizeof(cplx));
   return 0;
 }
 

@@ -94,6 +94,20 @@ int lmo_set_scalar(lmo *o, int on, double schmidt);
 int lmo_set_scalar_state(lmo *o, const double *z);
 int lmo_get_scalar_state(const lmo *o, double *z);
 
+/* Variable viscosity (an extension restated from branches/loma/src/cross.f:
+ * 1591-1596, 2177-2196): mu = k = rho D = T^sigma.  In physical space
+ *   RHS(T) = -u.grad T + T^sigma (T lap T + sigma |grad T|^2) / Pe,
+ *   RHS(Z) = -u.grad Z + T^sigma (T lap Z + sigma grad T.grad Z) / (Re Sc),
+ * and the products rho u_i u_j lose the variable part of the stress,
+ * 2 (T^sigma - 1) S_ij / Re, with S_ij from d(u_i)/dx_j = T d(rho u_i)/dx_j
+ * + rho u_i dT/dx_j (six more transform inputs); lomacte3's constant-
+ * viscosity terms stay as they are, so that the total viscous force is the
+ * divergence of 2 T^sigma S_ij / Re up to a gradient (which the Omega_y and
+ * phi equations do not see).  The diffusive CFL limit takes T_max^(1+sigma).
+ * sigma in [0, 4]; sigma = 0 reproduces the constant-viscosity substep.
+ * Not for the 2014 variant. */
+int lmo_set_viscosity(lmo *o, int on, double sigma);
+
 /* Coefficient access for tests (band storage row-major [row][band]). */
 void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12,
                    double *prem3_lu, double *dt21, double *dt22, double *fmap);

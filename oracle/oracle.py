@@ -67,6 +67,7 @@ def lib():
         L.lmo_set_scalar.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.lmo_set_scalar_state.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_get_scalar_state.argtypes = [ctypes.c_void_p, _dp]
+        L.lmo_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.lmo_cft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         L.lmo_rft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         _lib = L
@@ -147,6 +148,13 @@ class Oracle:
         a = np.zeros(self.shape, dtype=np.complex128)
         lib().lmo_get_scalar_state(self.h, _p(a.view(np.float64).ravel()))
         return a
+
+    # variable viscosity mu = k = rho D = T^sigma (lomacte_oracle.h)
+    def set_viscosity(self, sigma):
+        """sigma = None: constant viscosity (the lomacte3 substep)."""
+        on = sigma is not None
+        if lib().lmo_set_viscosity(self.h, int(on), float(sigma or 0.0)) != 0:
+            raise ValueError("lmo_set_viscosity rejected its arguments")
 
     # statistics: addstats1/2 and the phys2 sums (cross.f:578-585, 794-812,
     # 1583-1607), resetstats (escru.f:485-580)

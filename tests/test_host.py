@@ -77,3 +77,25 @@ def test_oracle_runs_ic_stably():
         assert np.isfinite(s[k]).all()
     assert abs(d["masst"] - (y[-1] - y[0])) < 0.05
     assert 3.5 < d["dw"] < 4.5
+
+
+def test_params_struct_matches_header():
+    src = open(os.path.join(ROOT, "include", "lomacte_b200.h")).read()
+    body = re.search(r"typedef struct lmc_params \{(.*?)\} lmc_params;", src, flags=re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if decl:
+            names += [n.strip() for n in decl.split(None, 1)[1].split(",")]
+    assert names == [f[0] for f in lm.lmc_params._fields_]
+
+
+def test_footprint_counts_the_viscosity_buffers():
+    base = Params.from_modes(64, 64, 65)
+    vis = Params.from_modes(64, 64, 65, visc=1, sigma=0.7)
+    zp = (64 // 2) * 65 * 96 * 16  # one FP64 z-physical buffer
+    assert lm.footprint(vis) - lm.footprint(base) >= 3 * zp
+    both = Params.from_modes(64, 64, 65, visc=1, sigma=0.7, scalar=1)
+    sc = Params.from_modes(64, 64, 65, scalar=1)
+    assert lm.footprint(both) - lm.footprint(sc) >= 6 * zp

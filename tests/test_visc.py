@@ -1,0 +1,159 @@
+"""Variable viscosity mu = k = rho D = T^sigma on the CPU: the oracle's
+restatement (lmo_set_viscosity) checked without the device.
+
+No lomacte code carries a variable viscosity; the physics follows
+branches/loma/src/cross.f:1591-1596 (conduction) and 2177-2196 (stress
+tau_ij = 2 T^sigma S_ij, isotropic part in the pressure).  The checks:
+
+* sigma = 0 with the extension on reproduces the constant-viscosity
+  substep bit for bit;
+* 1-D state (00 modes only), one substep: the increments of T and of the
+  00 mode of rho u against an independent evaluation of
+  T^sigma (T T'' + sigma T'^2) / Pe - v T' and d/dy((T^sigma - 1) du/dy)/Re;
+* uniform T = T0: the run equals a constant-viscosity run at Re / T0^sigma
+  up to the truncation difference between d/dy(d/dy) and d2/dy2 (the
+  three-dimensional stress, x and z derivatives included);
+* x <-> z mirror: swapping the two periodic directions (u <-> w,
+  Omega_y -> -Omega_y) commutes with the substep to round-off;
+* the passive scalar follows T under the affine map when Re Sc = Pe
+  (both equations carry the same T^sigma terms).
+"""
+import numpy as np
+
+from oracle.oracle import Oracle
+from tests.helpers import FIELDS, case, oracle_for, rel_l2
+
+PR = float(np.float32(0.7))  # Pe = Re*0.7f (main.f:569)
+
+
+def _run(p, y, st, sigma, n=1, sub=None, Re=None, peclet=None):
+    """n RK3 steps (or substep sub) of the oracle; Re, peclet override p's."""
+    if Re is None:
+        o = oracle_for(p, y, st, nthreads=4)
+    else:
+        o = Oracle(p.mgalx, p.mgalz, y, Re, p.alp, p.bet, peclet=peclet, cfl=p.cfl, ncfl=p.ncfl, dtmode=1,
+                   dt0=p.dt, nthreads=4)
+        o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"], 0.0)
+    if sigma is not None:
+        o.set_viscosity(sigma)
+    if sub is not None:
+        o.substep(sub)
+    else:
+        o.step(n)
+    return o.get_state(), o
+
+
+def test_sigma_zero_is_the_constant_viscosity_substep():
+    p, y, st = case(24, 24, 33)
+    a, _ = _run(p, y, st, None, 3)
+    b, _ = _run(p, y, st, 0.0, 3)
+    c, _ = _run(p, y, st, 0.7, 3)
+    for k in FIELDS + ("u00", "v00", "w00"):
+        assert np.array_equal(a[k], b[k]), k
+    assert rel_l2(c["vor"], a["vor"]) > 1e-5 and rel_l2(c["scal"], a["scal"]) > 1e-6
+
+
+def _one_d(p, y, st):
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    for k in ("vor", "phi", "psi", "scal"):
+        keep = s[k][0, 0, :].copy()
+        s[k][:] = 0
+        s[k][0, 0, :] = keep
+    s["u00"] = 0.5 * np.tanh(y / 2)
+    s["v00"] = 0.01 * np.exp(-y ** 2 / 4)
+    return s
+
+
+def test_one_dimensional_increments():
+    sig = 0.7
+    p, y, st = case(24, 24, 65, dt=1e-3)
+    s = _one_d(p, y, st)
+    r0, o = _run(p, y, s, None, sub=0)
+    r1, _ = _run(p, y, s, sig, sub=0)
+    T, ru, rv = s["scal"][0, 0, :].real, s["u00"], s["v00"]
+    h = p.dt * 8.0 / 15.0  # first substep: gamma_1 Deltat, xi_1 = 0
+    pe, ire = p.Re * PR, 1.0 / p.Re
+    Ty, Tyy = o.deryr(T), o.deryyr(T)
+    inner = slice(1, -1)
+    dT = (r1["scal"][0, 0, :].real - T) / h
+    pred = -T * rv * Ty + T ** sig * (T * Tyy + sig * Ty ** 2) / pe
+    assert np.abs(dT - pred)[inner].max() < 1e-8 * np.abs(pred[inner]).max()
+    # the 00 mode of rho u: only the stress differs between the two runs
+    du = (r1["u00"] - r0["u00"]) / h
+    tau = ire * (T ** sig - 1.0) * (T * o.deryr(ru) + ru * Ty)
+    pu = o.deryr(tau)
+    assert np.abs(pu).max() > 1e-4
+    assert np.abs(du - pu)[inner].max() < 1e-8 * np.abs(pu[inner]).max()
+
+
+def test_uniform_temperature_rescales_reynolds():
+    T0, sig, Re = 2.0, 0.7, 160.0
+    p, y, st = case(24, 24, 65, dt=0.002)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    s["scal"][:] = 0
+    s["scal"][0, 0, :] = T0
+    pe = Re * 0.7
+    a, _ = _run(p, y, s, sig, 5, Re=Re, peclet=pe)
+    b, _ = _run(p, y, s, None, 5, Re=Re / T0 ** sig, peclet=pe)
+    c, _ = _run(p, y, s, None, 5, Re=Re, peclet=pe)
+    for k in ("vor", "phi", "u00", "w00"):
+        eff = rel_l2(a[k], c[k])
+        assert eff > 1e-6, k
+        assert rel_l2(a[k], b[k]) < 1e-3 * eff, (k, rel_l2(a[k], b[k]), eff)
+
+
+def _swap(a, sign=1.0):
+    """f(kx, kz) -> f(kz, kx) on the stored half spectrum [kx >= 0][kz][y]
+    (a negative kx taken from the conjugate mode)."""
+    nkx, mz, _ = a.shape
+    nz1 = (mz - 1) // 2
+    assert nkx == nz1 + 1
+    out = np.zeros_like(a)
+    for i in range(nkx):
+        for k in range(mz):
+            b = k if k <= nz1 else k - mz
+            out[i, k] = a[b, i] if b >= 0 else np.conj(a[-b, (-i) % mz])
+    return sign * out
+
+
+def test_mirror_x_z():
+    p, y, st = case(24, 24, 33)
+    s2 = dict(st)
+    s2["vor"] = _swap(st["vor"], -1.0)
+    for k in ("phi", "psi", "scal"):
+        s2[k] = _swap(st[k])
+    s2["u00"], s2["w00"] = st["w00"].copy(), st["u00"].copy()
+    a, _ = _run(p, y, st, 0.7, 3)
+    b, _ = _run(p, y, s2, 0.7, 3)
+    assert rel_l2(_swap(a["vor"], -1.0), b["vor"]) < 1e-12
+    for k in ("phi", "psi", "scal"):
+        assert rel_l2(_swap(a[k]), b[k]) < 1e-12, k
+    assert np.abs(a["u00"] - b["w00"]).max() < 1e-12 * np.abs(a["u00"]).max()
+
+
+def test_scalar_follows_temperature_with_sigma():
+    p, y, st = case(24, 24, 33)
+    o = oracle_for(p, y, st, nthreads=4)
+    T = st["scal"]
+    tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
+    a, b = -tb / (tt - tb), 1.0 / (tt - tb)
+    Z = b * T.copy()
+    Z[0, 0, :] += a
+    o.set_scalar(Z, p.Re * PR / p.Re)
+    o.set_viscosity(0.7)
+    o.step(5)
+    s = o.get_state()
+    pred = b * s["scal"]
+    pred[0, 0, :] += a
+    assert np.abs(o.get_scalar() - pred).max() < 1e-13 * np.abs(pred).max()
+
+
+def test_viscosity_arguments_checked():
+    p, y, st = case(24, 24, 33)
+    o = oracle_for(p, y, st, nthreads=1)
+    for bad in (-0.1, 4.5, float("nan")):
+        try:
+            o.set_viscosity(bad)
+        except ValueError:
+            continue
+        raise AssertionError(f"sigma {bad} accepted")
