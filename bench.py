@@ -3,7 +3,10 @@
 
 Workload (default): nx = nz = 256 Fourier modes (3/2 dealiased: mgalx =
 mgalz = 384), ny = 257 on y = 12 sinh(2 eta)/sinh(2), seeded initial
-condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed Deltat = 0.01.
+condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed Deltat = 0.01,
+Pr = Sc = 0.7, mu = k = rho D = T^0.7 and a passive scalar Z = (T -
+T_bot)/(T_top - T_bot) (both extensions of the lomacte3 substep;
+``--no-scalar --sigma -1`` gives the substep exactly as lomacte3 has it).
 One "step" = one full RK3 step (3 substeps).  The metric is
 (nx*ny*nz/1e6) * steps / seconds, measured for the mixed-precision form
 (the headline value) and the FP64 plain path (reported beside it, with the
@@ -106,14 +109,17 @@ def parse():
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also run an ensemble of this many independent cases of uneven grids (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=500)
-    ap.add_argument("--scalar", action="store_true",
-                    help="carry the passive scalar Z (extension; e2e loads the flow state only)")
-    ap.add_argument("--sigma", type=float, default=None,
-                    help="variable viscosity mu = k = rho D = T^sigma (extension; default: constant)")
+    ap.add_argument("--no-scalar", dest="scalar", action="store_false",
+                    help="without the passive scalar Z (the lomacte3 substep carries none)")
+    ap.add_argument("--sigma", type=float, default=0.7,
+                    help="mu = k = rho D = T^sigma; negative: the constant viscosity of lomacte3")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-only", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.sigma < 0:
+        a.sigma = None
+    return a
 
 
 def peaks():

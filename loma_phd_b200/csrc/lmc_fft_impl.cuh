@@ -397,11 +397,11 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
         const double u = ru * T, v = rv * T, w = rw * T;                // cross.f:1613-1622
         double tn = T + dtxi * rhp;                                      // cross.f:1626
         double d8 = dtxi * rhp;                                          // cross.f:1627
-        double mu = 1.0;                                                 // mu = k = rho D = T^sigma
+        double tsg = 1.0;                                                // mu = k = rho D = T^sigma
         double rhs;
         if constexpr (VS) {  // branches/loma/src/cross.f:1591-1596
-          mu = pow(T, d.sigma);
-          rhs = -u * tx - v * ty - w * tz + mu * (T * lapT + d.sigma * (tx * tx + ty * ty + tz * tz)) * ipe;
+          tsg = exp(d.sigma * log(T));  // T > 0
+          rhs = -u * tx - v * ty - w * tz + tsg * (T * lapT + d.sigma * (tx * tx + ty * ty + tz * tz)) * ipe;
         } else {
           rhs = -u * tx - v * ty - w * tz + T * lapT * ipe;              // cross.f:1632-1634
         }
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
           }
           const double lapZ = p4.x, zx = p4.y, zy = p5.x, zz = p5.y;
           double rzs;
-          if constexpr (VS) rzs = -u * zx - v * zy - w * zz + mu * (T * lapZ + d.sigma * (tx * zx + ty * zy + tz * zz)) / d.pez;
+          if constexpr (VS) rzs = -u * zx - v * zy - w * zz + tsg * (T * lapZ + d.sigma * (tx * zx + ty * zy + tz * zz)) / d.pez;
           else rzs = -u * zx - v * zy - w * zz + T * lapZ / d.pez;
           d.rhsz[((size_t)y * d.mgalz + z0 + l) * N + pos] = rzs;
           o[ODZ] = dtxi * rz[j] + dtg * rzs;
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
             g1.y += s_min[9];
             g2.y += s_min[10];
           }
-          const double c = d.ire * (mu - 1.0);
+          const double c = d.ire * (tsg - 1.0);
           o[ORUU] -= 2.0 * c * (T * g0.x + ru * tx);
           o[ORVV] -= 2.0 * c * (T * g0.y + rv * ty);
           o[ORWW] -= 2.0 * c * (T * g1.x + rw * tz);

@@ -881,11 +881,11 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         double tnext = T[x] + dtxi * rh[x];                            /* cross.f:1625-1629 */
         double d8 = dtxi * rh[x];
         double rhs = -u * tx[x] - v * ty[x] - w * tz[x] + T[x] * lapT[x] / o->peclet; /* cross.f:1631-1637 */
-        double mu = 1.0;
-        if (o->vs) { /* k = T^sigma: branches/loma/src/cross.f:1591-1596 */
-          mu = pow(T[x], o->vsig);
+        double tsg = 1.0; /* mu = k = rho D = T^sigma */
+        if (o->vs) { /* branches/loma/src/cross.f:1591-1596 */
+          tsg = pow(T[x], o->vsig);
           const double g2 = tx[x] * tx[x] + ty[x] * ty[x] + tz[x] * tz[x];
-          rhs = -u * tx[x] - v * ty[x] - w * tz[x] + mu * (T[x] * lapT[x] + o->vsig * g2) / o->peclet;
+          rhs = -u * tx[x] - v * ty[x] - w * tz[x] + tsg * (T[x] * lapT[x] + o->vsig * g2) / o->peclet;
         }
         rh[x] = rhs;
         tnext = tnext + dtgamma * rhs; /* cross.f:1640-1643 */
@@ -898,7 +898,7 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
           double rzs = -u * zx[x] - v * zy[x] - w * zz[x] + T[x] * zl[x] / o->pez;
           if (o->vs) /* rho D = T^sigma */
             rzs = -u * zx[x] - v * zy[x] - w * zz[x] +
-                  mu * (T[x] * zl[x] + o->vsig * (tx[x] * zx[x] + ty[x] * zy[x] + tz[x] * zz[x])) / o->pez;
+                  tsg * (T[x] * zl[x] + o->vsig * (tx[x] * zx[x] + ty[x] * zy[x] + tz[x] * zz[x])) / o->pez;
           rz[x] = rzs;
           q[11][x] = dz + dtgamma * rzs;
         }
@@ -908,7 +908,7 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
         if (o->vs) { /* minus the variable part of the stress, 2 (T^sigma - 1) S_ij / Re */
           const double *g0 = p[vb], *g1 = p[vb + 1], *g2 = p[vb + 2], *g3 = p[vb + 3], *g4 = p[vb + 4],
                        *g5 = p[vb + 5];
-          const double c = o->ire * (mu - 1.0), Tx = T[x];
+          const double c = o->ire * (tsg - 1.0), Tx = T[x];
           q[3][x] -= 2.0 * c * (Tx * g0[x] + ru[x] * tx[x]);
           q[4][x] -= 2.0 * c * (Tx * g1[x] + rv[x] * ty[x]);
           q[5][x] -= 2.0 * c * (Tx * g2[x] + rw[x] * tz[x]);

@@ -105,8 +105,11 @@ def test_one_step_matches_oracle(gpu, grid):
         assert abs(dg[k] - do[k]) <= STEP1_TOL * max(1.0, abs(do[k])), (k, dg[k], do[k])
 
 
-def test_cfl_mode_matches_oracle(gpu):
-    p, y, st = case(24, 24, 33, dt_mode=0, dt=1e-4, ncfl=2)
+@pytest.mark.parametrize("ncfl", [1, 2])
+@pytest.mark.parametrize("family", ["warp", "mode"])
+def test_cfl_mode_matches_oracle(gpu, monkeypatch, ncfl, family):
+    monkeypatch.setenv("LMC_YPATH", family)
+    p, y, st = case(24, 24, 33, dt_mode=0, dt=1e-4, ncfl=ncfl)
     sg, so, dg, do, hg, ho = _run_pair(p, y, st, 5, hist=True)
     for a, b in zip(hg, ho):
         assert a["Deltat"] == b["Deltat"]
