@@ -124,6 +124,21 @@ int pick_chunks(int my, int &C, int &lpm, int &base, int &extra) {
   return LMC_OK;
 }
 
+// The x stage holds a tile's input rows and transform lines in shared
+// memory; with the passive scalar and the variable viscosity the largest
+// lengths need more than the 227 KB a B200 block can have.
+constexpr size_t SMEM_BLOCK_MAX = 227 * 1024;
+bool xstage_fits(const lmc::Grid &g, int scalar, int visc) {
+  lmc::Dev d;
+  std::memset(&d, 0, sizeof(d));
+  d.mgalx = g.mgalx;
+  d.nkx = g.nkx;
+  d.scalar = scalar;
+  d.visc = visc;
+  const size_t need = lmc::xphys_smem(d);
+  return need > 0 && need + 1024 <= SMEM_BLOCK_MAX;
+}
+
 // y kernels: mode-parallel (one thread per mode) once there are enough
 // modes to fill the GPU, warp-per-mode below that.  LMC_YPATH=mode|warp
 // forces one family (tests compare them).
@@ -253,6 +268,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   // x lengths from 24 up; z also 3 (mz = 1: a 2-D run, one kz mode)
   if (g.nkx < 1 || g.mz < 1 || g.mgalx < 24 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz))
     rc = LMC_EINVAL;
+  if (!rc && !xstage_fits(g, p->scalar, p->visc)) rc = LMC_EINVAL;
   if (!rc) rc = pick_chunks(g.my, d.C, d.lpm, d.base, d.extra);
   if (rc) { delete h; return rc; }
   try {
@@ -860,6 +876,7 @@ size_t lmc_footprint(const lmc_params *p) {
   int C, lpm, base, extra;
   if (g.nkx < 1 || g.mz < 1 || pick_chunks(g.my, C, lpm, base, extra) != LMC_OK) return 0;
   if (g.mgalx < 24 || !lmc::fft_supported(g.mgalx) || !lmc::fft_supported(g.mgalz)) return 0;
+  if (!xstage_fits(g, p->scalar, p->visc)) return 0;
   const size_t S = (size_t)g.nmode * g.my, Z = (size_t)g.nkx * g.my * g.mgalz;
   const size_t P = (size_t)g.my * g.mgalz * g.mgalx;
   size_t b = 6 * S * 16 + P * 8;  // state, R_om, R_phi, RHS(T)

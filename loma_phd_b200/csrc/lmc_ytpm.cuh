@@ -587,42 +587,25 @@ __global__ void __launch_bounds__(TB) t_zupd(Dev d) {
 // The mixed forms take the 00 pencils from the exact FP64 profiles (mi rows
 // 0..2) and leave the 00 profiles of the results in mi rows 8..10.
 // ----------------------------------------------------------------------
-// a pencil of CT values, or (the mixed forms' 00 mode) an FP64 profile
-template <typename CT, int K>
-struct RdP {
-  Rd<CT, K> r;
-  const double *prof;
-  int my, dir, nxt;
-  __device__ __forceinline__ void start(const CT *base, size_t ld, int my_, int dir_, int first, const double *pr) {
-    prof = pr;
-    my = my_;
-    dir = dir_;
-    nxt = first;
-    if (!pr) r.start(base, ld, my_, dir_, first);
-  }
-  __device__ __forceinline__ double2 pop() {
-    if (!prof) return r.pop();
-    const double v = (nxt >= 0 && nxt < my) ? prof[nxt] : 0.0;
-    nxt += dir;
-    return make_double2(v, 0.0);
-  }
+// an FP64 profile read as a pencil (imaginary parts zero)
+struct RdM {
+  RdS<4> s;
+  __device__ __forceinline__ void start(const double *p, int my, int dir, int first) { s.start(p, 1, my, dir, first); }
+  __device__ __forceinline__ double2 pop() { return make_double2(s.pop(), 0.0); }
 };
 
-template <typename CT>
-__global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
-  Mode M;
-  if (!mode_of(d, M)) return;
+// d/dy of the three pencils (forward halves into s0, s1, s2, then the
+// backward halves), sink(j, du, dv, dw, u, v, w) per row, j descending;
+// start(reader, field 0..2, direction, first row) opens the readers
+template <typename RT, typename Start, typename Sink>
+__device__ __forceinline__ void sgrad_pass(const Dev &d, size_t ld, double2 *s0, double2 *s1, double2 *s2,
+                                           Start start, Sink sink) {
   const int my = d.my;
-  const size_t ld = d.nmode;
-  const bool x00 = mixed<CT>() && M.m == 0;
-  double2 *s0 = d.ws[0] + M.m, *s1 = d.ws[1] + M.m, *s2 = d.ws[4] + M.m;
-  const CT *RU = wsb<CT>(d, SB_RU) + M.m, *RV = wsb<CT>(d, SB_RV) + M.m, *RW = wsb<CT>(d, SB_RW) + M.m;
-  const double *pu = x00 ? d.mi : nullptr, *pv = x00 ? d.mi + my : nullptr, *pw = x00 ? d.mi + 2 * my : nullptr;
-  {  // forward halves of d/dy of rho u, rho v, rho w
-    RdP<CT, kq<CT>(4)> ru, rv, rw;
-    ru.start(RU, ld, my, 1, 0, pu);
-    rv.start(RV, ld, my, 1, 0, pv);
-    rw.start(RW, ld, my, 1, 0, pw);
+  {
+    RT ru, rv, rw;
+    start(ru, 0, 1, 0);
+    start(rv, 1, 1, 0);
+    start(rw, 2, 1, 0);
     Win wu, wv, ww;
     wu.clear();
     wv.clear();
@@ -646,35 +629,54 @@ __global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
       s2[(size_t)j * ld] = d1f(d, j, ww, hw);
     }
   }
-  {  // backward halves, then the sums
-    Rd<double2, 4> r0, r1, r2;
-    r0.start(s0, ld, my, -1, my - 1);
-    r1.start(s1, ld, my, -1, my - 1);
-    r2.start(s2, ld, my, -1, my - 1);
-    RdP<CT, kq<CT>(4)> ru, rv, rw;
-    ru.start(RU, ld, my, -1, my - 1, pu);
-    rv.start(RV, ld, my, -1, my - 1, pv);
-    rw.start(RW, ld, my, -1, my - 1, pw);
-    CT *GYY = wsb<CT>(d, SB_GYY) + M.m, *G12 = wsb<CT>(d, SB_G12) + M.m;
-    CT *G13 = wsb<CT>(d, SB_G13) + M.m, *G23 = wsb<CT>(d, SB_G23) + M.m;
-    Hist hu, hv, hw;
-    hu.clear();
-    hv.clear();
-    hw.clear();
-    #pragma unroll 2
-    for (int j = my - 1; j >= 0; j--) {
-      const double2 du = d1b(d, j, r0.pop(), hu), dv = d1b(d, j, r1.pop(), hv), dw = d1b(d, j, r2.pop(), hw);
-      const double2 u = ru.pop(), v = rv.pop(), w = rw.pop();
-      if (x00) {
-        d.mi[(size_t)8 * my + j] = dv.x;
-        d.mi[(size_t)9 * my + j] = du.x;
-        d.mi[(size_t)10 * my + j] = dw.x;
-      }
-      put(GYY, ld, j, dv);
-      put(G12, ld, j, cadd(du, cik(M.kx, v)));
-      put(G13, ld, j, cadd(cik(M.kz, u), cik(M.kx, w)));
-      put(G23, ld, j, cadd(cik(M.kz, v), dw));
-    }
+  Rd<double2, 3> r0, r1, r2;
+  r0.start(s0, ld, my, -1, my - 1);
+  r1.start(s1, ld, my, -1, my - 1);
+  r2.start(s2, ld, my, -1, my - 1);
+  RT ru, rv, rw;
+  start(ru, 0, -1, my - 1);
+  start(rv, 1, -1, my - 1);
+  start(rw, 2, -1, my - 1);
+  Hist hu, hv, hw;
+  hu.clear();
+  hv.clear();
+  hw.clear();
+  #pragma unroll 2
+  for (int j = my - 1; j >= 0; j--) {
+    const double2 du = d1b(d, j, r0.pop(), hu), dv = d1b(d, j, r1.pop(), hv), dw = d1b(d, j, r2.pop(), hw);
+    sink(j, du, dv, dw, ru.pop(), rv.pop(), rw.pop());
+  }
+}
+
+template <typename CT>
+__global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  double2 *s0 = d.ws[0] + M.m, *s1 = d.ws[1] + M.m, *s2 = d.ws[4] + M.m;
+  const CT *src[3] = {wsb<CT>(d, SB_RU) + M.m, wsb<CT>(d, SB_RV) + M.m, wsb<CT>(d, SB_RW) + M.m};
+  CT *GYY = wsb<CT>(d, SB_GYY) + M.m, *G12 = wsb<CT>(d, SB_G12) + M.m;
+  CT *G13 = wsb<CT>(d, SB_G13) + M.m, *G23 = wsb<CT>(d, SB_G23) + M.m;
+  sgrad_pass<Rd<CT, kq<CT>(3)>>(
+      d, ld, s0, s1, s2, [&](auto &r, int f, int dir, int first) { r.start(src[f], ld, my, dir, first); },
+      [&](int j, double2 du, double2 dv, double2 dw, double2 u, double2 v, double2 w) {
+        put(GYY, ld, j, dv);
+        put(G12, ld, j, cadd(du, cik(M.kx, v)));
+        put(G13, ld, j, cadd(cik(M.kz, u), cik(M.kx, w)));
+        put(G23, ld, j, cadd(cik(M.kz, v), dw));
+      });
+  if constexpr (mixed<CT>()) {
+    if (M.m != 0) return;
+    // the exact 00 profiles: from mi rows 0..2 into mi rows 8..10 (the FP32
+    // buffers' 00 coefficients are not read: the transforms drop them)
+    sgrad_pass<RdM>(
+        d, ld, s0, s1, s2, [&](auto &r, int f, int dir, int first) { r.start(d.mi + (size_t)f * my, my, dir, first); },
+        [&](int j, double2 du, double2 dv, double2 dw, double2, double2, double2) {
+          d.mi[(size_t)8 * my + j] = dv.x;
+          d.mi[(size_t)9 * my + j] = du.x;
+          d.mi[(size_t)10 * my + j] = dw.x;
+        });
   }
 }
 

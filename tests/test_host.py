@@ -99,3 +99,13 @@ def test_footprint_counts_the_viscosity_buffers():
     both = Params.from_modes(64, 64, 65, visc=1, sigma=0.7, scalar=1)
     sc = Params.from_modes(64, 64, 65, scalar=1)
     assert lm.footprint(both) - lm.footprint(sc) >= 6 * zp
+
+
+def test_viscosity_x_grid_limit():
+    # the x stage's shared memory: mgalx 768 with the scalar, 1152 without
+    ok = Params.from_modes(512, 1, 65, visc=1, sigma=0.7, scalar=1)
+    big = Params.from_modes(768, 1, 65, visc=1, sigma=0.7, scalar=1)
+    big_ns = Params.from_modes(768, 1, 65, visc=1, sigma=0.7)
+    assert lm.footprint(ok) > 0 and lm.footprint(big_ns) > 0
+    assert lm.footprint(big) == 0
+    assert lm.footprint(Params.from_modes(768, 1, 65, scalar=1)) > 0
