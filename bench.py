@@ -74,15 +74,18 @@ ALGO = {
     "psi": lambda S, Z, P, w, sc, vs: S * 16 + S * w + S * 7 * 8 // 2,
 }
 
-# DRAM bytes (read + write) per launch measured by ncu (full-set capture of
-# the 256x65x256 case of this workload, one launch per kernel).  Traffic
+# DRAM bytes (read + write) per launch measured by ncu (full-set captures
+# of the 256x65x256 case of each workload, one launch per kernel).  Traffic
 # grows in proportion to ny at fixed x/z sizes, so for nx = nz = 256 it is
 # scaled by ny/65; other sizes, and kernels not captured, report null.
-NCU_TRAFFIC_256x65 = {  # zinv: its two launches of a substep together
-    "zinv": 553.0e6, "xphys": 1064.5e6, "zfwd": 903.9e6, "post1": 609.9e6, "post2": 956.2e6,
-}
-NCU_TRAFFIC_MIXED_256x65 = {
-    "zinv": 217.7e6, "xphys": 584.0e6, "zfwd": 433.6e6, "post1": 410.3e6, "post2": 768.8e6,
+# Keyed by (FP64 form, passive scalar, variable viscosity).
+NCU_TRAFFIC_256x65 = {
+    (True, 0, 0): {  # zinv: its two launches of a substep together
+        "zinv": 553.0e6, "xphys": 1064.5e6, "zfwd": 903.9e6, "post1": 609.9e6, "post2": 956.2e6},
+    (False, 0, 0): {
+        "zinv": 217.7e6, "xphys": 584.0e6, "zfwd": 433.6e6, "post1": 410.3e6, "post2": 768.8e6},
+    (True, 1, 1): {"xphys": 1786.2e6},
+    (False, 1, 1): {"xphys": 1027.4e6},
 }
 
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
@@ -380,8 +383,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     # chain, so the fractions can sum above 1
     share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES if prof[k][1]}
     traffic = None
-    table = NCU_TRAFFIC_256x65 if prec == 0 else NCU_TRAFFIC_MIXED_256x65
-    if a.nx == 256 and a.nz == 256 and top in table and not sc and not vs:
+    table = NCU_TRAFFIC_256x65.get((prec == 0, sc, vs), {}) if prec in (0, 1) else {}
+    if a.nx == 256 and a.nz == 256 and top in table:
         traffic = table[top] * a.ny / 65.0
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,

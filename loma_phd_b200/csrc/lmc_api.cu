@@ -415,7 +415,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   if (d.prec) {
     // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
     d.mpart_ld = 4 * g.mgalz;
-    if ((rc = dalloc(h, &d.mi, (size_t)lmc::NMI * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
+    if ((d.visc && (rc = dalloc(h, &d.vscr, (size_t)3 * g.my))) || (rc = dalloc(h, &d.mi, (size_t)lmc::NMI * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &h->mo[1], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &d.mpart, (size_t)12 * g.my * d.mpart_ld))) {
       lmc_destroy(h);
@@ -892,7 +892,7 @@ size_t lmc_footprint(const lmc_params *p) {
   if (p->visc) {  // spectral buffers up to 15, z-physical ones up to 14 (18 with the scalar)
     const size_t have = p->scalar ? 12 : 11, xs = 15 - have, xz = (p->scalar ? 18 : 14) - have;
     const size_t e = p->precision == 0 ? 16 : 8;
-    b += xs * S * e + xz * Z * e + 3 * (size_t)g.my * 8;
+    b += xs * S * e + xz * Z * e + 3 * (size_t)g.my * (8 + 16);  // + mixed 00 profiles and their scratch
   }
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
   else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;

@@ -72,6 +72,7 @@ struct Dev {
   // of d(rho u_i)/dx_j, see vbase); T's and Z's diffusion take T^sigma.
   int visc;
   double sigma;
+  double2 *vscr;  // [3][my] scratch of the mixed forms' exact 00 strain-rate inputs
   double *rhst;
   // device scalars: [0] Deltat, [1] dtr, [2] time, [3] rhobot, [4] rhotop
   double *scal_d;

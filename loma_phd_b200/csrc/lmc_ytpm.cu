@@ -35,7 +35,10 @@ void tpm_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *ou
 }
 void launch_zder(const Dev &d, cudaStream_t s) { LMC_TPM(t_zder, d); }
 void launch_zupd(const Dev &d, cudaStream_t s) { LMC_TPM(t_zupd, d); }
-void launch_sgrad(const Dev &d, cudaStream_t s) { LMC_TPM(t_sgrad, d); }
+void launch_sgrad(const Dev &d, cudaStream_t s) {  // mixed: one more block for the exact 00 profiles
+  if (d.prec) tpm::t_sgrad<float2><<<tgrid(d) + 1, tpm::TB, 0, s>>>(d);
+  else tpm::t_sgrad<double2><<<tgrid(d), tpm::TB, 0, s>>>(d);
+}
 void tpm_cfl14(const Dev &d, int do_cfl, cudaStream_t s) { tpm::k_cfl14<<<1, 32, 0, s>>>(d, do_cfl); }
 void tpm_psi00_14(const Dev &d, int rk, cudaStream_t s) { tpm::k_psi00_14<<<1, 32, 0, s>>>(d, rk); }
 

@@ -584,8 +584,8 @@ __global__ void __launch_bounds__(TB) t_zupd(Dev d) {
 // derivative of the substep.  Runs after t_assemble on the same stream;
 // scratch fields 0, 1 and 4 hold the forward halves (2 and 3 belong to
 // t_tder / t_zder on the second stream, 4 is free until the psi solve).
-// The mixed forms take the 00 pencils from the exact FP64 profiles (mi rows
-// 0..2) and leave the 00 profiles of the results in mi rows 8..10.
+// The mixed forms also form the 00 profiles of the results exactly, from
+// the FP64 profiles of rho u_i (mi rows 0..2) into mi rows 8..10.
 // ----------------------------------------------------------------------
 // an FP64 profile read as a pencil (imaginary parts zero)
 struct RdM {
@@ -648,11 +648,29 @@ __device__ __forceinline__ void sgrad_pass(const Dev &d, size_t ld, double2 *s0,
   }
 }
 
+// The mixed forms launch one block more than the pencils need: its first
+// thread runs the exact 00 profiles (mi rows 0..2 into rows 8..10, scratch
+// vscr) beside the pencils; the FP32 buffers' 00 coefficients are not read
+// (the transforms drop them).
 template <typename CT>
 __global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
+  const int my = d.my;
+  if constexpr (mixed<CT>()) {
+    if (blockIdx.x == gridDim.x - 1) {
+      if (threadIdx.x != 0) return;
+      sgrad_pass<RdM>(
+          d, 1, d.vscr, d.vscr + my, d.vscr + 2 * my,
+          [&](auto &r, int f, int dir, int first) { r.start(d.mi + (size_t)f * my, my, dir, first); },
+          [&](int j, double2 du, double2 dv, double2 dw, double2, double2, double2) {
+            d.mi[(size_t)8 * my + j] = dv.x;
+            d.mi[(size_t)9 * my + j] = du.x;
+            d.mi[(size_t)10 * my + j] = dw.x;
+          });
+      return;
+    }
+  }
   Mode M;
   if (!mode_of(d, M)) return;
-  const int my = d.my;
   const size_t ld = d.nmode;
   double2 *s0 = d.ws[0] + M.m, *s1 = d.ws[1] + M.m, *s2 = d.ws[4] + M.m;
   const CT *src[3] = {wsb<CT>(d, SB_RU) + M.m, wsb<CT>(d, SB_RV) + M.m, wsb<CT>(d, SB_RW) + M.m};
@@ -666,18 +684,6 @@ __global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
         put(G13, ld, j, cadd(cik(M.kz, u), cik(M.kx, w)));
         put(G23, ld, j, cadd(cik(M.kz, v), dw));
       });
-  if constexpr (mixed<CT>()) {
-    if (M.m != 0) return;
-    // the exact 00 profiles: from mi rows 0..2 into mi rows 8..10 (the FP32
-    // buffers' 00 coefficients are not read: the transforms drop them)
-    sgrad_pass<RdM>(
-        d, ld, s0, s1, s2, [&](auto &r, int f, int dir, int first) { r.start(d.mi + (size_t)f * my, my, dir, first); },
-        [&](int j, double2 du, double2 dv, double2 dw, double2, double2, double2) {
-          d.mi[(size_t)8 * my + j] = dv.x;
-          d.mi[(size_t)9 * my + j] = du.x;
-          d.mi[(size_t)10 * my + j] = dw.x;
-        });
-  }
 }
 
 // ----------------------------------------------------------------------
