@@ -47,6 +47,16 @@ struct Geo {
   static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
 };
 
+// Threads of an x-stage block.  With the variable viscosity the x stage
+// stages 14 or 18 inputs and transforms 7 or 9 lines per z line, so shared
+// memory admits half the blocks per SM: those blocks get twice the
+// threads (at most four warps, the partial-sum slots of the mixed form).
+template <int N1, int N2, bool VS>
+struct XGeo {
+  static constexpr int XT = VS ? (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128) : Geo<N1, N2>::XT;
+  static constexpr int PT = (Geo<N1, N2>::ZB * Geo<N1, N2>::N + XT - 1) / XT;
+};
+
 // z-transform blocks by butterfly type: twice as many kx lines for FP32
 // butterflies (and FP32 storage), so that every strided z row moves the same
 // number of bytes; FP64 butterflies keep the FP64 block, whose shared-memory
@@ -256,14 +266,14 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 template <int N1, int N2, typename CT, typename ST, bool ZS, bool VS>
 // FP32 butterflies: at most about 128 registers, so that eight 64-thread
 // blocks (or the same thread count in larger blocks) share an SM
-__global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) ? 512 / Geo<N1, N2>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
+__global__ void __launch_bounds__(XGeo<N1, N2, VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
-  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = G::PT;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, VS>::PT, XT = XGeo<N1, N2, VS>::XT;
   constexpr int VB = ZS ? 12 : 8;  // first viscosity input
   constexpr int NI = VB + (VS ? 6 : 0), NL = NI / 2, NO = ZS ? 12 : 11, NM = VS ? NMI : ZS ? 8 : 6;
-  static_assert(G::XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
+  static_assert(XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nkx = d.nkx;  // a multiple of 8 for every supported length
   CT *W = (CT *)smraw;                                        // NL buffers x ZB lines x LD
@@ -475,7 +485,7 @@ __global__ void __launch_bounds__(Geo<N1, N2>::XT, sizeof(CT) == sizeof(float2) 
       if ((threadIdx.x & 31) == 0) atomicAdd(d.rhom + y, rs);
     }
     if constexpr (MX) {  // FP64 partial plane sums, one slot per (tile, warp)
-      const int slot = (z0 / ZB) * (G::XT / 32) + (threadIdx.x >> 5);
+      const int slot = (z0 / ZB) * (XT / 32) + (threadIdx.x >> 5);
 #pragma unroll
       for (int q = 0; q < NO; q++) {
         const double v = warp_sum(acc[q]);
@@ -752,10 +762,11 @@ struct Launch {
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
     const size_t sm = xphys_sm(d.nkx, ZS, VS);
-    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS, VS>, G::XT, sm, ntiles);
-    k_xphys<N1, N2, CT, ST, ZS, VS><<<g, G::XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    constexpr int XT = XGeo<N1, N2, VS>::XT;
+    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS, VS>, XT, sm, ntiles);
+    k_xphys<N1, N2, CT, ST, ZS, VS><<<g, XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
     if constexpr (sizeof(ST) == sizeof(float2)) {
-      const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (G::XT / 32);
+      const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (XT / 32);
       k_msum<N1, N2><<<dim3(d.my, n_out(d)), 128, 0, s>>>(d, nslot);
     }
   }
