@@ -84,8 +84,8 @@ NCU_TRAFFIC_256x65 = {
         "zinv": 553.0e6, "xphys": 1064.5e6, "zfwd": 903.9e6, "post1": 609.9e6, "post2": 956.2e6},
     (False, 0, 0): {
         "zinv": 217.7e6, "xphys": 584.0e6, "zfwd": 433.6e6, "post1": 410.3e6, "post2": 768.8e6},
-    (True, 1, 1): {"xphys": 1786.2e6},
-    (False, 1, 1): {"xphys": 1027.4e6},
+    (True, 1, 1): {"xphys": 1791.0e6},
+    (False, 1, 1): {"xphys": 1026.2e6},
 }
 
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",

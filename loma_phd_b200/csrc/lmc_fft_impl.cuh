@@ -47,13 +47,14 @@ struct Geo {
   static constexpr int PT = (ZB * N + XT - 1) / XT;         // physical points per thread
 };
 
-// Threads of an x-stage block.  With the variable viscosity the x stage
-// stages 14 or 18 inputs and transforms 7 or 9 lines per z line, so shared
-// memory admits half the blocks per SM: those blocks get twice the
-// threads (at most four warps, the partial-sum slots of the mixed form).
-template <int N1, int N2, bool VS>
+// Threads of an x-stage block.  With the passive scalar or the variable
+// viscosity the x stage stages 12 to 18 inputs and transforms 6 to 9 lines
+// per z line, so shared memory admits fewer blocks per SM: those blocks
+// get twice the threads (at most four warps, the partial-sum slots of the
+// mixed form).
+template <int N1, int N2, bool WIDE>
 struct XGeo {
-  static constexpr int XT = VS ? (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128) : Geo<N1, N2>::XT;
+  static constexpr int XT = WIDE ? (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128) : Geo<N1, N2>::XT;
   static constexpr int PT = (Geo<N1, N2>::ZB * Geo<N1, N2>::N + XT - 1) / XT;
 };
 
@@ -266,11 +267,11 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 template <int N1, int N2, typename CT, typename ST, bool ZS, bool VS>
 // FP32 butterflies: at most about 128 registers, so that eight 64-thread
 // blocks (or the same thread count in larger blocks) share an SM
-__global__ void __launch_bounds__(XGeo<N1, N2, VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
+__global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, ZS || VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
-  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, VS>::PT, XT = XGeo<N1, N2, VS>::XT;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, ZS || VS>::PT, XT = XGeo<N1, N2, ZS || VS>::XT;
   constexpr int VB = ZS ? 12 : 8;  // first viscosity input
   constexpr int NI = VB + (VS ? 6 : 0), NL = NI / 2, NO = ZS ? 12 : 11, NM = VS ? NMI : ZS ? 8 : 6;
   static_assert(XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
@@ -762,7 +763,7 @@ struct Launch {
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
     const size_t sm = xphys_sm(d.nkx, ZS, VS);
-    constexpr int XT = XGeo<N1, N2, VS>::XT;
+    constexpr int XT = XGeo<N1, N2, ZS || VS>::XT;
     const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS, VS>, XT, sm, ntiles);
     k_xphys<N1, N2, CT, ST, ZS, VS><<<g, XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
     if constexpr (sizeof(ST) == sizeof(float2)) {
