@@ -130,6 +130,21 @@ int lmc_get_state_f32(lmc_handle *h, float *vor, float *phi, float *psi,
 int lmc_load_scalar_f64(lmc_handle *h, const double *z);
 int lmc_get_scalar_f64(lmc_handle *h, double *z);
 
+/* Physical fields of the current state on chosen y planes: the quantities
+ * tofis_loma writes (escrphys, trunk/tofis_loma/src/escru.f:11-314; y work
+ * of uvw.f:7-94), formed from the solver's own rho u_i, i.e. Lapvdvhom with
+ * the wall conditions of the substep (cross.f:315-349, 365-499) rather than
+ * tofis_loma's own Robin-condition solve for rho v: for each 1-based row
+ * jplanes[p] the mgalz x mgalx planes (x fastest, natural order) of u, v, w,
+ * T, omega_x, omega_y, omega_z and, with the scalar, Z, in that order:
+ * out[p][q][z][x], q < 7 (8).  omega = curl(T rho u) = T curl(rho u) +
+ * grad T x rho u, per point.  Computed in FP64 whatever the precision form,
+ * on device buffers of its own (about 11 spectral and 10 z-padded fields,
+ * freed before returning); the state and its RK3 memory are not changed.
+ * Not for the 2014 variant.  Replaces tofis_loma's main program
+ * (trunk/tofis_loma/src/main.f:14) for a restart the library holds. */
+int lmc_physical_f64(lmc_handle *h, int nplanes, const int *jplanes, double *out);
+
 /* Variable viscosity (lmc_params.visc = 1): mu = k = rho D = T^sigma.  The
  * lomacte3 substep keeps its constant-viscosity terms; in physical space
  *   RHS(T) = -u.grad T + T^sigma (T lap T + sigma |grad T|^2) / Pe

@@ -522,6 +522,67 @@ int lmc_get_state_f64(lmc_handle *h, double *vor, double *phi, double *psi, doub
   return h->err;
 }
 
+int lmc_physical_f64(lmc_handle *h, int nplanes, const int *jplanes, double *out) {
+  if (!h || nplanes < 0 || (nplanes > 0 && (!jplanes || !out)) || h->d.variant) return LMC_EINVAL;
+  if (h->err) return h->err;
+  const lmc::Dev &d = h->d;
+  for (int p = 0; p < nplanes; p++)
+    if (jplanes[p] < 1 || jplanes[p] > d.my) return LMC_EINVAL;
+  if (nplanes == 0) return LMC_OK;
+  LMC_CK(cudaSetDevice(h->p.device));
+  // an FP64 view of the case on buffers of its own: the state and its RK3
+  // memory are read, never written
+  lmc::Dev e = d;
+  e.prec = 0;
+  e.fft64 = 0;
+  const int nf = d.scalar ? 11 : 10, nq = d.scalar ? 8 : 7;
+  const size_t ns = (size_t)d.nmode * d.my, nzp = (size_t)d.nkx * d.my * d.mgalz;
+  const size_t nout = (size_t)nplanes * nq * d.mgalz * d.mgalx;
+  std::vector<void *> tmp;
+  int rc = LMC_OK;
+  auto get = [&](void **q, size_t bytes) {
+    if (rc) return;
+    const cudaError_t err = cudaMallocAsync(q, bytes, h->s);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      rc = err == cudaErrorMemoryAllocation ? LMC_ENOMEM : LMC_ECUDA;
+      *q = nullptr;
+      return;
+    }
+    tmp.push_back(*q);
+  };
+  for (int f = 0; f < lmc::NWB; f++) {
+    e.sb[f] = e.zb[f] = nullptr;
+    e.sbf[f] = e.zbf[f] = nullptr;
+  }
+  for (int q = 0; q < nf; q++) get((void **)&e.sb[lmc::xslot(q)], ns * sizeof(double2));
+  get((void **)&e.sb[lmc::SB_MY], ns * sizeof(double2));
+  get((void **)&e.sb[lmc::SB_DMY], ns * sizeof(double2));
+  for (int q = 0; q < nf; q++) get((void **)&e.zb[q], nzp * sizeof(double2));
+  for (int k = 0; k < 4; k++) get((void **)&e.ws[k], ns * sizeof(double2));
+  int *jrow = nullptr;
+  double *od = nullptr;
+  get((void **)&jrow, (size_t)nplanes * sizeof(int));
+  get((void **)&od, nout * sizeof(double));
+  std::vector<int> j0(nplanes);
+  for (int p = 0; p < nplanes; p++) j0[p] = jplanes[p] - 1;
+  if (!rc) {
+    cudaError_t err = cudaMemcpyAsync(jrow, j0.data(), j0.size() * sizeof(int), cudaMemcpyHostToDevice, h->s);
+    if (err == cudaSuccess) {
+      lmc::launch_lapv(e, h->s);
+      lmc::launch_xprep(e, h->s);
+      lmc::launch_zinv(e, h->s, 2, 0, nf);
+      lmc::launch_xexport(e, jrow, nplanes, nf, od, h->s);
+      err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpyAsync(out, od, nout * sizeof(double), cudaMemcpyDeviceToHost, h->s);
+    if (err != cudaSuccess) rc = LMC_ECUDA;
+  }
+  for (void *q : tmp) cudaFreeAsync(q, h->s);
+  if (cudaStreamSynchronize(h->s) != cudaSuccess && !rc) rc = LMC_ECUDA;
+  return rc;
+}
+
 int lmc_load_scalar_f64(lmc_handle *h, const double *z) {
   if (!h || !z || !h->d.scalar) return LMC_EINVAL;
   if (h->err) return h->err;

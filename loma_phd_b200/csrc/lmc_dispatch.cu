@@ -16,6 +16,7 @@ namespace lmc {
   bool fft_xdrho_##SUF(const Dev &d, cudaStream_t s);                                  \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s); \
   bool fft_xstats_##SUF(const Dev &d, const Stats &st, cudaStream_t s);                \
+  bool fft_xexport_##SUF(const Dev &d, const int *jrow, int nplanes, int nf, double *out, cudaStream_t s); \
   size_t fft_zsm_##SUF(int n);                                                         \
   size_t fft_xsm_##SUF(int n, bool zs, bool vs);                                       \
   cudaError_t fft_init_##SUF(int limit);
@@ -38,6 +39,10 @@ void launch_xdrho(const Dev &d, cudaStream_t s) {
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
   if (!fft_xphys_a(d, rk, do_cfl, do_diag, s) && !fft_xphys_b(d, rk, do_cfl, do_diag, s))
     fft_xphys_c(d, rk, do_cfl, do_diag, s);
+}
+void launch_xexport(const Dev &d, const int *jrow, int nplanes, int nf, double *out, cudaStream_t s) {
+  if (!fft_xexport_a(d, jrow, nplanes, nf, out, s) && !fft_xexport_b(d, jrow, nplanes, nf, out, s))
+    fft_xexport_c(d, jrow, nplanes, nf, out, s);
 }
 void launch_xstats(const Dev &d, const Stats &st, cudaStream_t s) {
   if (!fft_xstats_a(d, st, s) && !fft_xstats_b(d, st, s)) fft_xstats_c(d, st, s);

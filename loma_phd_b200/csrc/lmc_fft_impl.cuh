@@ -85,7 +85,8 @@ __device__ __forceinline__ int kz_pad(const Dev &d, int k) { return k <= d.nz1 ?
 // tile is read from offset `lead` in the staging buffer.
 // mode 0: the transform inputs of the substep (vbase); mode 1 (2014
 // variant, FP64): T before the substep and Delta T, for d(rho)
-// (lomacte/cross.f:1760-1770)
+// (lomacte/cross.f:1760-1770); mode 2 (physical-field export, FP64): the
+// export inputs, written in natural z order
 template <int N1, int N2, typename CT, typename ST>
 __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles, int mode, int f0) {
   using F = Four<N1, N2, CT>;
@@ -100,8 +101,10 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
   __shared__ int s_ok;
   const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb, vb = vbase(d);
   auto src_of = [&](int f) -> const ST * {
-    if constexpr (sizeof(ST) == sizeof(double2))
+    if constexpr (sizeof(ST) == sizeof(double2)) {
       if (mode == 1) return f == 0 ? d.Told : d.dTs;
+      if (mode == 2) return wsb<ST>(d, xslot(f));
+    }
     if (f >= vb) {  // variable viscosity: rho u (for d/dx), the sums, rho w (for d/dz)
       switch (f - vb) {
         case 0: return wsb<ST>(d, SB_RU);
@@ -185,7 +188,10 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.nkx + i0;
     for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
       const int z = idx / KB, il = idx - z * KB;
-      if (il < nb) dst[(size_t)z * d.nkx + il] = ccvt<ST>(W[il * LD + F::sk(z)]);
+      // the samples stay in the transform's order (z = k1 + N1 k2 holds the
+      // natural sample k2 + N2 k1), except for the export
+      const int zr = mode == 2 ? z / N1 + N2 * (z % N1) : z;
+      if (il < nb) dst[(size_t)zr * d.nkx + il] = ccvt<ST>(W[il * LD + F::sk(z)]);
     }
     __syncthreads();
   }
@@ -550,6 +556,56 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
   }
 }
 
+// Physical-field export (FP64): one block per (plane, z tile); the inverse
+// x transforms of the export inputs (rows in natural z order, zinv mode 2),
+// then per point u = T rho u, v, w, T, omega = T curl(rho u) + grad T x
+// rho u (the quantities of tofis_loma's escrphys, trunk/tofis_loma/src/
+// escru.f:101-314) and Z, written in natural x order to out[p][q][z][x]
+template <int N1, int N2>
+__global__ void __launch_bounds__(Geo<N1, N2>::XT) k_xexport(Dev d, const int *jrow, int nplanes, int nf,
+                                                             double *out) {
+  using F = Four<N1, N2, double2>;
+  using G = Geo<N1, N2>;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2 *W = (double2 *)smraw;
+  const int nkx = d.nkx, nzk = (d.mgalz + ZB - 1) / ZB, NL = (nf + 1) / 2, nq = d.scalar ? 8 : 7;
+  const int p = blockIdx.x / nzk, z0 = (blockIdx.x - p * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
+  if (p >= nplanes) return;
+  const int y = jrow[p];
+  auto load = [&](int b, int n) -> double2 {
+    const int pr = b / ZB, l = b - pr * ZB;
+    if (l >= nzb) return czero();
+    const size_t g = ((size_t)y * d.mgalz + z0 + l) * nkx;
+    const double2 *A = d.zb[2 * pr] + g;
+    const double2 *B = 2 * pr + 1 < nf ? d.zb[2 * pr + 1] + g : nullptr;
+    int k = n;
+    bool up = false;
+    if (n >= nkx) {
+      k = N - n;
+      up = true;
+      if (k >= nkx) return czero();
+    }
+    const double2 a = A[k], c = B ? B[k] : czero();
+    if (!up) return k == 0 ? make_double2(a.x, c.x) : make_double2(a.x - c.y, a.y + c.x);
+    return make_double2(a.x + c.y, c.x - a.y);
+  };
+  F::template nat2perm_in<+1>(W, NL * ZB, LD, d.twx, load);
+  F::template nat2perm_p2<+1>(W, NL * ZB, LD);
+  for (int q = threadIdx.x; q < nzb * N; q += blockDim.x) {
+    const int l = q / N, pos = q - l * N;
+    const int x = pos / N1 + N2 * (pos % N1);  // natural x of the sample at pos
+    const double2 *c = W + (size_t)l * LD + F::sk(pos);
+    const double2 p0 = c[0], p1 = c[(size_t)ZB * LD], p2 = c[(size_t)2 * ZB * LD], p3 = c[(size_t)3 * ZB * LD];
+    const double2 p4 = c[(size_t)4 * ZB * LD];
+    const double ru = p0.x, rv = p0.y, rw = p1.x, T = p1.y, tx = p2.x, ty = p2.y, tz = p3.x;
+    const double v[8] = {ru * T, rv * T, rw * T, T, T * p3.y + ty * rw - tz * rv, T * p4.x + tz * ru - tx * rw,
+                         T * p4.y + tx * rv - ty * ru, nf > 10 ? c[(size_t)5 * ZB * LD].x : 0.0};
+    double *o = out + (((size_t)p * nq) * d.mgalz + z0 + l) * d.mgalx + x;
+    for (int k = 0; k < nq; k++) o[(size_t)k * d.mgalz * d.mgalx] = v[k];
+  }
+}
+
 // 2014 variant: d(rho) = -Delta T / (T (T + Delta T)) at every physical
 // point (tensor2, lomacte/cross.f:1819-1908): T and Delta T arrive as one
 // complex line per (y, z), the result leaves in z-physical buffer 0.
@@ -753,6 +809,13 @@ struct Launch {
     dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : n_out(d)));
     k_zfwd<N1, N2, CT, ST><<<g, ZG::ZT, zsm(), s>>>(d, mode);
   }
+  static size_t xexport_sm() { return (size_t)6 * G::ZB * G::LD * sizeof(double2); }
+  static void xexport(const Dev &d, const int *jrow, int nplanes, int nf, double *out, cudaStream_t s) {
+    if constexpr (sizeof(CT) == sizeof(double2) && sizeof(ST) == sizeof(double2)) {
+      const int nzk = (d.mgalz + G::ZB - 1) / G::ZB;
+      k_xexport<N1, N2><<<nplanes * nzk, G::XT, xexport_sm(), s>>>(d, jrow, nplanes, nf, out);
+    }
+  }
   static void xdrho(const Dev &d, cudaStream_t s) {
     if constexpr (sizeof(CT) == sizeof(double2) && sizeof(ST) == sizeof(double2)) {
       dim3 g((d.mgalz + G::ZB - 1) / G::ZB, d.my);
@@ -797,6 +860,8 @@ struct Launch {
     if ((e = optin1((const void *)k_zinv<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_zfwd<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xstats<N1, N2, CT, ST>, limit)) != cudaSuccess) return e;
+    if constexpr (sizeof(CT) == sizeof(double2) && sizeof(ST) == sizeof(double2))
+      if ((e = optin1((const void *)k_xexport<N1, N2>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true, true>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, false, true>, limit)) != cudaSuccess) return e;
     if ((e = optin1((const void *)k_xphys<N1, N2, CT, ST, true, false>, limit)) != cudaSuccess) return e;
@@ -846,6 +911,8 @@ inline cudaError_t upload_twiddles() {
   case N: Launch<N1, N2, double2, double2>::xdrho(d, s); return true;
 #define LMC_FFT_CASE_X(N, N1, N2) \
   case N: LMC_FFT_FORMS_M(N1, N2, 2, xphys(d, rk, do_cfl, do_diag, s)) return true;
+#define LMC_FFT_CASE_XE(N, N1, N2) \
+  case N: Launch<N1, N2, double2, double2>::xexport(d, jrow, nplanes, nf, out, s); return true;
 #define LMC_FFT_CASE_XST(N, N1, N2) \
   case N: LMC_FFT_FORMS(N1, N2, xstats(d, st, s)) return true;
 #define LMC_FFT_CASE_ZI(N, N1, N2) \
@@ -876,6 +943,9 @@ inline cudaError_t upload_twiddles() {
   }                                                                                               \
   bool fft_xphys_##SUF(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {           \
     switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_X) default: return false; }                      \
+  }                                                                                               \
+  bool fft_xexport_##SUF(const Dev &d, const int *jrow, int nplanes, int nf, double *out, cudaStream_t s) { \
+    switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_XE) default: return false; }                     \
   }                                                                                               \
   bool fft_xstats_##SUF(const Dev &d, const Stats &st, cudaStream_t s) {                          \
     switch (d.mgalx) { LMC_FFT_SIZES(LMC_FFT_CASE_XST) default: return false; }                    \

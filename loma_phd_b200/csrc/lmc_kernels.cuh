@@ -147,6 +147,10 @@ __host__ __device__ inline int n_sbuf(const Dev &d) { return d.visc ? SB_G23 + 1
 __host__ __device__ inline int n_zbuf(const Dev &d) { return n_in(d) > n_out(d) ? n_in(d) : n_out(d); }
 // 00 profiles held for the mixed form's transform inputs
 constexpr int NMI = 11;
+// Physical-field export (FP64 work buffers of its own): spectral slot of
+// export input q = 0..10 (rho u, rho v, rho w, T, dT/dx, dT/dy, dT/dz,
+// curl(rho u) x, y, z, Z), past SB_MY and SB_DMY, which Lapvdvhom fills
+__host__ __device__ inline int xslot(int q) { return q < 5 ? q : q + 2; }
 
 // work-buffer views of the two precisions
 template <typename CT>
@@ -180,8 +184,15 @@ void launch_zupd(const Dev &d, cudaStream_t s);
 // variable viscosity: the SB_GYY .. SB_G23 inputs from rho u_i (after
 // launch_assemble)
 void launch_sgrad(const Dev &d, cudaStream_t s);
-// mode 1 (2014 variant): the d(rho) round trip of T and Delta T; f0, nf:
-// only inputs f0 .. f0+nf-1 (nf <= 0: all)
+// physical-field export (FP64 Dev of the export's own buffers): the
+// spectral inputs (after launch_lapv), then, after launch_zinv mode 2, the
+// planes jrow[0..nplanes-1] (0-based) of the nq quantities into
+// out[p][q][z][x]
+void launch_xprep(const Dev &d, cudaStream_t s);
+void launch_xexport(const Dev &d, const int *jrow, int nplanes, int nf, double *out, cudaStream_t s);
+// mode 1 (2014 variant): the d(rho) round trip of T and Delta T; mode 2
+// (export, FP64): the inputs in slots xslot(f), rows in natural z order;
+// f0, nf: only inputs f0 .. f0+nf-1 (nf <= 0: all)
 void launch_zinv(const Dev &d, cudaStream_t s, int mode = 0, int f0 = 0, int nf = 0);
 void launch_xdrho(const Dev &d, cudaStream_t s);
 void launch_xphys(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s);

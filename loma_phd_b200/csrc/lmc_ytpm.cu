@@ -35,6 +35,7 @@ void tpm_op_y(const Dev &d, int op, const double2 *in, double2 *out, double2 *ou
 }
 void launch_zder(const Dev &d, cudaStream_t s) { LMC_TPM(t_zder, d); }
 void launch_zupd(const Dev &d, cudaStream_t s) { LMC_TPM(t_zupd, d); }
+void launch_xprep(const Dev &d, cudaStream_t s) { tpm::t_xprep<<<tgrid(d), tpm::TB, 0, s>>>(d); }
 void launch_sgrad(const Dev &d, cudaStream_t s) {  // mixed: one more block for the exact 00 profiles
   if (d.prec) tpm::t_sgrad<float2><<<tgrid(d) + 1, tpm::TB, 0, s>>>(d);
   else tpm::t_sgrad<double2><<<tgrid(d), tpm::TB, 0, s>>>(d);

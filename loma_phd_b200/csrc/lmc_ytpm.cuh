@@ -687,6 +687,120 @@ __global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
 }
 
 // ----------------------------------------------------------------------
+// Physical-field export (lmc_physical_f64), FP64: the transform inputs of
+// tofis_loma's escrphys quantities from the state, without writing it:
+// rho u_i assembled as the substep does (cross.f:315-349, 395-499, with
+// xi = 0), T with its wall values, grad T, and C = curl(rho u).  Reads
+// m_y, dm_y/dy from SB_MY, SB_DMY (launch_lapv before); writes the export
+// slots xslot(0..10) (lmc_kernels.cuh); scratch ws[0..3].
+// ----------------------------------------------------------------------
+__global__ void __launch_bounds__(TB) t_xprep(Dev d) {
+  Mode M;
+  if (!mode_of(d, M)) return;
+  const int my = d.my;
+  const size_t ld = d.nmode;
+  const bool m00 = M.m == 0;
+  const double ta = (M.k2 != 0.0) ? M.kx / M.k2 : 0.0, tb = (M.k2 != 0.0) ? M.kz / M.k2 : 0.0;
+  double2 *s0 = d.ws[0] + M.m, *s1 = d.ws[1] + M.m, *s2 = d.ws[2] + M.m, *s3 = d.ws[3] + M.m;
+  double2 *F[11];
+  for (int q = 0; q < 11; q++) F[q] = d.sb[xslot(q)] + M.m;
+  const double2 vor1 = d.vor[ld + M.m], vorn = d.vor[(size_t)(my - 2) * ld + M.m];  // cross.f:315-327
+  const double2 tb0 = m00 ? make_double2(1.0 / d.scal_d[3], 0.0) : czero();       // cross.f:336-349
+  const double2 tbn = m00 ? make_double2(1.0 / d.scal_d[4], 0.0) : czero();
+  {
+    Rd<double2, 3> rpsi, rT, rvor, rdmy;
+    rpsi.start(d.psi + M.m, ld, my, 1, 0);
+    rT.start(d.scal + M.m, ld, my, 1, 0);
+    rvor.start(d.vor + M.m, ld, my, 1, 0);
+    rdmy.start(d.sb[SB_DMY] + M.m, ld, my, 1, 0);
+    Win wp, wt, wu, ww;
+    wp.clear();
+    wt.clear();
+    wu.clear();
+    ww.clear();
+    Hist hp, ht, hu, hw;
+    hp.clear();
+    ht.clear();
+    hu.clear();
+    hw.clear();
+    // row r of rho u, rho w (the psi value of row r is the newest in wp)
+    auto ru_rw = [&](int r, double2 ps, double2 &ru, double2 &rw) {
+      const double2 a = rdmy.pop(), vr = rvor.pop();
+      const double2 vo = r == 0 ? vor1 : r == my - 1 ? vorn : vr;
+      ru = cadd(csub(cik(ta, a), cik(tb, vo)), cik(M.kx, ps));
+      rw = cadd(cadd(cik(tb, a), cik(ta, vo)), cik(M.kz, ps));
+      if (m00) {
+        const bool in = r >= 0 && r < my;
+        ru = make_double2(in ? d.u00[r] : 0.0, 0.0);
+        rw = make_double2(in ? d.w00[r] : 0.0, 0.0);
+      }
+      if (r >= my) ru = rw = czero();
+    };
+    auto T_of = [&](int r, double2 v) { return r == 0 ? tb0 : r == my - 1 ? tbn : r >= my ? czero() : v; };
+    for (int r = 0; r < 3; r++) {
+      const double2 ps = rpsi.pop();
+      wp.push(ps);
+      wt.push(T_of(r, rT.pop()));
+      double2 ru, rw;
+      ru_rw(r, ps, ru, rw);
+      wu.push(ru);
+      ww.push(rw);
+    }
+    #pragma unroll 1
+    for (int j = 0; j < my; j++) {
+      const int r = j + 3;
+      const double2 ps = rpsi.pop();
+      wp.push(ps);
+      wt.push(T_of(r, rT.pop()));
+      double2 ru, rw;
+      ru_rw(r, ps, ru, rw);
+      wu.push(ru);
+      ww.push(rw);
+      const double2 T = wt.c();
+      put(F[0], ld, j, wu.c());
+      put(F[2], ld, j, ww.c());
+      put(F[3], ld, j, T);
+      put(F[4], ld, j, cik(M.kx, T));
+      put(F[6], ld, j, cik(M.kz, T));
+      s0[(size_t)j * ld] = d1f(d, j, wp, hp);
+      s1[(size_t)j * ld] = d1f(d, j, wt, ht);
+      s2[(size_t)j * ld] = d1f(d, j, wu, hu);
+      s3[(size_t)j * ld] = d1f(d, j, ww, hw);
+    }
+  }
+  Rd<double2, 3> r0, r1, r2, r3, rmy, ru, rw;
+  r0.start(s0, ld, my, -1, my - 1);
+  r1.start(s1, ld, my, -1, my - 1);
+  r2.start(s2, ld, my, -1, my - 1);
+  r3.start(s3, ld, my, -1, my - 1);
+  rmy.start(d.sb[SB_MY] + M.m, ld, my, -1, my - 1);
+  ru.start(F[0], ld, my, -1, my - 1);
+  rw.start(F[2], ld, my, -1, my - 1);
+  Hist hp, ht, hu, hw;
+  hp.clear();
+  ht.clear();
+  hu.clear();
+  hw.clear();
+  #pragma unroll 1
+  for (int j = my - 1; j >= 0; j--) {
+    double2 rv = cadd(d1b(d, j, r0.pop(), hp), rmy.pop());  // cross.f:434-437, 471
+    if (m00) rv = make_double2(d.v00[j], 0.0);
+    const double2 Ty = d1b(d, j, r1.pop(), ht), dudy = d1b(d, j, r2.pop(), hu), dwdy = d1b(d, j, r3.pop(), hw);
+    const double2 u = ru.pop(), w = rw.pop();
+    put(F[1], ld, j, rv);
+    put(F[5], ld, j, Ty);
+    put(F[7], ld, j, csub(dwdy, cik(M.kz, rv)));
+    put(F[8], ld, j, csub(cik(M.kz, u), cik(M.kx, w)));
+    put(F[9], ld, j, csub(cik(M.kx, rv), dudy));
+    if (d.scalar) {
+      double2 z = d.zsc[(size_t)j * ld + M.m];
+      if (j == 0 || j == my - 1) z = m00 ? make_double2(d.scal_d[j == 0 ? 5 : 6], 0.0) : czero();
+      put(F[10], ld, j, z);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------
 // (6a)-(6b) T update and N_i (cross.f:619-682); rf0u / rf0w get the 00
 // pencils of d(rho uv)/dy and d(rho vw)/dy for the 00 tail.
 // ----------------------------------------------------------------------

@@ -33,7 +33,11 @@ SYMBOLS = (
     "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
     "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read", "lmc_load_scalar_f64", "lmc_get_scalar_f64",
+    "lmc_physical_f64",
 )
+
+# quantities of lmc_physical_f64, in order (the scalar adds "Z")
+PHYSICAL_NAMES = ("u", "v", "w", "T", "omega_x", "omega_y", "omega_z")
 
 KERNEL_NAMES = ("lapv", "assemble", "tder", "zinv", "xphys", "zfwd", "post1", "post2", "psi", "memset", "stats")
 
@@ -115,6 +119,7 @@ def _lib():
         L.lmc_stats_read.argtypes = [vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.lmc_load_scalar_f64.argtypes = [vp, _dp]
         L.lmc_get_scalar_f64.argtypes = [vp, _dp]
+        L.lmc_physical_f64.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
         L.lmc_footprint.argtypes = [ctypes.POINTER(lmc_params)]
         L.lmc_footprint.restype = ctypes.c_size_t
         _LIB = L
@@ -325,6 +330,17 @@ class Lomacte:
         a = np.zeros(self.shape, dtype=np.complex128)
         _check(_lib().lmc_get_scalar_f64(self._h, _ptr(a.view(np.float64))), "lmc_get_scalar_f64")
         return a
+
+    def physical(self, planes) -> dict:
+        """Physical fields on the 1-based y rows planes (lmc_physical_f64):
+        a dict of [nplanes, mgalz, mgalx] arrays u, v, w, T, omega_x,
+        omega_y, omega_z (and Z with the scalar), x fastest."""
+        pl = np.ascontiguousarray(planes, dtype=np.int32)
+        names = PHYSICAL_NAMES + (("Z",) if self.p.scalar else ())
+        out = np.zeros((len(pl), len(names), self.p.mgalz, self.p.mgalx))
+        _check(_lib().lmc_physical_f64(self._h, len(pl), pl.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                       _ptr(out.ravel())), "lmc_physical_f64")
+        return {k: out[:, q] for q, k in enumerate(names)}
 
     def sync(self):
         _check(_lib().lmc_sync(self._h), "lmc_sync")

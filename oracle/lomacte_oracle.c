@@ -1778,6 +1778,107 @@ int lmo_step(lmo *o, int nsteps) {
   return 0;
 }
 
+/* Physical fields of the current state on chosen y planes: the quantities
+ * of tofis_loma's escrphys (trunk/tofis_loma/src/escru.f:11-314, with the
+ * y work of uvw.f:7-94), formed from the solver's own rho u_i (Lapvdvhom
+ * with the wall conditions of the substep, cross.f:315-349, 365-499):
+ * u = T rho u, v, w, T, and the vorticity omega = curl(T rho u) = T C +
+ * grad T x rho u with C = curl(rho u) (C_y is Omega_y), then Z with the
+ * scalar.  out[p][q][z][x] (x fastest), q = 0..6 (7 with the scalar);
+ * jplanes 1-based.  The state is not changed. */
+int lmo_physical(const lmo *o, int nplanes, const int *jplanes, double *out) {
+  if (!o || nplanes < 0 || (nplanes && (!jplanes || !out)) || o->variant) return -1;
+  for (int p = 0; p < nplanes; p++)
+    if (jplanes[p] < 1 || jplanes[p] > o->my) return -1;
+  const int my = o->my, mz = o->mz, mgalx = o->mgalx, mgalz = o->mgalz, nkx = o->nkx;
+  const int nf = o->scalar ? 11 : 10, nq = o->scalar ? 8 : 7;
+  const size_t ns = (size_t)o->nmode * my, nl = (size_t)mgalz * my * nkx;
+  cplx *f[11], *ln[11];
+  for (int q = 0; q < nf; q++) { f[q] = xcalloc(ns, sizeof(cplx)); ln[q] = xcalloc(nl, sizeof(cplx)); }
+  /* f: 0 rho u, 1 rho v, 2 rho w, 3 T, 4 dT/dx, 5 dT/dy, 6 dT/dz, 7 C_x, 8 C_y, 9 C_z, 10 Z */
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *s = malloc(sizeof(double) * 24 * my);
+    cplx *c = malloc(sizeof(cplx) * 6 * my);
+    double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
+    cplx *vo = c, *ph = c + my, *mv = c + 2 * my, *dmv = c + 3 * my, *d1 = c + 4 * my, *d2 = c + 5 * my;
+#pragma omp for schedule(static)
+    for (int m = 0; m < o->nmode; m++) {
+      int i = m / mz, k = m % mz;
+      double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
+      size_t b = (size_t)m * my;
+      for (int j = 0; j < my; j++) { vo[j] = o->vor[b + j]; ph[j] = o->phi[b + j]; f[3][b + j] = o->scal[b + j]; }
+      vo[0] = vo[1]; vo[my - 1] = vo[my - 2];           /* cross.f:315-327 */
+      ph[0] = 0; ph[my - 1] = 0;                        /* cross.f:329-335 */
+      f[3][b] = m == 0 ? 1.0 / o->rhobot : 0.0;         /* cross.f:336-349 */
+      f[3][b + my - 1] = m == 0 ? 1.0 / o->rhotop : 0.0;
+      lapvdvhom_c(o, ph, mv, dmv, rK, sc);              /* cross.f:365-372 */
+      deryr2_c(o, o->psi + b, d1, w1, w2, tt1, tt2);    /* cross.f:434-437 */
+      cplx ta = 0, tb = 0;
+      if (rK != 0.0) { ta = I * kx / rK; tb = I * kz / rK; }
+      for (int j = 0; j < my; j++) {                    /* cross.f:395-407, 463-482 */
+        f[0][b + j] = dmv[j] * ta - vo[j] * tb + I * kx * o->psi[b + j];
+        f[2][b + j] = dmv[j] * tb + vo[j] * ta + I * kz * o->psi[b + j];
+        f[1][b + j] = mv[j] + d1[j];
+      }
+      if (m == 0)                                        /* cross.f:486-491 */
+        for (int j = 0; j < my; j++) { f[0][j] = o->u00wk[j]; f[1][j] = o->v00wk[j]; f[2][j] = o->w00wk[j]; }
+      deryr2_c(o, f[3] + b, f[5] + b, w1, w2, tt1, tt2);
+      deryr2_c(o, f[0] + b, d1, w1, w2, tt1, tt2);
+      deryr2_c(o, f[2] + b, d2, w1, w2, tt1, tt2);
+      for (int j = 0; j < my; j++) {
+        f[4][b + j] = I * kx * f[3][b + j];
+        f[6][b + j] = I * kz * f[3][b + j];
+        f[7][b + j] = d2[j] - I * kz * f[1][b + j];
+        f[8][b + j] = I * kz * f[0][b + j] - I * kx * f[2][b + j];
+        f[9][b + j] = I * kx * f[1][b + j] - d1[j];
+      }
+      if (o->scalar) {
+        for (int j = 0; j < my; j++) f[10][b + j] = o->zsc[b + j];
+        f[10][b] = m == 0 ? o->zbot : 0.0;
+        f[10][b + my - 1] = m == 0 ? o->ztop : 0.0;
+      }
+    }
+    free(s); free(c);
+  }
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    cplx *buf = malloc(sizeof(cplx) * (mgalz > mgalx ? mgalz : mgalx)), *fo = malloc(sizeof(cplx) * (mgalz > mgalx ? mgalz : mgalx));
+#pragma omp for collapse(2) schedule(static)
+    for (int q = 0; q < nf; q++)
+      for (int i = 0; i < nkx; i++) zinv_plane(o, i, f[q], ln[q], buf, fo);
+    free(buf); free(fo);
+  }
+#pragma omp parallel num_threads(o->nthreads)
+  {
+    double *ph = malloc(sizeof(double) * mgalx * 12);
+    cplx *buf = malloc(sizeof(cplx) * mgalx), *fo = malloc(sizeof(cplx) * mgalx);
+#pragma omp for collapse(2) schedule(static)
+    for (int p = 0; p < nplanes; p++)
+      for (int z = 0; z < mgalz; z++) {
+        const size_t L = (size_t)(jplanes[p] - 1) * mgalz + z;
+        double *r[12];
+        for (int q = 0; q < 12; q++) r[q] = ph + (size_t)q * mgalx;
+        for (int q = 0; q < nf; q += 2)
+          xinv2(o, ln[q] + L * nkx, q + 1 < nf ? ln[q + 1] + L * nkx : ln[q] + L * nkx, r[q], r[q + 1], buf, fo);
+        for (int x = 0; x < mgalx; x++) {
+          const double mu = r[0][x], mvv = r[1][x], mw = r[2][x], T = r[3][x];
+          const double tx = r[4][x], ty = r[5][x], tz = r[6][x];
+          double v[8];
+          v[0] = mu * T; v[1] = mvv * T; v[2] = mw * T; v[3] = T;
+          v[4] = T * r[7][x] + ty * mw - tz * mvv;
+          v[5] = T * r[8][x] + tz * mu - tx * mw;
+          v[6] = T * r[9][x] + tx * mvv - ty * mu;
+          v[7] = o->scalar ? r[10][x] : 0.0;
+          for (int q = 0; q < nq; q++) out[(((size_t)p * nq + q) * mgalz + z) * mgalx + x] = v[q];
+        }
+      }
+    free(ph); free(buf); free(fo);
+  }
+  for (int q = 0; q < nf; q++) { free(f[q]); free(ln[q]); }
+  return 0;
+}
+
 int lmo_set_variant(lmo *o, int variant) {
   if (!o || variant < 0 || variant > 1 || (variant && (o->scalar || o->vs))) return -1;
   o->variant = variant;

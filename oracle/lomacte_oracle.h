@@ -108,6 +108,12 @@ int lmo_get_scalar_state(const lmo *o, double *z);
  * Not for the 2014 variant. */
 int lmo_set_viscosity(lmo *o, int on, double sigma);
 
+/* Physical fields of the current state on chosen y planes (the quantities
+ * of tofis_loma's escrphys, trunk/tofis_loma/src/escru.f:11-314, from the
+ * solver's own rho u_i): out[p][q][z][x] with q = u, v, w, T, omega_x,
+ * omega_y, omega_z (and Z with the scalar); jplanes 1-based. */
+int lmo_physical(const lmo *o, int nplanes, const int *jplanes, double *out);
+
 /* Coefficient access for tests (band storage row-major [row][band]). */
 void lmo_get_coefs(const lmo *o, double *prem1_lu, double *dt11, double *dt12,
                    double *prem3_lu, double *dt21, double *dt22, double *fmap);

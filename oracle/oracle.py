@@ -68,6 +68,7 @@ def lib():
         L.lmo_set_scalar_state.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_get_scalar_state.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_set_viscosity.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.lmo_physical.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp]
         L.lmo_cft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         L.lmo_rft.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         _lib = L
@@ -96,6 +97,7 @@ class Oracle:
         if nthreads is None:
             nthreads = os.cpu_count() or 1
         self.nthreads = nthreads
+        self._scalar = False
         self.h = lib().lmo_create(mgalx, mgalz, self.my, _p(self.y), Re, alp, bet,
                                   peclet, cfl, ncfl, dtmode, dt0, nthreads)
         if not self.h:
@@ -141,6 +143,7 @@ class Oracle:
     def set_scalar(self, z, schmidt):
         if lib().lmo_set_scalar(self.h, 1, float(schmidt)) != 0:
             raise ValueError("lmo_set_scalar rejected its arguments")
+        self._scalar = True
         a = np.ascontiguousarray(np.asarray(z, dtype=np.complex128).reshape(self.shape)).view(np.float64)
         lib().lmo_set_scalar_state(self.h, _p(a.ravel()))
 
@@ -155,6 +158,18 @@ class Oracle:
         on = sigma is not None
         if lib().lmo_set_viscosity(self.h, int(on), float(sigma or 0.0)) != 0:
             raise ValueError("lmo_set_viscosity rejected its arguments")
+
+    # physical fields on y planes (lomacte_oracle.h: lmo_physical)
+    def physical(self, planes):
+        """[nplanes, nq, mgalz, mgalx]: u, v, w, T, omega_x, omega_y,
+        omega_z (and Z with the scalar) on the 1-based rows planes."""
+        pl = np.ascontiguousarray(planes, dtype=np.int32)
+        nq = 8 if self._scalar else 7
+        out = np.zeros((len(pl), nq, self.mgalz, self.mgalx))
+        rc = lib().lmo_physical(self.h, len(pl), pl.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(out.ravel()))
+        if rc != 0:
+            raise ValueError("lmo_physical rejected its arguments")
+        return out
 
     # statistics: addstats1/2 and the phys2 sums (cross.f:578-585, 794-812,
     # 1583-1607), resetstats (escru.f:485-580)
