@@ -133,8 +133,9 @@ int lmc_get_scalar_f64(lmc_handle *h, double *z);
 /* Physical fields of the current state on chosen y planes: the quantities
  * tofis_loma writes (escrphys, trunk/tofis_loma/src/escru.f:11-314; y work
  * of uvw.f:7-94), formed from the solver's own rho u_i, i.e. Lapvdvhom with
- * the wall conditions of the substep (cross.f:315-349, 365-499) rather than
- * tofis_loma's own Robin-condition solve for rho v: for each 1-based row
+ * the substep's wall conditions of Omega_y and phi (cross.f:315-335,
+ * 365-499) rather than tofis_loma's own Robin-condition solve for rho v,
+ * and T, Z as stored (as tofis_loma reads them): for each 1-based row
  * jplanes[p] the mgalz x mgalx planes (x fastest, natural order) of u, v, w,
  * T, omega_x, omega_y, omega_z and, with the scalar, Z, in that order:
  * out[p][q][z][x], q < 7 (8).  omega = curl(T rho u) = T curl(rho u) +

@@ -689,8 +689,9 @@ __global__ void __launch_bounds__(TB) t_sgrad(Dev d) {
 // ----------------------------------------------------------------------
 // Physical-field export (lmc_physical_f64), FP64: the transform inputs of
 // tofis_loma's escrphys quantities from the state, without writing it:
-// rho u_i assembled as the substep does (cross.f:315-349, 395-499, with
-// xi = 0), T with its wall values, grad T, and C = curl(rho u).  Reads
+// rho u_i assembled as the substep does (the wall conditions of Omega_y and
+// phi, cross.f:315-335, then cross.f:395-499 with xi = 0), T and Z as
+// stored (as tofis_loma reads them), grad T, and C = curl(rho u).  Reads
 // m_y, dm_y/dy from SB_MY, SB_DMY (launch_lapv before); writes the export
 // slots xslot(0..10) (lmc_kernels.cuh); scratch ws[0..3].
 // ----------------------------------------------------------------------
@@ -705,8 +706,6 @@ __global__ void __launch_bounds__(TB) t_xprep(Dev d) {
   double2 *F[11];
   for (int q = 0; q < 11; q++) F[q] = d.sb[xslot(q)] + M.m;
   const double2 vor1 = d.vor[ld + M.m], vorn = d.vor[(size_t)(my - 2) * ld + M.m];  // cross.f:315-327
-  const double2 tb0 = m00 ? make_double2(1.0 / d.scal_d[3], 0.0) : czero();       // cross.f:336-349
-  const double2 tbn = m00 ? make_double2(1.0 / d.scal_d[4], 0.0) : czero();
   {
     Rd<double2, 3> rpsi, rT, rvor, rdmy;
     rpsi.start(d.psi + M.m, ld, my, 1, 0);
@@ -736,11 +735,10 @@ __global__ void __launch_bounds__(TB) t_xprep(Dev d) {
       }
       if (r >= my) ru = rw = czero();
     };
-    auto T_of = [&](int r, double2 v) { return r == 0 ? tb0 : r == my - 1 ? tbn : r >= my ? czero() : v; };
     for (int r = 0; r < 3; r++) {
       const double2 ps = rpsi.pop();
       wp.push(ps);
-      wt.push(T_of(r, rT.pop()));
+      wt.push(rT.pop());
       double2 ru, rw;
       ru_rw(r, ps, ru, rw);
       wu.push(ru);
@@ -751,7 +749,7 @@ __global__ void __launch_bounds__(TB) t_xprep(Dev d) {
       const int r = j + 3;
       const double2 ps = rpsi.pop();
       wp.push(ps);
-      wt.push(T_of(r, rT.pop()));
+      wt.push(rT.pop());
       double2 ru, rw;
       ru_rw(r, ps, ru, rw);
       wu.push(ru);
@@ -792,11 +790,7 @@ __global__ void __launch_bounds__(TB) t_xprep(Dev d) {
     put(F[7], ld, j, csub(dwdy, cik(M.kz, rv)));
     put(F[8], ld, j, csub(cik(M.kz, u), cik(M.kx, w)));
     put(F[9], ld, j, csub(cik(M.kx, rv), dudy));
-    if (d.scalar) {
-      double2 z = d.zsc[(size_t)j * ld + M.m];
-      if (j == 0 || j == my - 1) z = m00 ? make_double2(d.scal_d[j == 0 ? 5 : 6], 0.0) : czero();
-      put(F[10], ld, j, z);
-    }
+    if (d.scalar) put(F[10], ld, j, d.zsc[(size_t)j * ld + M.m]);
   }
 }
 

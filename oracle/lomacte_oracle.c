@@ -1781,7 +1781,8 @@ int lmo_step(lmo *o, int nsteps) {
 /* Physical fields of the current state on chosen y planes: the quantities
  * of tofis_loma's escrphys (trunk/tofis_loma/src/escru.f:11-314, with the
  * y work of uvw.f:7-94), formed from the solver's own rho u_i (Lapvdvhom
- * with the wall conditions of the substep, cross.f:315-349, 365-499):
+ * with the wall conditions of Omega_y and phi, cross.f:315-335, 365-499;
+ * T and Z as stored, as tofis_loma reads them):
  * u = T rho u, v, w, T, and the vorticity omega = curl(T rho u) = T C +
  * grad T x rho u with C = curl(rho u) (C_y is Omega_y), then Z with the
  * scalar.  out[p][q][z][x] (x fastest), q = 0..6 (7 with the scalar);
@@ -1810,8 +1811,6 @@ int lmo_physical(const lmo *o, int nplanes, const int *jplanes, double *out) {
       for (int j = 0; j < my; j++) { vo[j] = o->vor[b + j]; ph[j] = o->phi[b + j]; f[3][b + j] = o->scal[b + j]; }
       vo[0] = vo[1]; vo[my - 1] = vo[my - 2];           /* cross.f:315-327 */
       ph[0] = 0; ph[my - 1] = 0;                        /* cross.f:329-335 */
-      f[3][b] = m == 0 ? 1.0 / o->rhobot : 0.0;         /* cross.f:336-349 */
-      f[3][b + my - 1] = m == 0 ? 1.0 / o->rhotop : 0.0;
       lapvdvhom_c(o, ph, mv, dmv, rK, sc);              /* cross.f:365-372 */
       deryr2_c(o, o->psi + b, d1, w1, w2, tt1, tt2);    /* cross.f:434-437 */
       cplx ta = 0, tb = 0;
@@ -1835,8 +1834,6 @@ int lmo_physical(const lmo *o, int nplanes, const int *jplanes, double *out) {
       }
       if (o->scalar) {
         for (int j = 0; j < my; j++) f[10][b + j] = o->zsc[b + j];
-        f[10][b] = m == 0 ? o->zbot : 0.0;
-        f[10][b + my - 1] = m == 0 ? o->ztop : 0.0;
       }
     }
     free(s); free(c);

@@ -1,9 +1,10 @@
 """Physical-field export on the device (lmc_physical_f64) against the
 oracle's restatement from the same state, through the C ABI.
 
-Bars: every quantity (u, v, w, T, omega_x, omega_y, omega_z, Z) on the
-chosen planes <= 1e-12 relative max difference, FP64 and mixed cases (the
-export is FP64 in every form), with the scalar, in a 2-D run and with the
+Bars (those of the FP64 step parity): every quantity (u, v, w, T,
+omega_x, omega_y, omega_z, Z) on the chosen planes <= 1e-10 relative L2
+and <= 1e-9 relative max difference, FP64 and mixed cases (the export is
+FP64 in every form), with the scalar, in a 2-D run and with the
 variable viscosity; the state is bit for bit the same before and after,
 and the next step is unchanged by an export in between.
 """
@@ -11,7 +12,7 @@ import numpy as np
 import pytest
 
 from loma_phd_b200 import Lomacte
-from tests.helpers import FIELDS, case, oracle_for
+from tests.helpers import FIELDS, case, oracle_for, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -27,8 +28,9 @@ def _compare(g, p, y, planes, Z=None):
     assert ref.shape[1] == len(names)
     for q, k in enumerate(names):
         r = ref[:, q]
+        assert rel_l2(dev[k], r) < 1e-10, (k, rel_l2(dev[k], r))
         e = np.abs(dev[k] - r).max() / max(np.abs(r).max(), 1e-300)
-        assert e < 1e-12, (k, e)
+        assert e < 1e-9, (k, e)
     return dev
 
 

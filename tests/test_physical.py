@@ -3,8 +3,8 @@
 trunk/tofis_loma/src/escru.f:11-314), from the solver's own rho u_i.
 
 Checks: T on a plane equals numpy's inverse 2-D transform of the spectral T
-(with the substep's wall values), so the natural z/x order and the
-normalisation are pinned independently; plane means of T and of rho u =
+as stored, so the natural z/x order and the normalisation are pinned
+independently; plane means of T and of rho u =
 u / T equal the 00 profiles; the mean of omega_y vanishes; the export
 leaves the state alone.
 """
@@ -46,7 +46,7 @@ def test_plane_means_and_state_untouched():
     o = oracle_for(p, y, st, nthreads=4)
     o.step(2)
     before = o.get_state()
-    planes = list(range(2, p.my))  # interior rows (the walls carry the boundary values)
+    planes = list(range(1, p.my + 1))
     out = o.physical(planes)
     after = o.get_state()
     for k in ("vor", "phi", "psi", "scal", "u00", "v00", "w00"):
