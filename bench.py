@@ -323,8 +323,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     state = g.get_state()
 
     # end-to-end through the public API with host buffers: every step loads
-    # the state from pinned host memory, advances one RK3 step and reads the
-    # state back.
+    # the state (and the scalar) from pinned host memory, advances one RK3
+    # step and reads the state back.
     e2e = None
     S, Z, P = sizes(p)
     if want_e2e:
@@ -334,19 +334,27 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
                for k in ("u00", "v00", "w00")}
         ptrs = [host[k].data_ptr() for k in ("vor", "phi", "psi", "scal")] + \
                [h00[k].data_ptr() for k in ("u00", "v00", "w00")]
-        ne = max(1, min(a.steps, 5))
-        for _ in range(2):
+        zh = torch.from_numpy(np.ascontiguousarray(scalar_ic(st)).view(np.float64).copy()).pin_memory() \
+            if a.scalar else None
+
+        def e2e_step():
             g.load_state_ptrs(*ptrs)
+            if zh is not None:
+                g.load_scalar_ptr(zh.data_ptr())
             g.step(1)
             g.get_state_ptrs(*ptrs)
+            if zh is not None:
+                g.get_scalar_ptr(zh.data_ptr())
+
+        ne = max(1, min(a.steps, 5))
+        for _ in range(2):
+            e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(ne):
-            g.load_state_ptrs(*ptrs)
-            g.step(1)
-            g.get_state_ptrs(*ptrs)
+            e2e_step()
         el = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{dev}")
-        nbytes = 4 * S * 16 + 3 * p.my * 8
+        nbytes = (5 if a.scalar else 4) * S * 16 + 3 * p.my * 8
         e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
 

@@ -414,6 +414,13 @@ class Lomacte:
                                         _ptr(t)), "lmc_get_state_f64")
         return float(t[0])
 
+    def load_scalar_ptr(self, z):
+        """Load Z from a raw host pointer (reference layout, complex*16)."""
+        _check(_lib().lmc_load_scalar_f64(self._h, ctypes.cast(ctypes.c_void_p(z), _dp)), "lmc_load_scalar_f64")
+
+    def get_scalar_ptr(self, z):
+        _check(_lib().lmc_get_scalar_f64(self._h, ctypes.cast(ctypes.c_void_p(z), _dp)), "lmc_get_scalar_f64")
+
     @property
     def stream(self) -> int:
         return int(_lib().lmc_stream(self._h) or 0)
