@@ -390,6 +390,14 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     # T derivatives and the psi solve run on a second stream beside the main
     # chain, so the fractions can sum above 1
     share = {k: round(prof[k][0] / max(ms, 1e-9), 4) for k in KERNEL_NAMES if prof[k][1]}
+    # the same by stage: the plane/line transposes are fused into the
+    # transform kernels and the RK3 update into post2 (normalised to the
+    # sum of the groups, as the two streams overlap)
+    stages = {"fft_and_transposes": ("zinv", "xphys", "zfwd"),
+              "y_solves": ("lapv", "assemble", "tder", "post1", "psi"),
+              "rhs_and_rk3_update": ("post2",)}
+    tot = sum(share.get(k, 0.0) for ks in stages.values() for k in ks)
+    stage_share = {n: round(sum(share.get(k, 0.0) for k in ks) / max(tot, 1e-12), 4) for n, ks in stages.items()}
     traffic = None
     table = NCU_TRAFFIC_256x65.get((prec == 0, sc, vs), {}) if prec in (0, 1) else {}
     if a.nx == 256 and a.nz == 256 and top in table:
@@ -402,7 +410,8 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     launches = g_launches
     step_bytes = 3 * sum(f(S, Z, P, w, sc, vs) for f in ALGO.values())
     return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
-            "kernel_share": share, "e2e": e2e, "state": state, "diag": diag, "step_bytes": step_bytes,
+            "kernel_share": share, "stage_share": stage_share, "e2e": e2e, "state": state, "diag": diag,
+            "step_bytes": step_bytes,
             "stats_step": stats_step,
             "launches_per_step": launches, "y_family": y_family,
             "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
@@ -508,6 +517,7 @@ def main():
             "gpu_launches": head["launches_per_step"] * a.steps,
             "y_kernels": head["y_family"],
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
+            "stage_share": head["stage_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving, "stats_step": head["stats_step"],
             "ensemble": ensemble,
@@ -515,7 +525,8 @@ def main():
         if mixed and 0 in arms:
             f64 = arms[0]
             line["fp64"] = {"value": f64["value"], "ms_per_step": f64["ms"] / a.steps, "roofline": f64["roofline"],
-                            "kernel_share": f64["kernel_share"], "e2e": f64["e2e"], "clocks": f64["clocks"],
+                            "kernel_share": f64["kernel_share"], "stage_share": f64["stage_share"],
+                            "e2e": f64["e2e"], "clocks": f64["clocks"],
                             "stats_step": f64["stats_step"]}
             line["mixed_over_fp64"] = head["value"] / f64["value"]
             line["error_vs_fp64"] = {"rel_l2": errs, "steps": a.warmup + a.steps,

@@ -10,7 +10,10 @@ main.f:559, recomputed every ncfl steps), and writes what the reference
 writes: an image every nimag steps (filout.NNN, escru.f:11-193), the
 statistics of the ntimes steps before each nhist boundary when nstart /= 0
 (filstt_NNN.sta / .spe, escru.f:276-484), and a .cf line every nhist steps
-(filstt.cf, cross.f:1172-1176).
+(filstt.cf, cross.f:1172-1176).  A restart file whose plane records carry
+a fifth field (the passive scalar, "mfz") runs with the scalar and writes
+it into its images; sigma selects the variable viscosity mu = T^sigma
+(branches/loma reads it as hre.dat's fourth value, main.f:543).
 """
 from __future__ import annotations
 
@@ -51,23 +54,30 @@ def grid_of(mx: int, mz: int):
 
 def run(hre_path: str, workdir: Optional[str] = None, precision: int = 0, device: int = 0,
         planes: Optional[List[int]] = None, nstep: Optional[int] = None,
-        log: Optional[Callable[[str], None]] = None) -> Dict[str, object]:
+        log: Optional[Callable[[str], None]] = None, sigma: Optional[float] = None,
+        schmidt: float = 0.0) -> Dict[str, object]:
     """Run a case as the reference's main program does.  File names in
     hre.dat are relative to workdir (default: the directory of hre.dat).
     planes: 1-based rows of the spectra (default: the centre row, the
-    reference's jsptot(nspec+1)); nstep overrides hre.dat's."""
+    reference's jsptot(nspec+1)); nstep overrides hre.dat's; sigma: mu =
+    T^sigma (None: constant viscosity); schmidt: Sc of a scalar the restart
+    carries (<= 0: Sc = Pr)."""
     wd = workdir or os.path.dirname(os.path.abspath(hre_path))
     h = files.read_hre(hre_path)
     r = files.read_restart(os.path.join(wd, h.filinp))
     hd = r["header"]
     mgalx, mgalz = grid_of(hd.mx, hd.mz)
+    has_z = "mfz" in r
     p = Params(mgalx=mgalx, mgalz=mgalz, my=hd.my, Re=h.Re, alp=h.alp, bet=h.bet, cfl=h.cfl, ncfl=h.ncfl,
-               dt_mode=0, dt=1e-4, precision=precision, device=device)
+               dt_mode=0, dt=1e-4, precision=precision, device=device, scalar=int(has_z), schmidt=schmidt,
+               visc=0 if sigma is None else 1, sigma=sigma or 0.0)
     y = np.asarray(hd.y)
     met = y_metrics(y)
     fmap = met["fmap"]
     case = Lomacte(p, y)
     case.load_state_f32({k: r[k] for k in ("vor", "phi", "psi", "scal")}, r["u00"], r["v00"], r["w00"], r["time"])
+    if has_z:
+        case.load_scalar(np.asarray(r["mfz"], dtype=np.complex128))
     planes = planes or [(hd.my + 1) // 2]
     case.stats_reset(planes)
     id22, ista = h.id22, h.id22  # main.f:565-566
@@ -80,6 +90,8 @@ def run(hre_path: str, workdir: Optional[str] = None, precision: int = 0, device
             fl, istati = step_flags(istep, h.nimag, h.nhist, h.ntimes, h.nstart, istati)
             if fl.image:
                 st = case.get_state()
+                if has_z:
+                    st["mfz"] = case.get_scalar()
                 path = os.path.join(wd, f"{h.filout}.{id22:03d}")
                 files.write_restart(path, st, y, fmap, time=st["time"], Re=h.Re, alp=h.alp, bet=h.bet, a0=h.a0)
                 out["images"].append(path)
@@ -112,5 +124,7 @@ def run(hre_path: str, workdir: Optional[str] = None, precision: int = 0, device
                     log(f"step {istep} time {d['time']:.6f} Deltat {d['Deltat']:.3e} dm {d['dm']:.6f}")
             out["steps"] = istep
     out["state"] = case.get_state()
+    if has_z:
+        out["state"]["mfz"] = case.get_scalar()
     case.close()
     return out

@@ -70,3 +70,32 @@ def test_driver_run(gpu, tmp_path):
     g.close()
     for k in FIELDS:
         np.testing.assert_array_equal(out["state"][k], ref[k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_driver_run_with_scalar_and_viscosity(gpu, tmp_path):
+    p, y, st = case(24, 24, 33)
+    T = st["scal"]
+    tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
+    z = T / (tt - tb)
+    z[0, 0, :] -= tb / (tt - tb)
+    st = dict(st, mfz=z)
+    tmp = str(tmp_path)
+    _write_case(tmp, p, y, st)
+    out = run(os.path.join(tmp, "hre.dat"), sigma=0.7)
+    assert out["steps"] == 12 and "mfz" in out["state"]
+    img = files.read_restart(out["images"][0])
+    assert "mfz" in img
+    # the same steps without the driver
+    r = files.read_restart(os.path.join(tmp, "start.000"))
+    q = type(p)(**{**p.__dict__, "dt_mode": 0, "dt": 1e-4, "cfl": 0.5, "ncfl": 2, "scalar": 1, "visc": 1,
+                   "sigma": 0.7})
+    g = Lomacte(q, y)
+    g.load_state_f32({k: r[k] for k in FIELDS}, r["u00"], r["v00"], r["w00"], 0.0)
+    g.load_scalar(np.asarray(r["mfz"], dtype=np.complex128))
+    g.step(12)
+    ref, zr = g.get_state(), g.get_scalar()
+    g.close()
+    for k in FIELDS:
+        np.testing.assert_array_equal(out["state"][k], ref[k], err_msg=k)
+    np.testing.assert_array_equal(out["state"]["mfz"], zr)
