@@ -1,6 +1,6 @@
 """2-D runs (one kz mode: nz = 1, mz = 1, mgalz = 3) and the longest x
-transform (1536 points, nx = 1024), the request shapes of BASELINE's
-serving config, against the FP64 oracle through the C ABI.
+transform (1536 points, nx = 1024), the 2-D request shapes of the serving
+stream, against the FP64 oracle through the C ABI.
 
 Bars as in test_gpu_parity.py: FP64 1 RK3 step <= 1e-10 relative L2 per
 field, 20 steps <= 1e-9 with the momentum thickness to 1e-9; mixed forms 1

@@ -118,7 +118,7 @@ def test_cfl_mode_matches_oracle(gpu, monkeypatch, ncfl, family):
 
 
 def test_hundred_steps_match_oracle(gpu):
-    # BASELINE configs[0] shape: 64^2 Fourier modes x 129, s = 4, dt = 0.01
+    # the small mixing-layer case: 64^2 Fourier modes x 129, s = 4, dt = 0.01
     p, y, st = case(64, 64, 129)
     sg, so, dg, do, hg, ho = _run_pair(p, y, st, 100, hist=True)
     for k in FIELDS:
