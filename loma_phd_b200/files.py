@@ -336,3 +336,74 @@ def read_spe(path: str) -> Dict[str, object]:
             spec[i] = np.frombuffer(r, dtype="<f4").reshape(12, nsp, nk)
     return dict(time=time, Re=Re, alp=alp, bet=bet, mx=mx, my=my, mz=mz, nacumsp=nacumsp, planes=planes,
                 y=yf[:, 0].copy(), fmap=yf[:, 1].copy(), spec=spec)
+
+
+# tofis_loma's physical-field files (escrphys, trunk/tofis_loma/src/
+# escru.f:11-314): per quantity (u, v, w, T, omega_x, omega_y, omega_z) a yz
+# file, a yx file and an xz file, each opening with the header record
+# time, Re, alp, bet (real*4), mgalx, my, mgalz, nspec, nacum (int) and the
+# record of the spectra rows and (y, fmap) pairs (escru.f:88-92); then per
+# row j = 1..my the yz line (x = plyz) over z and the yx line (z = plyx)
+# over x, and for the rows jspec the whole xz plane (x fastest), real*4.
+TOFIS_EXT = (".upyz", ".upyx", ".upxz", ".vpyz", ".vpyx", ".vpxz", ".wpyz", ".wpyx", ".wpxz",
+             ".Tfyz", ".Tfyx", ".Tfxz", ".o1yz", ".o1yx", ".o1xz", ".o2yz", ".o2yx", ".o2xz",
+             ".o3yz", ".o3yx", ".o3xz")
+TOFIS_FIELDS = ("u", "v", "w", "T", "omega_x", "omega_y", "omega_z")
+
+
+def write_tofis(base: str, fields: Dict[str, np.ndarray], y: np.ndarray, fmap: np.ndarray, *, time: float,
+                Re: float, alp: float, bet: float, jspec: Iterable[int], plyz: int = 1, plyx: int = 48,
+                nacum: int = 1) -> List[str]:
+    """Write the 21 files of escrphys from whole fields [my][mgalz][mgalx]
+    (e.g. Lomacte.physical(range(1, my + 1))).  jspec: 1-based rows of the
+    xz files; plyz, plyx: 1-based x index of the yz files and z index of
+    the yx files (escru.f:86-87).  Returns the paths."""
+    my, mgalz, mgalx = np.asarray(fields["u"]).shape
+    jspec = [int(j) for j in jspec]
+    if not (1 <= plyz <= mgalx and 1 <= plyx <= mgalz) or any(not 1 <= j <= my for j in jspec):
+        raise ValueError("plane indices outside the grid")
+    head = struct.pack("<4f5i", time, Re, alp, bet, mgalx, my, mgalz, len(jspec), nacum)
+    yf = np.empty(2 * my)
+    yf[0::2], yf[1::2] = np.asarray(y, dtype=np.float64), np.asarray(fmap, dtype=np.float64)
+    head2 = np.asarray(jspec, dtype="<i4").tobytes() + yf.astype("<f8").tobytes()
+    paths = []
+    for q, name in enumerate(TOFIS_FIELDS):
+        a = np.asarray(fields[name], dtype=np.float64)
+        for kind in range(3):
+            path = base + TOFIS_EXT[3 * q + kind]
+            with open(path, "wb") as f:
+                _write_record(f, head)
+                _write_record(f, head2)
+                for j in range(my):
+                    if kind == 0:
+                        _write_record(f, a[j, :, plyz - 1].astype("<f4").tobytes())
+                    elif kind == 1:
+                        _write_record(f, a[j, plyx - 1, :].astype("<f4").tobytes())
+                    elif j + 1 in jspec:
+                        _write_record(f, a[j].astype("<f4").tobytes())
+            paths.append(path)
+    return paths
+
+
+def read_tofis(path: str) -> Dict[str, object]:
+    """One escrphys file: header values and its records as float32 arrays
+    (yz and yx: [my][n]; xz: [nspec][mgalz][mgalx])."""
+    with open(path, "rb") as f:
+        h = struct.unpack("<4f5i", _read_record(f))
+        mgalx, my, mgalz, nspec = h[4], h[5], h[6], h[7]
+        r2 = _read_record(f)
+        jspec = np.frombuffer(r2[:4 * nspec], dtype="<i4")
+        yf = np.frombuffer(r2[4 * nspec:], dtype="<f8")
+        recs = []
+        while True:
+            r = _read_record(f)
+            if r is None:
+                break
+            recs.append(np.frombuffer(r, dtype="<f4"))
+    out = {"time": h[0], "Re": h[1], "alp": h[2], "bet": h[3], "mgalx": mgalx, "my": my, "mgalz": mgalz,
+           "nspec": nspec, "nacum": h[8], "jspec": jspec, "y": yf[0::2], "fmap": yf[1::2]}
+    if path.endswith("xz"):
+        out["data"] = np.array(recs).reshape(len(recs), mgalz, mgalx)
+    else:
+        out["data"] = np.array(recs)
+    return out

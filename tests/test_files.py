@@ -146,3 +146,33 @@ def test_restart_drives_the_gpu_path(gpu, tmp_path):
     write_restart(out, sg, y, y_metrics(y)["fmap"], time=g.diag()["time"], Re=p.Re, alp=p.alp, bet=p.bet)
     assert np.array_equal(read_restart(out)["scal"], _f32(sg)["scal"])
     g.close()
+
+
+def test_tofis_files_round_trip(tmp_path):
+    """escrphys's 21 files (trunk/tofis_loma/src/escru.f:11-314) from the
+    oracle's physical fields of a seeded state: headers, yz/yx lines and
+    xz planes read back as written."""
+    from loma_phd_b200 import files, y_metrics
+    from tests.helpers import case, oracle_for
+    p, y, st = case(24, 24, 33)
+    o = oracle_for(p, y, st, nthreads=2)
+    o.step(1)
+    ph = o.physical(list(range(1, p.my + 1)))
+    names = files.TOFIS_FIELDS
+    fields = {k: ph[:, q] for q, k in enumerate(names)}
+    fmap = y_metrics(y)["fmap"]
+    base = str(tmp_path / "run")
+    paths = files.write_tofis(base, fields, y, fmap, time=0.5, Re=p.Re, alp=p.alp, bet=p.bet, jspec=[16, 17],
+                              plyz=3, plyx=5)
+    assert len(paths) == 21
+    for q, k in enumerate(names):
+        a = fields[k].astype(np.float32)
+        yz = files.read_tofis(base + files.TOFIS_EXT[3 * q])
+        yx = files.read_tofis(base + files.TOFIS_EXT[3 * q + 1])
+        xz = files.read_tofis(base + files.TOFIS_EXT[3 * q + 2])
+        for r in (yz, yx, xz):
+            assert (r["mgalx"], r["my"], r["mgalz"], r["nspec"]) == (p.mgalx, p.my, p.mgalz, 2)
+            assert list(r["jspec"]) == [16, 17] and np.array_equal(r["y"], y)
+        assert np.array_equal(yz["data"], a[:, :, 2])
+        assert np.array_equal(yx["data"], a[:, 4, :])
+        assert np.array_equal(xz["data"], a[[15, 16]])
