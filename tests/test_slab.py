@@ -70,3 +70,56 @@ def test_exchange_gloo(world, nplanes):
         assert p.exitcode == 0
     assert [o[0] for o in out] == list(range(world))
     assert all(o[1] and o[2] for o in out), out
+
+
+def _transform_rank(rank, world, port, q):
+    """One rank of a slab-split inverse transform of T: z transforms of its
+    kx planes, the plane -> line exchange, x transforms of its lines (numpy
+    stands in for the device transforms); its lines of T against the
+    oracle's physical T of the whole state."""
+    import torch
+    import torch.distributed as dist
+
+    from loma_phd_b200.slab import SlabPlan, planes_to_lines
+    from tests.helpers import case, oracle_for
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    p, y, st = case(24, 24, 33)
+    o = oracle_for(p, y, st, nthreads=1)
+    T = o.get_state()["scal"]                                   # [kx][kz][y]
+    nkx, mz, my = T.shape
+    plan = SlabPlan(nplanes=nkx, mgalz=p.mgalz, my=my, nranks=world)
+    pb, pe = plan.planes(rank)
+    nz1 = (mz - 1) // 2
+    pad = np.zeros((pe - pb, p.mgalz, my), dtype=complex)       # kz padded (localyz2zy)
+    for k in range(mz):
+        pad[:, k if k <= nz1 else k + p.mgalz - mz, :] = T[pb:pe, k, :]
+    zphys = np.fft.ifft(pad, axis=1) * p.mgalz                  # e^{+i kz z}
+    block = np.ascontiguousarray(zphys.transpose(2, 1, 0).reshape(my * p.mgalz, pe - pb))  # [line][kx]
+    lines = planes_to_lines(torch.from_numpy(block), plan, rank).numpy()
+    lines[:, 0] = lines[:, 0].real                              # Im of mode 0 dropped (rftsingle.f:85-88)
+    full = np.zeros((lines.shape[0], p.mgalx), dtype=complex)
+    full[:, :nkx] = lines
+    full[:, p.mgalx - nkx + 1:] = np.conj(lines[:, 1:][:, ::-1])
+    phys = np.real(np.fft.ifft(full, axis=1)) * p.mgalx
+    lb, le = plan.lines(rank)
+    ref = o.physical(list(range(1, my + 1)))[:, 3]              # T [y][z][x]
+    want = ref.reshape(my * p.mgalz, p.mgalx)[lb:le]
+    err = float(np.abs(phys - want).max() / np.abs(want).max())
+    dist.barrier()
+    q.put((rank, err))
+    dist.destroy_process_group()
+
+
+def test_split_inverse_transform_gloo():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_transform_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(e < 1e-13 for _, e in out), out
