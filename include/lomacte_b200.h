@@ -20,6 +20,8 @@
 #ifndef LOMACTE_B200_H
 #define LOMACTE_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif

@@ -109,3 +109,14 @@ def test_viscosity_x_grid_limit():
     assert lm.footprint(ok) > 0 and lm.footprint(big_ns) > 0
     assert lm.footprint(big) == 0
     assert lm.footprint(Params.from_modes(768, 1, 65, scalar=1)) > 0
+
+
+@pytest.mark.parametrize("lang,cc", [("c", "gcc"), ("c++", "g++")])
+def test_header_compiles_alone(lang, cc, tmp_path):
+    import shutil
+    import subprocess
+    if not shutil.which(cc):
+        pytest.skip(f"no {cc}")
+    r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-x", lang,
+                        os.path.join(ROOT, "include", "lomacte_b200.h")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
