@@ -16,7 +16,11 @@ tau_ij = 2 T^sigma S_ij, isotropic part in the pressure).  The checks:
 * x <-> z mirror: swapping the two periodic directions (u <-> w,
   Omega_y -> -Omega_y) commutes with the substep to round-off;
 * the passive scalar follows T under the affine map when Re Sc = Pe
-  (both equations carry the same T^sigma terms).
+  (both equations carry the same T^sigma terms);
+* a motionless state with a 3-D temperature perturbation: one substep's
+  Delta T equals numpy's dealiased transform of T^sigma (T lap T + sigma
+  |grad T|^2) / Pe from the stored spectral T (x and z gradients
+  included).
 """
 import numpy as np
 
@@ -157,3 +161,66 @@ def test_viscosity_arguments_checked():
         except ValueError:
             continue
         raise AssertionError(f"sigma {bad} accepted")
+
+
+def _phys(c, mgalx, mgalz):
+    """half spectrum c[kx >= 0][kz signed] -> real plane [z][x] (e^{+i})"""
+    nkx, mz = c.shape
+    nz1 = (mz - 1) // 2
+    F = np.zeros((mgalz, mgalx), dtype=complex)
+    for i in range(nkx):
+        for k in range(mz):
+            kk = k if k <= nz1 else k - mz
+            F[kk % mgalz, i] += c[i, k]
+            if i > 0:
+                F[(-kk) % mgalz, (-i) % mgalx] += np.conj(c[i, k])
+    return np.real(np.fft.ifft2(F)) * mgalx * mgalz
+
+
+def test_three_dimensional_conduction():
+    """A motionless state (rho u = 0) with a 3-D temperature perturbation:
+    one substep's Delta T equals the dealiased transform of
+    T^sigma (T lap T + sigma |grad T|^2) / Pe, evaluated with numpy from
+    the stored spectral T (compact d/dy, d2/dy2 of the oracle per mode)."""
+    sig = 0.7
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    for k in ("vor", "phi", "psi"):
+        s[k][:] = 0
+    for k in ("u00", "v00", "w00"):
+        s[k] = np.zeros_like(s[k])
+    T = s["scal"]
+    T[:, :, :] = 0
+    T[0, 0, :] = st["scal"][0, 0, :]
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)      # zero at the walls
+    rng = np.random.default_rng(3)
+    nkx, mz, my = T.shape
+    for (i, k) in ((1, 0), (0, 2), (2, 1), (1, mz - 1), (3, 3)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    r1, o = _run(p, y, s, sig, sub=0)
+    dT = r1["scal"] - T
+    pe = p.Re * PR
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    Ty = np.zeros_like(T)
+    Tyy = np.zeros_like(T)
+    for i in range(nkx):
+        for k in range(mz):
+            Ty[i, k] = o.deryr(T[i, k].real) + 1j * o.deryr(T[i, k].imag)
+            Tyy[i, k] = o.deryyr(T[i, k].real) + 1j * o.deryyr(T[i, k].imag)
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    lap = Tyy - k2 * T
+    Tx = 1j * kxv[:, None, None] * T
+    Tz = 1j * kzv[None, :, None] * T
+    h = p.dt * 8.0 / 15.0
+    pred = np.zeros_like(T)
+    for j in range(1, my - 1):
+        ph = {n: _phys(a[:, :, j], p.mgalx, p.mgalz) for n, a in (("T", T), ("x", Tx), ("y", Ty), ("z", Tz), ("l", lap))}
+        rhs = ph["T"] ** sig * (ph["T"] * ph["l"] + sig * (ph["x"] ** 2 + ph["y"] ** 2 + ph["z"] ** 2)) / pe
+        F = np.fft.fft2(rhs) / (p.mgalx * p.mgalz)
+        for i in range(nkx):
+            for k in range(mz):
+                pred[i, k, j] = h * F[(k if k <= (mz - 1) // 2 else k - mz) % p.mgalz, i]
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-7
+    assert np.abs(dT[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
