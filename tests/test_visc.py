@@ -20,7 +20,11 @@ tau_ij = 2 T^sigma S_ij, isotropic part in the pressure).  The checks:
 * a motionless state with a 3-D temperature perturbation: one substep's
   Delta T equals numpy's dealiased transform of T^sigma (T lap T + sigma
   |grad T|^2) / Pe from the stored spectral T (x and z gradients
-  included).
+  included);
+* Omega_y in two modes over a 3-D temperature: the sigma-part of one
+  substep's Omega_y increment equals the curl of the divergence of tau'
+  formed by numpy (the x and z temperature-gradient terms of the stress
+  and its diagonal factor 2 included).
 """
 import numpy as np
 
@@ -224,3 +228,84 @@ def test_three_dimensional_conduction():
     inner = (slice(None), slice(None), slice(1, my - 1))
     assert np.abs(pred[inner]).max() > 1e-7
     assert np.abs(dT[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
+
+
+def _spec(plane, nkx, mz):
+    """real plane [z][x] -> the stored half spectrum [kx][kz] (dealiased)"""
+    mgalz, mgalx = plane.shape
+    F = np.fft.fft2(plane) / (mgalx * mgalz)
+    out = np.zeros((nkx, mz), dtype=complex)
+    for k in range(mz):
+        out[:, k] = F[(k if k <= (mz - 1) // 2 else k - mz) % mgalz, :nkx]
+    return out
+
+
+def test_three_dimensional_stress():
+    """Omega_y in two modes (so rho u = -i kz Omega/k^2, rho w = i kx
+    Omega/k^2), u00 a shear profile and a 3-D temperature: the sigma-part
+    of one substep's Omega_y increment equals i kz div(tau')_x - i kx
+    div(tau')_z with tau'_ij = (T^sigma - 1)(d(u_i)/dx_j + d(u_j)/dx_i)/Re
+    formed by numpy (x and z temperature gradients included)."""
+    sig = 0.7
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    nkx, mz, my = st["vor"].shape
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)
+    rng = np.random.default_rng(4)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    s["phi"][:] = 0
+    s["psi"][:] = 0
+    s["vor"][:] = 0
+    for (i, k) in ((1, 2), (2, mz - 1)):
+        s["vor"][i, k, :] = 0.05 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["u00"] = 0.5 * np.tanh(y / 2)
+    s["v00"] = np.zeros(my)
+    s["w00"] = np.zeros(my)
+    T = np.zeros_like(s["scal"])
+    T[0, 0, :] = st["scal"][0, 0, :]
+    for (i, k) in ((1, 0), (0, 2), (2, 1), (1, mz - 1)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["scal"] = T
+    r1, o = _run(p, y, s, sig, sub=0)
+    r0, _ = _run(p, y, s, None, sub=0)
+    h = p.dt * 8.0 / 15.0
+    got = (r1["vor"] - r0["vor"]) / h
+
+    def dy(a):
+        out = np.zeros_like(a)
+        for i in range(nkx):
+            for k in range(mz):
+                out[i, k] = o.deryr(a[i, k].real) + 1j * o.deryr(a[i, k].imag)
+        return out
+
+    vo = s["vor"].copy()
+    vo[:, :, 0], vo[:, :, -1] = vo[:, :, 1], vo[:, :, -2]  # the wall condition of Omega_y (cross.f:315-327)
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    k2[0, 0] = 1.0
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    ru, rw = -IZ * vo / k2, IX * vo / k2
+    ru[0, 0], rw[0, 0] = s["u00"], 0.0
+    rv = np.zeros_like(ru)
+    dru, drw = dy(ru), dy(rw)
+    g = {"xx": IX * ru, "yy": dy(rv), "zz": IZ * rw, "xy": dru + IX * rv, "xz": IZ * ru + IX * rw,
+         "yz": IZ * rv + drw}
+    grads = {"x": IX * T, "y": dy(T), "z": IZ * T}
+    tau = {n: np.zeros_like(T) for n in g}
+    ire = 1.0 / p.Re
+    for j in range(my):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp, u, v, w = P(T), P(ru), P(rv), P(rw)
+        tx, ty, tz = P(grads["x"]), P(grads["y"]), P(grads["z"])
+        c = ire * (Tp ** sig - 1.0)
+        phys = {"xx": 2 * c * (Tp * P(g["xx"]) + u * tx), "yy": 2 * c * (Tp * P(g["yy"]) + v * ty),
+                "zz": 2 * c * (Tp * P(g["zz"]) + w * tz), "xy": c * (Tp * P(g["xy"]) + u * ty + v * tx),
+                "xz": c * (Tp * P(g["xz"]) + u * tz + w * tx), "yz": c * (Tp * P(g["yz"]) + v * tz + w * ty)}
+        for n in tau:
+            tau[n][:, :, j] = _spec(phys[n], nkx, mz)
+    fx = IX * tau["xx"] + dy(tau["xy"]) + IZ * tau["xz"]
+    fz = IX * tau["xz"] + dy(tau["yz"]) + IZ * tau["zz"]
+    pred = IZ * fx - IX * fz
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-6
+    assert np.abs(got[inner] - pred[inner]).max() < 1e-8 * np.abs(pred[inner]).max()
