@@ -24,7 +24,9 @@ tau_ij = 2 T^sigma S_ij, isotropic part in the pressure).  The checks:
 * Omega_y in two modes over a 3-D temperature: the sigma-part of one
   substep's Omega_y increment equals the curl of the divergence of tau'
   formed by numpy (the x and z temperature-gradient terms of the stress
-  and its diagonal factor 2 included).
+  and its diagonal factor 2 included);
+* a motionless state with 3-D T and Z: one substep's Delta Z equals
+  numpy's T^sigma (T lap Z + sigma grad T . grad Z) / (Re Sc).
 """
 import numpy as np
 
@@ -309,3 +311,58 @@ def test_three_dimensional_stress():
     inner = (slice(None), slice(None), slice(1, my - 1))
     assert np.abs(pred[inner]).max() > 1e-6
     assert np.abs(got[inner] - pred[inner]).max() < 1e-8 * np.abs(pred[inner]).max()
+
+
+def test_three_dimensional_scalar_diffusion():
+    """A motionless state with 3-D T and Z: one substep's Delta Z equals
+    numpy's dealiased transform of T^sigma (T lap Z + sigma grad T . grad
+    Z) / (Re Sc)."""
+    sig, sc = 0.7, 1.3
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    nkx, mz, my = st["vor"].shape
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    for k in ("vor", "phi", "psi"):
+        s[k][:] = 0
+    for k in ("u00", "v00", "w00"):
+        s[k] = np.zeros_like(s[k])
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)
+    rng = np.random.default_rng(7)
+    T = np.zeros_like(s["scal"])
+    T[0, 0, :] = st["scal"][0, 0, :]
+    Z = np.zeros_like(T)
+    Z[0, 0, :] = 0.5 * (1 + np.tanh(y / 2))
+    Z[0, 0, 0], Z[0, 0, -1] = 0.0, 1.0
+    for (i, k) in ((1, 0), (0, 2), (2, 1)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    for (i, k) in ((1, 0), (1, mz - 1), (3, 2)):
+        Z[i, k, :] = 0.02 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["scal"] = T
+    o = oracle_for(p, y, s, nthreads=4)
+    o.set_scalar(Z, sc)
+    o.set_viscosity(sig)
+    o.substep(0)
+    dZ = o.get_scalar() - Z
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+
+    def dy(a, f):
+        r = np.zeros_like(a)
+        for i in range(nkx):
+            for k in range(mz):
+                r[i, k] = f(a[i, k].real) + 1j * f(a[i, k].imag)
+        return r
+
+    lapZ = dy(Z, o.deryyr) - (kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2) * Z
+    tg = (IX * T, dy(T, o.deryr), IZ * T)
+    zg = (IX * Z, dy(Z, o.deryr), IZ * Z)
+    h = p.dt * 8.0 / 15.0
+    pred = np.zeros_like(Z)
+    for j in range(1, my - 1):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        rhs = Tp ** sig * (Tp * P(lapZ) + sig * sum(P(a) * P(b) for a, b in zip(tg, zg))) / (p.Re * sc)
+        pred[:, :, j] = h * _spec(rhs, nkx, mz)
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-8
+    assert np.abs(dZ[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
