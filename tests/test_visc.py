@@ -366,3 +366,21 @@ def test_three_dimensional_scalar_diffusion():
     inner = (slice(None), slice(None), slice(1, my - 1))
     assert np.abs(pred[inner]).max() > 1e-8
     assert np.abs(dZ[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
+
+
+def test_mass_with_variable_viscosity():
+    """Impermeable walls: the total mass (masst, the integral of the plane
+    mean of rho = 1/T) stays within 1e-5 of its start over 30 steps with
+    mu = T^0.7, as it does with constant viscosity."""
+    p, y, st = case(24, 24, 65)
+    out = []
+    for sig in (None, 0.7):
+        o = oracle_for(p, y, st, nthreads=4)
+        if sig is not None:
+            o.set_viscosity(sig)
+        m = []
+        for _ in range(30):
+            o.step(1)
+            m.append(o.diag()["masst"])
+        out.append(abs(m[-1] - m[0]) / m[0])
+    assert out[1] < 1e-5 and out[0] < 1e-5
