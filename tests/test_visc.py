@@ -384,3 +384,20 @@ def test_mass_with_variable_viscosity():
             m.append(o.diag()["masst"])
         out.append(abs(m[-1] - m[0]) / m[0])
     assert out[1] < 1e-5 and out[0] < 1e-5
+
+
+def test_extensions_golden():
+    """The oracle's scalar and variable-viscosity run against its committed
+    regression pin (tests/golden/make_extension_golden.py)."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_extension_golden as g
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "extensions_24x33x24.npz"))
+    s = g.run()
+    assert np.allclose(s["u00"], ref["u00"], rtol=0, atol=1e-13 * np.abs(ref["u00"]).max())
+    for k in g.FIELDS:
+        n = float(ref[k + "_norm"])
+        assert abs(np.linalg.norm(s[k]) - n) <= 1e-12 * n, k
+        got = s[k][g.sample_index(s[k].shape)]
+        assert np.abs(got - ref[k + "_sample"]).max() <= 1e-12 * n, k
