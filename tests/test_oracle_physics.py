@@ -1,0 +1,149 @@
+"""The oracle's Omega_y equation (trunk/lomacte3/src/cross.f:652-921) and
+T equation (cross.f:1625-1647) against the physics evaluated independently
+with numpy, on the CPU.
+
+State: Omega_y in two modes (so rho u = -i kz Omega/k^2, rho w = i kx
+Omega/k^2, rho v = 0), a shear profile in the 00 mode of rho u, a 3-D
+temperature.  numpy forms the velocity u_i = T rho u_i and the fluxes
+rho u_i u_j on the 3/2 grid, transforms and truncates them, and builds
+RHS(Omega_y) = i kz N_x - i kx N_z + lap(omega_y)/Re with N_i = -d_j(rho
+u_i u_j) and omega_y = i kz u - i kx w from the dealiased velocity (d/dy
+and d2/dy2 by the compact schemes the oracle exposes).  One substep's
+Omega_y increment (gamma_1 Deltat RHS, xi_1 = 0) must match it; the same
+for T with RHS(T) = -u.grad T + T lap T / Pe.
+"""
+import numpy as np
+
+from tests.helpers import case, oracle_for
+
+
+def _phys(c, mgalx, mgalz):
+    nkx, mz = c.shape
+    nz1 = (mz - 1) // 2
+    F = np.zeros((mgalz, mgalx), dtype=complex)
+    for i in range(nkx):
+        for k in range(mz):
+            kk = k if k <= nz1 else k - mz
+            F[kk % mgalz, i] += c[i, k]
+            if i > 0:
+                F[(-kk) % mgalz, (-i) % mgalx] += np.conj(c[i, k])
+    return np.real(np.fft.ifft2(F)) * mgalx * mgalz
+
+
+def _spec(plane, nkx, mz):
+    mgalz, mgalx = plane.shape
+    F = np.fft.fft2(plane) / (mgalx * mgalz)
+    out = np.zeros((nkx, mz), dtype=complex)
+    for k in range(mz):
+        out[:, k] = F[(k if k <= (mz - 1) // 2 else k - mz) % mgalz, :nkx]
+    return out
+
+
+def _state():
+    """Omega_y in three modes, a shear profile in rho u00, a 3-D T."""
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    nkx, mz, my = st["vor"].shape
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)
+    rng = np.random.default_rng(8)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    s["phi"][:] = 0
+    s["psi"][:] = 0
+    s["vor"][:] = 0
+    for (i, k) in ((1, 2), (2, mz - 1), (1, 0)):
+        s["vor"][i, k, :] = 0.05 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["u00"], s["v00"], s["w00"] = 0.5 * np.tanh(y / 2), np.zeros(my), np.zeros(my)
+    T = np.zeros_like(s["scal"])
+    T[0, 0, :] = st["scal"][0, 0, :]
+    for (i, k) in ((1, 0), (0, 2), (2, 1)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["scal"] = T
+    return p, y, s, kxv, kzv
+
+
+def _dy(o, a, f):
+    nkx, mz, _ = a.shape
+    r = np.zeros_like(a)
+    for i in range(nkx):
+        for k in range(mz):
+            r[i, k] = f(a[i, k].real) + 1j * f(a[i, k].imag)
+    return r
+
+
+def _momentum(p, s, kxv, kzv):
+    """rho u_i of the state (rho v = 0): -i kz Omega/k^2, i kx Omega/k^2,
+    the 00 profile in rho u; Omega_y with its wall values (cross.f:315-327)"""
+    vo = s["vor"].copy()
+    vo[:, :, 0], vo[:, :, -1] = vo[:, :, 1], vo[:, :, -2]
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    k2[0, 0] = 1.0
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    m = {"x": -IZ * vo / k2, "y": np.zeros_like(vo), "z": IX * vo / k2}
+    m["x"][0, 0], m["z"][0, 0] = s["u00"], 0.0
+    return m
+
+
+def test_vorticity_equation_against_numpy():
+    p, y, s, kxv, kzv = _state()
+    nkx, mz, my = s["vor"].shape
+    T = s["scal"]
+    o = oracle_for(p, y, s, nthreads=2)
+    o.substep(0)
+    h = p.dt * 8.0 / 15.0
+    got = (o.get_state()["vor"] - s["vor"]) / h
+
+    def dy(a, f):
+        return _dy(o, a, f)
+
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    m = _momentum(p, s, kxv, kzv)
+    pairs = ("xx", "xy", "xz", "yz", "zz")
+    M = {n: np.zeros_like(T) for n in pairs}
+    U = {c: np.zeros_like(T) for c in "xz"}
+    for j in range(my):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        mp = {c: P(m[c]) for c in "xyz"}
+        up = {c: mp[c] * Tp for c in "xyz"}
+        for n in pairs:
+            M[n][:, :, j] = _spec(mp[n[0]] * up[n[1]], nkx, mz)
+        for c in "xz":
+            U[c][:, :, j] = _spec(up[c], nkx, mz)
+    Nx = -(IX * M["xx"] + dy(M["xy"], o.deryr) + IZ * M["xz"])
+    Nz = -(IX * M["xz"] + dy(M["yz"], o.deryr) + IZ * M["zz"])
+    wy = IZ * U["x"] - IX * U["z"]
+    lap = dy(wy, o.deryyr) - k2 * wy
+    pred = IZ * Nx - IX * Nz + lap / p.Re
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-4
+    assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
+
+
+def test_temperature_equation_against_numpy():
+    """RHS(T) = -u.grad T + T lap T / Pe (cross.f:1631-1637) on the 3/2 grid,
+    transformed and truncated: one substep's Delta T (gamma_1 Deltat
+    RHS(T), the physical accumulator starting at zero)."""
+    p, y, s, kxv, kzv = _state()
+    nkx, mz, my = s["vor"].shape
+    T = s["scal"]
+    o = oracle_for(p, y, s, nthreads=2)
+    o.substep(0)
+    h = p.dt * 8.0 / 15.0
+    got = (o.get_state()["scal"] - T) / h
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    m = _momentum(p, s, kxv, kzv)
+    ty = _dy(o, T, o.deryr)
+    lap = _dy(o, T, o.deryyr) - k2 * T
+    pe = p.Re * float(np.float32(0.7))
+    pred = np.zeros_like(T)
+    for j in range(1, my - 1):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        rhs = -(P(m["x"]) * Tp * P(IX * T) + P(m["y"]) * Tp * P(ty) + P(m["z"]) * Tp * P(IZ * T)) + Tp * P(lap) / pe
+        pred[:, :, j] = _spec(rhs, nkx, mz)
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-5
+    assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
