@@ -1,6 +1,6 @@
-"""The oracle's Omega_y equation (trunk/lomacte3/src/cross.f:652-921) and
-T equation (cross.f:1625-1647) against the physics evaluated independently
-with numpy, on the CPU.
+"""The oracle's Omega_y and phi equations (trunk/lomacte3/src/
+cross.f:652-921) and T equation (cross.f:1625-1647) against the physics
+evaluated independently with numpy, on the CPU.
 
 State: Omega_y in two modes (so rho u = -i kz Omega/k^2, rho w = i kx
 Omega/k^2, rho v = 0), a shear profile in the 00 mode of rho u, a 3-D
@@ -10,7 +10,7 @@ RHS(Omega_y) = i kz N_x - i kx N_z + lap(omega_y)/Re with N_i = -d_j(rho
 u_i u_j) and omega_y = i kz u - i kx w from the dealiased velocity (d/dy
 and d2/dy2 by the compact schemes the oracle exposes).  One substep's
 Omega_y increment (gamma_1 Deltat RHS, xi_1 = 0) must match it; the same
-for T with RHS(T) = -u.grad T + T lap T / Pe.
+for phi and for T with RHS(T) = -u.grad T + T lap T / Pe.
 """
 import numpy as np
 
@@ -144,6 +144,44 @@ def test_temperature_equation_against_numpy():
         Tp = P(T)
         rhs = -(P(m["x"]) * Tp * P(IX * T) + P(m["y"]) * Tp * P(ty) + P(m["z"]) * Tp * P(IZ * T)) + Tp * P(lap) / pe
         pred[:, :, j] = _spec(rhs, nkx, mz)
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    assert np.abs(pred[inner]).max() > 1e-5
+    assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
+
+
+def test_phi_equation_against_numpy():
+    """RHS(phi) = -k^2 N_y - d/dy(i kx N_x + i kz N_z) - lap(i kz omega_x -
+    i kx omega_z)/Re (cross.f:748-921) with N_i = -d_j(rho u_i u_j) and the
+    vorticity of the dealiased velocity; here rho v = 0, so N_y = 0,
+    omega_x = dw/dy and omega_z = -du/dy."""
+    p, y, s, kxv, kzv = _state()
+    nkx, mz, my = s["vor"].shape
+    T = s["scal"]
+    o = oracle_for(p, y, s, nthreads=2)
+    o.substep(0)
+    h = p.dt * 8.0 / 15.0
+    got = (o.get_state()["phi"] - s["phi"]) / h
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    m = _momentum(p, s, kxv, kzv)
+    pairs = ("xx", "xy", "xz", "yz", "zz")
+    M = {n: np.zeros_like(T) for n in pairs}
+    U = {c: np.zeros_like(T) for c in "xz"}
+    for j in range(my):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        mp = {c: P(m[c]) for c in "xyz"}
+        up = {c: mp[c] * Tp for c in "xyz"}
+        for n in pairs:
+            M[n][:, :, j] = _spec(mp[n[0]] * up[n[1]], nkx, mz)
+        for c in "xz":
+            U[c][:, :, j] = _spec(up[c], nkx, mz)
+    Nx = -(IX * M["xx"] + _dy(o, M["xy"], o.deryr) + IZ * M["xz"])
+    Nz = -(IX * M["xz"] + _dy(o, M["yz"], o.deryr) + IZ * M["zz"])
+    wx, wz = _dy(o, U["z"], o.deryr), -_dy(o, U["x"], o.deryr)
+    cc = IZ * wx - IX * wz
+    lap = _dy(o, cc, o.deryyr) - k2 * cc
+    pred = -_dy(o, IX * Nx + IZ * Nz, o.deryr) - lap / p.Re
     inner = (slice(None), slice(None), slice(1, my - 1))
     assert np.abs(pred[inner]).max() > 1e-5
     assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
