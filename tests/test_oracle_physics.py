@@ -10,7 +10,9 @@ RHS(Omega_y) = i kz N_x - i kx N_z + lap(omega_y)/Re with N_i = -d_j(rho
 u_i u_j) and omega_y = i kz u - i kx w from the dealiased velocity (d/dy
 and d2/dy2 by the compact schemes the oracle exposes).  One substep's
 Omega_y increment (gamma_1 Deltat RHS, xi_1 = 0) must match it; the same
-for phi and for T with RHS(T) = -u.grad T + T lap T / Pe.
+for phi and for T with RHS(T) = -u.grad T + T lap T / Pe; and the
+divergence constraint: the d(rho)/dt source of the psi solve from the T
+update through rho = 1/T.
 """
 import numpy as np
 
@@ -185,3 +187,55 @@ def test_phi_equation_against_numpy():
     inner = (slice(None), slice(None), slice(1, my - 1))
     assert np.abs(pred[inner]).max() > 1e-5
     assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max()
+
+
+def test_divergence_constraint_against_numpy():
+    """A motionless state with a 3-D temperature: the d(rho)/dt source of
+    the psi solve (cross.f:1669-1673, rho = 1/T with T advanced by one
+    substep of conduction) evaluated with numpy on the 3/2 grid and
+    transformed; psi(n+1) of the oracle's substep equals the oracle's
+    Neumann Poisson solve (solvepsi) of that source, mode by mode."""
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    nkx, mz, my = st["vor"].shape
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)
+    rng = np.random.default_rng(9)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    for k in ("vor", "phi", "psi"):
+        s[k][:] = 0
+    for k in ("u00", "v00", "w00"):
+        s[k] = np.zeros_like(s[k])
+    T = np.zeros_like(s["scal"])
+    T[0, 0, :] = st["scal"][0, 0, :]
+    for (i, k) in ((1, 0), (0, 2), (2, 1), (1, mz - 1)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["scal"] = T
+    o = oracle_for(p, y, s, nthreads=2)
+    o.substep(0)
+    psi = o.get_state()["psi"]
+    # RK3 coefficients of the first substep (modulos.f:193-209)
+    gama0, p0 = 8.0 / 15.0, 5.0 / 66.0
+    beta0, alpha0 = gama0 - p0, p0
+    dtg, dtb, ab = p.dt * gama0, p.dt * beta0, alpha0 / beta0
+    pe = p.Re * float(np.float32(0.7))
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    lap = _dy(o, T, o.deryyr) - k2 * T
+    drho = np.zeros_like(T)
+    for j in range(my):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        rhs = Tp * P(lap) / pe
+        d8 = dtg * rhs
+        tn = Tp + d8
+        drho[:, :, j] = _spec((d8 / (Tp * tn)) / dtb - ab * rhs / (Tp * Tp), nkx, mz)
+    pred = np.zeros_like(psi)
+    for i in range(nkx):
+        for k in range(mz):
+            if i == 0 and k == 0:
+                continue
+            pred[i, k], _ = o.solvepsi(drho[i, k], float(k2[i, k, 0]))
+    mask = np.ones((nkx, mz), bool)
+    mask[0, 0] = False
+    assert np.abs(pred[mask]).max() > 1e-8
+    assert np.abs(psi[mask] - pred[mask]).max() < 1e-9 * np.abs(pred[mask]).max()
