@@ -239,3 +239,85 @@ def test_divergence_constraint_against_numpy():
     mask[0, 0] = False
     assert np.abs(pred[mask]).max() > 1e-8
     assert np.abs(psi[mask] - pred[mask]).max() < 1e-9 * np.abs(pred[mask]).max()
+
+
+def test_all_terms_with_phi():
+    """Omega_y and phi in several modes (rho v from the oracle's Lapvdvhom,
+    cross.f:365-372: rho u = (i kx dm_y/dy - i kz Omega)/k^2, rho v = m_y,
+    rho w = (i kz dm_y/dy + i kx Omega)/k^2), a shear profile, a 3-D T:
+    every advective term active.  One substep's increments of Omega_y, phi,
+    T and the 00 mode of rho u (its RHS -d(rho u v)_00/dy + d2(u_00)/dy2 /
+    Re, cross.f:686-722) against numpy."""
+    p, y, st = case(24, 24, 33, dt=1e-3)
+    nkx, mz, my = st["vor"].shape
+    kxv = p.alp * np.arange(nkx)
+    kzv = p.bet * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    env = np.exp(-y ** 2 / 8) * (1 - (y / y[-1]) ** 2)
+    rng = np.random.default_rng(10)
+    s = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    for k in ("vor", "phi", "psi"):
+        s[k][:] = 0
+    for (i, k) in ((1, 2), (2, mz - 1)):
+        s["vor"][i, k, :] = 0.05 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    for (i, k) in ((1, 1), (0, 3), (2, mz - 2)):
+        s["phi"][i, k, :] = 0.05 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["u00"], s["v00"], s["w00"] = 0.5 * np.tanh(y / 2), np.zeros(my), np.zeros(my)
+    T = np.zeros_like(s["scal"])
+    T[0, 0, :] = st["scal"][0, 0, :]
+    for (i, k) in ((1, 0), (0, 2), (2, 1)):
+        T[i, k, :] = 0.01 * (rng.standard_normal() + 1j * rng.standard_normal()) * env
+    s["scal"] = T
+    o = oracle_for(p, y, s, nthreads=2)
+    o.substep(0)
+    new = o.get_state()
+    h = p.dt * 8.0 / 15.0
+    IX, IZ = 1j * kxv[:, None, None], 1j * kzv[None, :, None]
+    k2 = kxv[:, None, None] ** 2 + kzv[None, :, None] ** 2
+    k2s = k2.copy()
+    k2s[0, 0] = 1.0
+    vo = s["vor"].copy()
+    vo[:, :, 0], vo[:, :, -1] = vo[:, :, 1], vo[:, :, -2]
+    my_, dmy = np.zeros_like(T), np.zeros_like(T)
+    for i in range(nkx):
+        for k in range(mz):
+            my_[i, k], dmy[i, k] = o.lapvdvhom(s["phi"][i, k], float(k2[i, k, 0]))
+    m = {"x": (IX * dmy - IZ * vo) / k2s, "y": my_, "z": (IZ * dmy + IX * vo) / k2s}
+    m["x"][0, 0], m["y"][0, 0], m["z"][0, 0] = s["u00"], 0.0, 0.0
+    pairs = ("xx", "xy", "xz", "yy", "yz", "zz")
+    M = {n: np.zeros_like(T) for n in pairs}
+    U = {c: np.zeros_like(T) for c in "xyz"}
+    RT = np.zeros_like(T)
+    ty = _dy(o, T, o.deryr)
+    lapT = _dy(o, T, o.deryyr) - k2 * T
+    pe = p.Re * float(np.float32(0.7))
+    for j in range(my):
+        P = lambda a: _phys(a[:, :, j], p.mgalx, p.mgalz)  # noqa: E731
+        Tp = P(T)
+        mp = {c: P(m[c]) for c in "xyz"}
+        up = {c: mp[c] * Tp for c in "xyz"}
+        for n in pairs:
+            M[n][:, :, j] = _spec(mp[n[0]] * up[n[1]], nkx, mz)
+        for c in "xyz":
+            U[c][:, :, j] = _spec(up[c], nkx, mz)
+        RT[:, :, j] = _spec(-(up["x"] * P(IX * T) + up["y"] * P(ty) + up["z"] * P(IZ * T)) + Tp * P(lapT) / pe,
+                            nkx, mz)
+    D = lambda a: _dy(o, a, o.deryr)  # noqa: E731
+    D2 = lambda a: _dy(o, a, o.deryyr)  # noqa: E731
+    Nx = -(IX * M["xx"] + D(M["xy"]) + IZ * M["xz"])
+    Ny = -(IX * M["xy"] + D(M["yy"]) + IZ * M["yz"])
+    Nz = -(IX * M["xz"] + D(M["yz"]) + IZ * M["zz"])
+    wx = D(U["z"]) - IZ * U["y"]
+    wy = IZ * U["x"] - IX * U["z"]
+    wz = IX * U["y"] - D(U["x"])
+    rhs_vor = IZ * Nx - IX * Nz + (D2(wy) - k2 * wy) / p.Re
+    cc = IZ * wx - IX * wz
+    rhs_phi = -k2 * Ny - D(IX * Nx + IZ * Nz) - (D2(cc) - k2 * cc) / p.Re
+    inner = (slice(None), slice(None), slice(1, my - 1))
+    for name, got, pred in (("vor", (new["vor"] - s["vor"]) / h, rhs_vor),
+                            ("phi", (new["phi"] - s["phi"]) / h, rhs_phi),
+                            ("scal", (new["scal"] - T) / h, RT)):
+        assert np.abs(pred[inner]).max() > 1e-5, name
+        assert np.abs(got[inner] - pred[inner]).max() < 1e-9 * np.abs(pred[inner]).max(), name
+    u00 = (new["u00"] - s["u00"]) / h
+    pred00 = -o.deryr(M["xy"][0, 0].real) + o.deryyr(U["x"][0, 0].real) / p.Re
+    assert np.abs(u00[1:-1] - pred00[1:-1]).max() < 1e-9 * np.abs(pred00[1:-1]).max()
