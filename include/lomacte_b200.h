@@ -283,11 +283,14 @@ int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev,
  * of cudaFree.  It has no counterpart in the reference.  It takes npencil
  * complex pencils of my points each (y fastest, re/im interleaved) at
  * in_dev and writes d/dy to out_dev on `stream` (a cudaStream_t; NULL for
- * the default stream).  Its operator tables live in one fixed 256 KiB
- * device array per device (no cudaMalloc/cudaFree): my <= 544, larger
- * returns LMC_EINVAL.  The array is shared by all calls and overwritten by
- * each; calls that overlap on the GPU race on it.  The first call on a
- * device takes the array's address and should precede any stream capture. */
+ * the default stream).  in_dev and out_dev must be 16-byte aligned and must
+ * not overlap.  Its operator tables live in one fixed 256 KiB device array
+ * per device (no cudaMalloc/cudaFree): my <= 544, larger returns
+ * LMC_EINVAL.  The array is shared by all calls and overwritten by each;
+ * calls that overlap on the GPU race on it.  The first call in a CUDA
+ * context takes the array's address and should precede any stream capture;
+ * while `stream` is being captured the call returns LMC_EINVAL (its table
+ * upload reads a host buffer that is released on return). */
 int lmc_deryr2_noalloc(int my, const double *y, int npencil,
                        const double *in_dev, double *out_dev, void *stream);
 

@@ -14,21 +14,30 @@
 //   * The scratch array is LMC_NOALLOC_SCRATCH_BYTES (256 KiB) per device;
 //     a grid whose tables do not fit (my > 544, the largest pencil one warp
 //     handles) is rejected with LMC_EINVAL before anything is launched.
+//   * in_dev and out_dev must be 16-byte aligned (the kernel moves whole
+//     complex values) and must not overlap; otherwise LMC_EINVAL, with
+//     nothing launched.
 //   * The array is shared by every call on a device and keeps the contents
 //     of the last call.  Each call rewrites the whole table region it reads
 //     (zero entries included), so nothing depends on earlier contents.
 //     Calls that overlap on the GPU (different streams, or another host
 //     thread) race on the array: serialise them.
-//   * The first call on a device (with that device current) looks up the
-//     array's device address with cudaGetSymbolAddress and caches it; make
-//     that first call before any stream capture starts.
-//   * No cudaMalloc, cudaFree or other device allocation is made; the host
-//     side builds the tables in host memory and copies them with
-//     cudaMemcpyAsync on the caller's stream.
+//   * The first call in a CUDA context (with that device current) looks up
+//     the array's device address with cudaGetSymbolAddress and caches it
+//     for that context; make that first call before any stream capture
+//     starts.
+//   * The tables are built in host memory and copied with cudaMemcpyAsync
+//     from a buffer that is released when the call returns, so the call
+//     returns LMC_EINVAL while `stream` is being captured (a captured copy
+//     would read the released buffer when the graph is replayed).
+//   * No cudaMalloc, cudaFree or other device allocation is made.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
+#include <map>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "lmc_internal.h"
@@ -46,7 +55,27 @@ constexpr int LMC_NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[LMC_NOALLOC_SCRATCH_BYTES];
 
 std::mutex g_mu;
-void *g_scratch_ptr[LMC_NOALLOC_MAX_DEVICES] = {nullptr};
+// device address of the array per (device, CUDA context): a context made
+// after cudaDeviceReset, or a non-primary one, gets its own look-up
+std::map<std::pair<int, void *>, void *> g_scratch_ptr;
+
+// the calling thread's current CUDA context (driver entry point reached
+// through the runtime, so the library does not link libcuda itself)
+void *current_context() {
+  using GetCtx = int (*)(void **);
+  static GetCtx fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (GetCtx)f;
+  });
+  void *ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 struct View {
   const double *dt12, *p1L, *p1U, *fmap, *k1L, *k1U;
@@ -89,21 +118,24 @@ int chunks(int my, int &C, int &lpm, int &base, int &extra) {
   return LMC_OK;
 }
 
-// device address of the scratch array on the current device (set-up once)
+// device address of the scratch array in the current context (set-up once
+// per device and context)
 int scratch_ptr(void **out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= LMC_NOALLOC_MAX_DEVICES) return LMC_ECUDA;
+  const std::pair<int, void *> key(dev, current_context());
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  auto it = g_scratch_ptr.find(key);
+  if (it == g_scratch_ptr.end()) {
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       std::fprintf(stderr, "lomacte_b200: scratch symbol address: %s\n", cudaGetErrorString(e));
       return LMC_ECUDA;
     }
-    g_scratch_ptr[dev] = p;
+    it = g_scratch_ptr.emplace(key, p).first;
   }
-  *out = g_scratch_ptr[dev];
+  *out = it->second;
   return LMC_OK;
 }
 
@@ -118,6 +150,23 @@ extern "C" int lmc_deryr2_noalloc(int my, const double *y, int npencil, const do
     return LMC_EINVAL;
   }
   if (npencil == 0) return LMC_OK;
+  const uintptr_t ia = (uintptr_t)in_dev, oa = (uintptr_t)out_dev;
+  if ((ia | oa) & 15) {
+    std::fprintf(stderr, "lomacte_b200: lmc_deryr2_noalloc: in_dev and out_dev must be 16-byte aligned\n");
+    return LMC_EINVAL;
+  }
+  const uintptr_t nb = (uintptr_t)npencil * (uintptr_t)my * sizeof(double2);
+  if (ia < oa + nb && oa < ia + nb) {
+    std::fprintf(stderr, "lomacte_b200: lmc_deryr2_noalloc: in_dev and out_dev overlap\n");
+    return LMC_EINVAL;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return LMC_ECUDA;
+  if (cs != cudaStreamCaptureStatusNone) {
+    std::fprintf(stderr, "lomacte_b200: lmc_deryr2_noalloc: the stream is being captured\n");
+    return LMC_EINVAL;
+  }
   // operator tables in host memory (the host code of lmc_create)
   std::vector<double> pack;
   size_t off[6];
@@ -145,7 +194,6 @@ extern "C" int lmc_deryr2_noalloc(int my, const double *y, int npencil, const do
   void *scr = nullptr;
   int rc = scratch_ptr(&scr);
   if (rc) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemcpyAsync(scr, pack.data(), pack.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return LMC_ECUDA;
   const double *base_ptr = (const double *)scr;

@@ -35,6 +35,22 @@ def test_strerror_and_nodev_paths():
     assert L.lmc_strerror(-6) == b"no CUDA device"
 
 
+def test_noalloc_rejects_bad_pointers_before_any_launch():
+    """lmc_deryr2_noalloc checks alignment and overlap on the host: these
+    pointer values are never dereferenced, so no device is needed."""
+    y = stretched_mesh(65)
+    n = 4
+    nb = n * 65 * 16
+    base = 1 << 20
+    # an input one double off the 16-byte grid
+    assert lm.deryr2_noalloc(y, n, base + 8, base + 4 * nb) == lm.LMC_EINVAL
+    # in place, and overlapping by one complex value
+    assert lm.deryr2_noalloc(y, n, base, base) == lm.LMC_EINVAL
+    assert lm.deryr2_noalloc(y, n, base, base + nb - 16) == lm.LMC_EINVAL
+    # beyond the scratch array's largest pencil
+    assert lm.deryr2_noalloc(stretched_mesh(545), 1, base, base + 4 * nb) == lm.LMC_EINVAL
+
+
 def test_create_without_gpu_fails_loudly():
     try:
         import torch
