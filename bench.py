@@ -1,29 +1,36 @@
 #!/usr/bin/env python
 """Benchmark of the lomacte RK3 step on B200 (Mpts.RK3-steps/s).
 
-Workload (default): nx = nz = 256 Fourier modes (3/2 dealiased: mgalx =
-mgalz = 384), ny = 257 on y = 12 sinh(2 eta)/sinh(2), seeded initial
-condition (s = 4, Re = 160, amp 1e-2 on |k| <= 8), fixed Deltat = 0.01,
-Pr = Sc = 0.7, mu = k = rho D = T^0.7 and a passive scalar Z = (T -
-T_bot)/(T_top - T_bot) (both extensions of the lomacte3 substep;
-``--no-scalar --sigma -1`` gives the substep exactly as lomacte3 has it).
-One "step" = one full RK3 step (3 substeps).  The metric is
-(nx*ny*nz/1e6) * steps / seconds, measured for the mixed-precision form
-(the headline value) and the FP64 plain path (reported beside it, with the
-ratio and the relative L2 difference of the two final states).
+Workload (default, ``--workload large``): the large single run of the
+low-Mach temporal mixing layer, nx = nz = 768 Fourier modes (3/2
+dealiased: mgalx = mgalz = 1152), ny = 513 on y = 12 sinh(2 eta)/sinh(2),
+Lx = Lz = 8 pi, seeded initial condition (density ratio s = T2/T1 = 8,
+seed 1, rms 1e-2 on |k| <= 8 windowed by exp(-y^2/4)), Re = 800, Deltat
+from CFL = 0.5 (recomputed every 10 steps, initial Deltat 1e-4 as the
+reference), Pr = Sc = 0.7, mu = k = rho D = T^0.7 and a passive scalar
+Z = 0.5 (1 + tanh(y/2)).  ``--workload medium`` is the 256^2 x 257 run
+(s = 4, Re = 160, Deltat = 0.01, seed 0) with the same physics, and its
+line is also reported beside the headline (``medium_grid``).  One "step"
+= one full RK3 step (3 substeps).  The metric is (nx*ny*nz/1e6) * steps /
+seconds, measured for the mixed-precision form (the headline value) and
+the FP64 plain path (reported beside it, with the ratio and the relative
+L2 difference of the two final states), and on the medium grid the
+difference of the two forms after 1000 steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision both|mixed|fp64]
+                    [--workload large|medium] [--precision both|mixed|fp64]
 
 N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
 time is the max over ranks and the value the aggregate over ranks.
 ``--impl reference`` times the CPU restatement of the reference algorithm
-(the reference Fortran cannot be built in this environment) on the host
-cores, on bounded samples (one RK3 substep each) of the same workload.
+(the reference Fortran cannot be built in this environment: no Fortran
+compiler, no MPI) on the host cores, on bounded samples of the same
+workload (see ``cpu_sample``); it never loads the product library.
 """
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -37,7 +44,22 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from loma_phd_b200.replicas import case_seed, job_throughput, max_over_ranks  # noqa: E402
+from loma_phd_b200.replicas import job_throughput, max_over_ranks  # noqa: E402
+
+# The two mixing-layer workloads (hre.dat-equivalent parameters).  y_cpu
+# and the strides are the bounded CPU samples: the oracle runs on the same
+# x/z grid with y_cpu of the y points (its per-point cost does not depend
+# on ny: every y solve is banded, every transform is per y row) and visits
+# 1/stride of a substep's modes, planes and lines (lmo_set_sample).
+WORKLOADS = {
+    "large": dict(nx=768, nz=768, ny=513, s=8.0, Re=800.0, seed=1, dt_mode=0, dt=1e-4, cfl=0.5, ncfl=10,
+                  y_cpu=65, cpu_stride=2, ref_stride=8,
+                  desc="768^2 x 513 modes (mgal 1152^2), s=8, Re=800, seed 1, Deltat from CFL=0.5 every 10 steps"),
+    "medium": dict(nx=256, nz=256, ny=257, s=4.0, Re=160.0, seed=0, dt_mode=1, dt=0.01, cfl=0.5, ncfl=10,
+                   y_cpu=257, cpu_stride=4, ref_stride=16,
+                   desc="256^2 x 257 modes (mgal 384^2), s=4, Re=160, Deltat=0.01"),
+}
+PR = float(np.float32(0.7))  # Pr = Sc = 0.7f (main.f:569)
 
 # Algorithmic HBM bytes per launch, in units of the spectral (S = nplanes *
 # mz * ny complex), z-padded (Z = nplanes * mgalz * ny complex) and physical
@@ -74,19 +96,12 @@ ALGO = {
     "psi": lambda S, Z, P, w, sc, vs: S * 16 + S * w + S * 7 * 8 // 2,
 }
 
-# DRAM bytes (read + write) per launch measured by ncu (full-set captures
-# of the 256x65x256 case of each workload, one launch per kernel).  Traffic
-# grows in proportion to ny at fixed x/z sizes, so for nx = nz = 256 it is
-# scaled by ny/65; other sizes, and kernels not captured, report null.
-# Keyed by (FP64 form, passive scalar, variable viscosity).
-NCU_TRAFFIC_256x65 = {
-    (True, 0, 0): {  # zinv: its two launches of a substep together
-        "zinv": 553.0e6, "xphys": 1064.5e6, "zfwd": 903.9e6, "post1": 609.9e6, "post2": 956.2e6},
-    (False, 0, 0): {
-        "zinv": 217.7e6, "xphys": 584.0e6, "zfwd": 433.6e6, "post1": 410.3e6, "post2": 768.8e6},
-    (True, 1, 1): {"xphys": 1791.0e6},
-    (False, 1, 1): {"xphys": 1026.2e6},
-}
+# DRAM bytes (read + write) per launch measured by ncu, by (workload, FP64
+# form): full-set captures of one launch on a case of the same x/z grid
+# with fewer y points (profiles/), scaled to a full launch by ny, as every
+# kernel's traffic grows in proportion to ny at fixed x/z sizes.  None:
+# not captured for that kernel.
+NCU_TRAFFIC = {}
 
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
                2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
@@ -98,13 +113,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--nx", type=int, default=256)
-    ap.add_argument("--nz", type=int, default=256)
-    ap.add_argument("--ny", type=int, default=257)
+    ap.add_argument("--workload", default="large", choices=tuple(WORKLOADS))
+    ap.add_argument("--ny", type=int, default=0, help="override the workload's ny (profiling of small cases)")
     ap.add_argument("--precision", default="both", choices=("both", "mixed", "fp64"),
                     help="both: time the FP64 and the mixed form; the headline value is the mixed form")
     ap.add_argument("--mixed-form", type=int, default=1, choices=(1, 2),
                     help="1: FP32 FFT arithmetic; 2: FP64 FFT arithmetic on FP32 storage")
+    ap.add_argument("--no-medium", action="store_true", help="skip the medium-grid line beside the headline")
+    ap.add_argument("--error-steps", type=int, default=1000,
+                    help="steps of the medium-grid mixed-vs-FP64 error run (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=16,
                     help="requests of the synthetic serving stream (0: skip)")
     ap.add_argument("--serve-scale", type=float, default=0.05,
@@ -123,6 +140,15 @@ def parse():
     if a.sigma < 0:
         a.sigma = None
     return a
+
+
+def wl(a, name=None):
+    """The workload's parameters (ny overridden by --ny for the main one)."""
+    w = dict(WORKLOADS[name or a.workload])
+    if name is None and a.ny:
+        w["ny"] = a.ny
+        w["y_cpu"] = min(w["y_cpu"], a.ny)
+    return w
 
 
 def peaks():
@@ -189,8 +215,8 @@ class ClockSampler:
         return out
 
 
-def mpts(a):
-    return a.nx * a.ny * a.nz / 1e6
+def mpts(w, ny=None):
+    return w["nx"] * (ny or w["ny"]) * w["nz"] / 1e6
 
 
 def sizes(p):
@@ -200,96 +226,112 @@ def sizes(p):
     return S, Z, P
 
 
-def scalar_ic(st):
-    """Z = (T - T_bot)/(T_top - T_bot): the passive scalar of the workload."""
-    T = st["scal"]
-    tb, tt = T[0, 0, 0].real, T[0, 0, -1].real
-    z = T / (tt - tb)
-    z[0, 0, :] -= tb / (tt - tb)
+def mixing_scalar(shape, y):
+    """Z = 0.5 (1 + tanh(y/2)): the kx = kz = 0 mode of the spectral Z."""
+    z = np.zeros(shape, dtype=np.complex128)
+    z[0, 0, :] = 0.5 * (1.0 + np.tanh(np.asarray(y) / 2.0))
     return z
 
 
-def oracle_case(a, p, y, st, nth):
-    """The oracle set up with the workload's extensions (Sc = Pr = 0.7f)."""
-    from oracle.oracle import Oracle
-    o = Oracle(p.mgalx, p.mgalz, y, p.Re, p.alp, p.bet, dtmode=p.dt_mode, dt0=p.dt, nthreads=nth)
-    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
-    if a.scalar:
-        o.set_scalar(scalar_ic(st), float(np.float32(0.7)))
-    if a.sigma is not None:
-        o.set_viscosity(a.sigma)
-    return o
-
-
 def extensions(a):
-    e = (" + passive scalar" if a.scalar else "") + (f" + mu = T^{a.sigma:g}" if a.sigma is not None else "")
+    e = (" + passive scalar Z=0.5(1+tanh(y/2)), Sc=0.7" if a.scalar else "") + \
+        (f" + mu = T^{a.sigma:g}" if a.sigma is not None else "")
     return e
 
 
-def cpu_baseline(a, p, y, st):
-    """The FP64 CPU restatement (oracle) on the host cores: a bounded sample
-    of the same workload (one RK3 substep), scaled to steps."""
-    nth = os.cpu_count() or 1
-    o = oracle_case(a, p, y, st, nth)
+def config(a, w, form):
+    return {"workload": f"lomacte {form}{extensions(a)}, Pr=0.7, {w['desc']}",
+            "grid": f"{w['nx']}x{w['ny']}x{w['nz']}", "parallelism": "replicas",
+            "l2": "inputs larger than L2"}
+
+
+def mesh(ny):
+    eta = np.linspace(-1.0, 1.0, ny)
+    return 12.0 * np.sinh(2.0 * eta) / np.sinh(2.0)
+
+
+def cpu_sample(a, w, stride, nth, warmup, nsamples):
+    """Bounded CPU samples of the workload with the FP64 oracle: the same
+    x/z grid, y_cpu of its y points, 1/stride of each substep's modes,
+    kx planes and physical lines (timing only; never the product library).
+    Returns (value in Mpts*RK3-steps/s, seconds per sample, description)."""
+    from oracle.ic import make_ic as oracle_ic
+    from oracle.oracle import Oracle
+    ny = w["y_cpu"]
+    y = mesh(ny)
+    mgx, mgz = 3 * w["nx"] // 2, 3 * w["nz"] // 2
+    st = oracle_ic(mgx, mgz, y, s=w["s"], seed=w["seed"])
+    o = Oracle(mgx, mgz, y, w["Re"], 0.25, 0.25, cfl=w["cfl"], ncfl=w["ncfl"], dtmode=w["dt_mode"], dt0=w["dt"],
+               nthreads=nth)
+    o.set_state(st["vor"], st["phi"], st["psi"], st["scal"], st["u00"], st["v00"], st["w00"])
+    if a.scalar:
+        o.set_scalar(mixing_scalar(o.shape, y), PR)
+    if a.sigma is not None:
+        o.set_viscosity(a.sigma)
+    del st
+    k = 0
+
+    def one():
+        nonlocal k
+        o.set_sample(stride, k % stride)
+        o.substep(k % 3)
+        k += 1
+    for _ in range(warmup):
+        one()
     t0 = time.perf_counter()
-    o.substep(0)
+    for _ in range(nsamples):
+        one()
     dt = time.perf_counter() - t0
-    steps = 1.0 / 3.0
-    return {"value": mpts(a) * steps / dt, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port",
-            "sample": f"one RK3 substep of the {a.nx}x{a.ny}x{a.nz} workload ({dt:.2f} s), FP64 CPU "
-                      f"restatement of cross.f:307-1141 with OpenMP ({nth} threads)"}
+    val = mpts(w, ny) * nsamples / (3.0 * stride) / dt
+    desc = (f"{nsamples} sample(s), each 1/{stride} of one RK3 substep (every {stride}th mode, kx plane and "
+            f"physical line) of the {w['nx']}x{ny}x{w['nz']} case ({ny} of the workload's {w['ny']} y points; "
+            f"per-point cost independent of ny), FP64 CPU restatement of cross.f:307-1141 with OpenMP "
+            f"({nth} threads), {dt / nsamples:.2f} s per sample")
+    return val, dt / nsamples, desc
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from loma_phd_b200 import ICParams, Params, make_ic, stretched_mesh
-    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01)
-    y = stretched_mesh(p.my)
-    st = make_ic(p, y, ICParams(s=4.0, seed=0))
+    w = wl(a)
     nth = os.cpu_count() or 1
-    o = oracle_case(a, p, y, st, nth)
-    for _ in range(a.warmup):
-        o.substep(0)
-    t0 = time.perf_counter()
-    for k in range(a.steps):
-        o.substep(k % 3)
-    dt = time.perf_counter() - t0
-    steps = a.steps / 3.0
-    val = mpts(a) * steps / dt
+    val, per, desc = cpu_sample(a, w, w["ref_stride"], nth, a.warmup, a.steps)
     line = {
         "impl": "reference", "metric": "Mpts*RK3-steps/s", "value": val, "unit": "Mpts*RK3-steps/s",
-        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / steps,
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * per,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded initial condition)",
-        "config": {"workload": f"lomacte FP64{extensions(a)} {a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), "
-                               f"s=4, Re=160, dt=0.01",
-                   "sample": "each step = one RK3 substep", "l2": "inputs larger than L2"},
+        "config": dict(config(a, w, "FP64 CPU restatement"), sample="each step = one bounded sample (cpu_baseline)"),
         "cpu_baseline": {"value": val, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port",
-                         "sample": f"{a.steps} RK3 substeps of the workload, FP64 CPU restatement "
-                                   f"(the Fortran reference cannot be compiled here), {nth} threads"},
+                         "sample": desc + " (the Fortran reference cannot be compiled here)"},
         "e2e": {"value": val, "unit": "Mpts*RK3-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_arm(a, prec, dev, rank, world, dist, want_e2e):
-    """Warm up, time K steps of one form (prec 0: FP64, 1: mixed) with CUDA
-    events, then optionally the end-to-end loop through the public API."""
-    import torch
+def make_case(a, w, prec, dev, rank):
     from loma_phd_b200 import ICParams, Lomacte, Params, make_ic, stretched_mesh
-    from loma_phd_b200.lomacte import KERNEL_NAMES
-
-    p = Params.from_modes(a.nx, a.nz, a.ny, dt_mode=1, dt=0.01, device=dev, precision=prec,
-                          scalar=1 if a.scalar else 0, visc=0 if a.sigma is None else 1,
-                          sigma=a.sigma or 0.0)
+    p = Params.from_modes(w["nx"], w["nz"], w["ny"], Re=w["Re"], dt_mode=w["dt_mode"], dt=w["dt"], cfl=w["cfl"],
+                          ncfl=w["ncfl"], device=dev, precision=prec, scalar=1 if a.scalar else 0,
+                          visc=0 if a.sigma is None else 1, sigma=a.sigma or 0.0)
     y = stretched_mesh(p.my)
-    st = make_ic(p, y, ICParams(s=4.0, seed=case_seed(rank)))
+    st = make_ic(p, y, ICParams(s=w["s"], seed=w["seed"] + rank))
     g = Lomacte(p, y)
     g.load_state(st)
-    if a.scalar:  # Z = (T - T_bot)/(T_top - T_bot), Sc = Pr
-        g.load_scalar(scalar_ic(st))
+    z = mixing_scalar(p.shape, y) if a.scalar else None
+    if a.scalar:
+        g.load_scalar(z)
+    return p, y, st, z, g
+
+
+def run_arm(a, w, prec, dev, rank, world, dist, want_e2e, steps, warmup, stats_cost=True):
+    """Warm up, time K steps of one form (prec 0: FP64, 1/2: mixed) with CUDA
+    events, then optionally the end-to-end loop through the public API."""
+    import torch
+    from loma_phd_b200.lomacte import KERNEL_NAMES
+
+    p, y, st, z0, g = make_case(a, w, prec, dev, rank)
     g_launches = g.launches_per_step
     y_family = g.y_family
     stream = torch.cuda.ExternalStream(g.stream, device=dev)
@@ -298,7 +340,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
         if dist is not None:
             dist.barrier()
 
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         g.step(1)
     g.sync()
     clocks = ClockSampler(dev)
@@ -309,18 +351,19 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
     e1 = torch.cuda.Event(enable_timing=True)
     g.profile_start()
     e0.record(stream)
-    g.step(a.steps)
+    g.step(steps)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     prof = g.profile_read()
     ck = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
-    value = job_throughput(mpts(a), a.steps, world, ms / 1e3)
+    value = job_throughput(mpts(w), steps, world, ms / 1e3)
     diag = g.diag()
-    if not np.isfinite(diag["dm"]):
-        raise RuntimeError("non-finite diagnostics after the timed steps")
+    if not np.isfinite(diag["dm"]) or diag["status"] != 0:
+        raise RuntimeError(f"bad diagnostics after the timed steps: {diag}")
     state = g.get_state()
+    zf = g.get_scalar() if a.scalar else None
 
     # end-to-end through the public API with host buffers: every step loads
     # the state (and the scalar) from pinned host memory, advances one RK3
@@ -334,7 +377,7 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
                for k in ("u00", "v00", "w00")}
         ptrs = [host[k].data_ptr() for k in ("vor", "phi", "psi", "scal")] + \
                [h00[k].data_ptr() for k in ("u00", "v00", "w00")]
-        zh = torch.from_numpy(np.ascontiguousarray(scalar_ic(st)).view(np.float64).copy()).pin_memory() \
+        zh = torch.from_numpy(np.ascontiguousarray(z0).view(np.float64).copy()).pin_memory() \
             if a.scalar else None
 
         def e2e_step():
@@ -346,44 +389,46 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
             if zh is not None:
                 g.get_scalar_ptr(zh.data_ptr())
 
-        ne = max(1, min(a.steps, 5))
-        for _ in range(2):
-            e2e_step()
+        ne = max(1, min(steps, 3))
+        e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(ne):
             e2e_step()
         el = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{dev}")
         nbytes = (5 if a.scalar else 4) * S * 16 + 3 * p.my * 8
-        e2e = {"value": mpts(a) * ne * world / el, "unit": "Mpts*RK3-steps/s",
+        e2e = {"value": mpts(w) * ne * world / el, "unit": "Mpts*RK3-steps/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ne}
+        del host, h00, zh
 
     # cost of a statistics step (addstats1/2 and the phys2 sums at the first
     # substep, lmc_stats_step) beside a plain step, CUDA events on the
     # library's stream, best of three each; plain steps replay a CUDA graph,
     # statistics steps enqueue their kernels directly
-    def one(fn):
-        g.sync()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        fn(1)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        return s0.elapsed_time(s1)
-    g.stats_reset([(p.my + 1) // 2])
-    t_plain = min(one(g.step) for _ in range(3))
-    t_stats = min(one(g.stats_step) for _ in range(3))
-    stats_step = {"plain_step_ms": t_plain, "stats_step_ms": t_stats, "spectra_planes": 1}
+    stats_step = None
+    if stats_cost:
+        def one(fn):
+            g.sync()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            fn(1)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            return s0.elapsed_time(s1)
+        g.stats_reset([(p.my + 1) // 2])
+        t_plain = min(one(g.step) for _ in range(3))
+        t_stats = min(one(g.stats_step) for _ in range(3))
+        stats_step = {"plain_step_ms": t_plain, "stats_step_ms": t_stats, "spectra_planes": 1}
     g.close()
 
     # roofline of the dominant kernel, live CUDA-event times of the timed region
-    w = 16 if prec == 0 else 8
+    wb = 16 if prec == 0 else 8
     top = max((k for k in KERNEL_NAMES if k in ALGO), key=lambda k: prof[k][0])
     tot_ms, cnt = prof[top]
     avg_s = tot_ms / max(cnt, 1) / 1e3
     sc, vs = int(a.scalar), int(a.sigma is not None)
-    algo = ALGO[top](S, Z, P, w, sc, vs)
+    algo = ALGO[top](S, Z, P, wb, sc, vs)
     peak, kind = peaks()
     achieved = algo / avg_s / 1e9
     # fraction of the timed region during which each kernel group runs; the
@@ -398,23 +443,61 @@ def run_arm(a, prec, dev, rank, world, dist, want_e2e):
               "rhs_and_rk3_update": ("post2",)}
     tot = sum(share.get(k, 0.0) for ks in stages.values() for k in ks)
     stage_share = {n: round(sum(share.get(k, 0.0) for k in ks) / max(tot, 1e-12), 4) for n, ks in stages.items()}
-    traffic = None
-    table = NCU_TRAFFIC_256x65.get((prec == 0, sc, vs), {}) if prec in (0, 1) else {}
-    if a.nx == 256 and a.nz == 256 and top in table:
-        traffic = table[top] * a.ny / 65.0
+    tr = NCU_TRAFFIC.get((a.workload, prec == 0, sc, vs), {}).get(top)
+    traffic = tr[0] * p.my / tr[1] if tr else None
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at "
-                                  "256x65x256, scaled by ny/65" if traffic else None,
+                "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at ny={tr[1]}, "
+                                  f"scaled by ny" if tr else None,
                 "algo_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3}
-    launches = g_launches
-    step_bytes = 3 * sum(f(S, Z, P, w, sc, vs) for f in ALGO.values())
-    return {"p": p, "y": y, "st": st, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
-            "kernel_share": share, "stage_share": stage_share, "e2e": e2e, "state": state, "diag": diag,
-            "step_bytes": step_bytes,
-            "stats_step": stats_step,
-            "launches_per_step": launches, "y_family": y_family,
-            "step_roofline_frac": (step_bytes * a.steps / (ms / 1e3) / 1e9) / peak}
+    step_bytes = 3 * sum(f(S, Z, P, wb, sc, vs) for f in ALGO.values())
+    return {"p": p, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
+            "kernel_share": share, "stage_share": stage_share, "e2e": e2e, "state": state, "Z": zf, "diag": diag,
+            "step_bytes": step_bytes, "stats_step": stats_step,
+            "launches_per_step": g_launches, "y_family": y_family,
+            "step_roofline_frac": (step_bytes * steps / (ms / 1e3) / 1e9) / peak}
+
+
+def state_errors(m, r):
+    """Relative L2 difference per field of two final states (v00 and w00,
+    second-order small, against the size of u00)."""
+    out = {}
+    for k in ("vor", "phi", "psi", "scal", "u00", "v00", "w00"):
+        den = np.linalg.norm(r["state"][k])
+        if k in ("v00", "w00"):
+            den = max(den, np.linalg.norm(r["state"]["u00"]))
+        out[k] = float(np.linalg.norm(np.asarray(m["state"][k]) - np.asarray(r["state"][k])) / den)
+    if m.get("Z") is not None and r.get("Z") is not None:
+        out["Z"] = float(np.linalg.norm(m["Z"] - r["Z"]) / np.linalg.norm(r["Z"]))
+    return out
+
+
+def error_run(a, dev, nsteps):
+    """Both forms advanced nsteps from the same seeded state of the medium
+    grid: relative L2 per field, the largest relative difference of the
+    momentum-thickness history, and the time per step of each form."""
+    import torch
+    w = wl(a, "medium")
+    res = {}
+    for prec in (0, a.mixed_form):
+        p, y, st, z0, g = make_case(a, w, prec, dev, 0)
+        dm = []
+        s = torch.cuda.ExternalStream(g.stream, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for n in range(nsteps // 50):
+            g.step(50)
+            dm.append(g.diag()["dm"])
+        e1.record(s)
+        torch.cuda.synchronize()
+        res[prec] = {"state": g.get_state(), "Z": g.get_scalar() if a.scalar else None, "dm": np.array(dm),
+                     "ms": e0.elapsed_time(e1) / max(1, nsteps // 50 * 50)}
+        g.close()
+    m, r = res[a.mixed_form], res[0]
+    dmerr = float(np.abs(m["dm"] - r["dm"]).max() / np.abs(r["dm"]).max()) if len(r["dm"]) else None
+    return {"steps": nsteps // 50 * 50, "grid": f"{w['nx']}x{w['ny']}x{w['nz']}", "form": a.mixed_form,
+            "rel_l2": state_errors(m, r), "dm_history_max_rel": dmerr,
+            "ms_per_step": {"mixed": m["ms"], "fp64": r["ms"]}, "note": "mixed vs FP64 GPU path, same seeded state"}
 
 
 def run_serving(a, dev):
@@ -458,6 +541,19 @@ def run_ensemble(a, dev):
     return out
 
 
+def medium_line(a, dev):
+    """The medium grid (256^2 x 257) beside the headline: both forms, short."""
+    w = wl(a, "medium")
+    arms = {prec: run_arm(a, w, prec, dev, 0, 1, None, False, 10, 3, stats_cost=False)
+            for prec in (0, a.mixed_form)}
+    m, r = arms[a.mixed_form], arms[0]
+    out = {"config": config(a, w, MIXED_NAMES[a.mixed_form]), "value": m["value"], "ms_per_step": m["ms"] / 10,
+           "fp64": {"value": r["value"], "ms_per_step": r["ms"] / 10, "roofline": r["roofline"]},
+           "mixed_over_fp64": m["value"] / r["value"], "roofline": m["roofline"], "clocks": m["clocks"],
+           "stage_share": m["stage_share"], "steps": 10, "warmup": 3}
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -476,20 +572,26 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
+    w = wl(a)
 
-    forms = {"mixed": [1], "fp64": [0], "both": [0, 1]}[a.precision]
-    arms = {prec: run_arm(a, a.mixed_form if prec else 0, dev, rank, world, dist, not a.no_e2e) for prec in forms}
-    head = arms[1] if 1 in arms else arms[0]
-    errs = None
-    if 0 in arms and 1 in arms:
-        # same seeded state advanced warmup + steps + e2e steps by both forms
-        errs = {}
-        ref = arms[0]["state"]
-        for k in ("vor", "phi", "psi", "scal", "u00", "v00", "w00"):
-            den = np.linalg.norm(ref[k])
-            if k in ("v00", "w00"):  # measured against the size of u00
-                den = max(den, np.linalg.norm(ref["u00"]))
-            errs[k] = float(np.linalg.norm(np.asarray(arms[1]["state"][k]) - np.asarray(ref[k])) / den)
+    forms = {"mixed": [a.mixed_form], "fp64": [0], "both": [0, a.mixed_form]}[a.precision]
+    arms = {}
+    for prec in forms:  # one case on the device at a time
+        arms[prec] = run_arm(a, w, prec, dev, rank, world, dist, not a.no_e2e, a.steps, a.warmup)
+        gc.collect()
+    mixed = a.mixed_form in arms
+    head = arms[a.mixed_form] if mixed else arms[0]
+    errs = state_errors(arms[a.mixed_form], arms[0]) if (mixed and 0 in arms) else None
+    for r in arms.values():
+        r.pop("state", None)
+        r.pop("Z", None)
+    gc.collect()
+    medium = None
+    if world == 1 and a.workload != "medium" and not a.no_medium:
+        medium = medium_line(a, dev)
+    err_long = None
+    if world == 1 and a.error_steps > 0:
+        err_long = error_run(a, dev, a.error_steps)
     serving = None
     if world == 1 and a.serve_requests > 0:
         serving = run_serving(a, dev)
@@ -498,10 +600,12 @@ def main():
         ensemble = run_ensemble(a, dev)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a, head["p"], head["y"], head["st"])
+        nth = os.cpu_count() or 1
+        val, per, desc = cpu_sample(a, w, w["cpu_stride"], nth, 0, 1)
+        cpu = {"value": val, "unit": "Mpts*RK3-steps/s", "cores": nth, "kind": "port", "sample": desc}
     if rank == 0:
         p = head["p"]
-        mixed = 1 in arms
+        form = MIXED_NAMES[a.mixed_form] if mixed else "FP64 plain path"
         line = {
             "metric": "Mpts*RK3-steps/s", "value": head["value"], "unit": "Mpts*RK3-steps/s",
             "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["ms"] / a.steps,
@@ -509,18 +613,16 @@ def main():
             "dtype": "mixed f32/f64" if mixed else "f64",
             "precision_form": a.mixed_form if mixed else 0,
             "data": "synthetic (seeded initial condition)",
-            "config": {"workload": f"lomacte {MIXED_NAMES[a.mixed_form] if mixed else 'FP64 plain path'}"
-                                   f"{extensions(a)} "
-                                   f"{a.nx}x{a.ny}x{a.nz} (mgal {p.mgalx}x{p.mgalz}), s=4, Re=160, dt=0.01",
-                       "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (~%.1f GB touched per step)" % (head["step_bytes"] / 1e9)},
+            "config": dict(config(a, w, form), parallelism=f"replicas{world}",
+                           l2="inputs larger than L2 (~%.0f GB touched per step)" % (head["step_bytes"] / 1e9),
+                           mgal=f"{p.mgalx}x{p.mgalz}"),
             "gpu_launches": head["launches_per_step"] * a.steps,
             "y_kernels": head["y_family"],
             "clocks": head["clocks"], "roofline": head["roofline"], "kernel_share": head["kernel_share"],
             "stage_share": head["stage_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving, "stats_step": head["stats_step"],
-            "ensemble": ensemble,
+            "ensemble": ensemble, "medium_grid": medium, "error_long": err_long,
         }
         if mixed and 0 in arms:
             f64 = arms[0]
@@ -530,7 +632,8 @@ def main():
                             "stats_step": f64["stats_step"]}
             line["mixed_over_fp64"] = head["value"] / f64["value"]
             line["error_vs_fp64"] = {"rel_l2": errs, "steps": a.warmup + a.steps,
-                                     "note": "mixed vs FP64 GPU path from the same seeded state"}
+                                     "note": "mixed vs FP64 GPU path from the same seeded state (e2e steps "
+                                             "restart from it)"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

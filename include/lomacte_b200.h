@@ -67,8 +67,8 @@ typedef struct lmc_params {
                            extension after branches/loma/src/cross.f:
                            1591-1596, 2177-2196); 0: the constant viscosity
                            of lomacte3.  Not with variant 1; the x stage
-                           then needs mgalx <= 768 (1152 without the
-                           scalar) for its shared memory */
+                           then needs mgalx <= 1152 with the scalar for
+                           its shared memory */
   double sigma;         /* exponent sigma in [0, 4] (0.7 for air;
                            branches/loma reads it as hre.dat's fourth
                            value, main.f:543) */

@@ -124,9 +124,10 @@ int pick_chunks(int my, int &C, int &lpm, int &base, int &extra) {
   return LMC_OK;
 }
 
-// The x stage holds a tile's input rows and transform lines in shared
-// memory; with the passive scalar and the variable viscosity the largest
-// lengths need more than the 227 KB a B200 block can have.
+// The x stage holds a tile's transform lines (and, where they fit, its
+// staged input rows) in shared memory; with the passive scalar and the
+// variable viscosity the lines of the largest lengths alone need more than
+// the 227 KB a B200 block can have.
 constexpr size_t SMEM_BLOCK_MAX = 227 * 1024;
 bool xstage_fits(const lmc::Grid &g, int scalar, int visc) {
   lmc::Dev d;
@@ -263,6 +264,10 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     const char *e = std::getenv("LMC_FFT64");
     d.fft64 = e ? (std::atoi(e) & 7) : 0;
   }
+  {  // LMC_XSTG=0: the x stage reads its input rows from global memory
+    const char *e = std::getenv("LMC_XSTG");
+    d.xstg = (e && std::strcmp(e, "0") == 0) ? 0 : 1;
+  }
   const lmc::Grid &g = h->g;
   int rc = LMC_OK;
   // x lengths from 24 up; z also 3 (mz = 1: a 2-D run, one kz mode)
@@ -283,7 +288,11 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   for (int k = 0; k < g.mz; k++) kz[k] = p->bet * ((k <= g.nz1) ? k : k - g.mz);  // main.f:769-778
   lmc::build_poisson(g, h->ops, kx.data(), kz.data(), h->pt);
 
-  if (cudaSetDevice(p->device) != cudaSuccess) { delete h; return LMC_ECUDA; }
+  if (cudaSetDevice(p->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&d.smem_limit, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device) != cudaSuccess) {
+    delete h;
+    return LMC_ECUDA;
+  }
   if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
@@ -414,7 +423,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   }
   if (d.prec) {
     // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
-    d.mpart_ld = 4 * g.mgalz;
+    d.mpart_ld = 8 * g.mgalz;  // one slot per (z tile, warp), at most eight warps per tile
     if ((d.visc && (rc = dalloc(h, &d.vscr, (size_t)3 * g.my))) || (rc = dalloc(h, &d.mi, (size_t)lmc::NMI * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &h->mo[1], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &d.mpart, (size_t)12 * g.my * d.mpart_ld))) {
@@ -948,7 +957,7 @@ size_t lmc_footprint(const lmc_params *p) {
     b += (size_t)g.nmode * ((size_t)C * 32 * (2 + 3 + 2) + 5) * 8 + (size_t)g.my * 15 * 8;  // Poisson, d/dy rows
   if (p->scalar) {  // Z, RHS(Z), one more spectral and z-physical work buffer
     b += S * 16 + P * 8 + (p->precision == 0 ? S * 16 + Z * 16 : S * 8 + Z * 8);
-    b += 2 * (size_t)g.my * 8 + (size_t)g.my * 8 * 4 * g.mgalz;  // mixed sums of the 12th output
+    b += 2 * (size_t)g.my * 8;  // mixed sums of the 12th output
   }
   if (p->visc) {  // spectral buffers up to 15, z-physical ones up to 14 (18 with the scalar)
     const size_t have = p->scalar ? 12 : 11, xs = 15 - have, xz = (p->scalar ? 18 : 14) - have;
@@ -956,7 +965,7 @@ size_t lmc_footprint(const lmc_params *p) {
     b += xs * S * e + xz * Z * e + 3 * (size_t)g.my * (8 + 16);  // + mixed 00 profiles and their scratch
   }
   if (p->precision == 0) b += 11 * S * 16 + 11 * Z * 16;          // FP64 work buffers
-  else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 44 * (size_t)g.my * g.mgalz * 8;
+  else b += 3 * S * 16 + 11 * S * 8 + 11 * Z * 8 + 28 * (size_t)g.my * 8 + 96 * (size_t)g.my * g.mgalz * 8;
   b += (size_t)C * 32 * 64 * 8 + 6 * 5 * 32 * 16 * 8 + (size_t)(g.mgalx + g.mgalz) * 24;  // y tables, twiddles
   b += 64 * 16 * 64;                                              // allocation padding and scalars
   return b;

@@ -50,11 +50,15 @@ struct Geo {
 // Threads of an x-stage block.  With the passive scalar or the variable
 // viscosity the x stage stages 12 to 18 inputs and transforms 6 to 9 lines
 // per z line, so shared memory admits fewer blocks per SM: those blocks
-// get twice the threads (at most four warps, the partial-sum slots of the
-// mixed form).
+// get twice the threads (four warps), and eight warps for lines of 1152
+// points and more (N1 >= 32), of which only one or two blocks fit an SM.
+// XW_MAX warps at most: the partial-sum slots of the mixed form.
+constexpr int XW_MAX = 8;
 template <int N1, int N2, bool WIDE>
 struct XGeo {
-  static constexpr int XT = WIDE ? (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128) : Geo<N1, N2>::XT;
+  static constexpr int XT = !WIDE ? Geo<N1, N2>::XT
+                            : N1 >= 32 ? 256
+                                       : (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128);
   static constexpr int PT = (Geo<N1, N2>::ZB * Geo<N1, N2>::N + XT - 1) / XT;
 };
 
@@ -265,7 +269,11 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 // Persistent: each block walks tiles (y, z block of ZB lines).  The next
 // tile's eight input rows (each ZB*nkx contiguous complex values in the
 // [y][z][kx] layout) and its RHS(T) row arrive by TMA bulk copies while the
-// current tile is transformed.  ZS: the passive scalar's four more input
+// current tile is transformed.  stg = 0 (lengths whose staged rows do not
+// fit in shared memory beside the transform lines): only the RHS rows are
+// staged and the first transform pass reads the input rows from global
+// memory; every row of a tile is read in that pass, before any output row
+// of the tile is written (in place, after the direct transforms).  ZS: the passive scalar's four more input
 // rows (lap Z, dZ/dx, dZ/dy, dZ/dz), its RHS(Z) row and Delta Z as a
 // twelfth output, packed beside Delta T.  VS: the variable viscosity's six
 // more input rows (vbase), with T^sigma in the diffusion of T and Z and
@@ -273,19 +281,22 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 template <int N1, int N2, typename CT, typename ST, bool ZS, bool VS>
 // FP32 butterflies: at most about 128 registers, so that eight 64-thread
 // blocks (or the same thread count in larger blocks) share an SM
-__global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, ZS || VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles) {
+__global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, ZS || VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles, int stg) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
   constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, ZS || VS>::PT, XT = XGeo<N1, N2, ZS || VS>::XT;
   constexpr int VB = ZS ? 12 : 8;  // first viscosity input
   constexpr int NI = VB + (VS ? 6 : 0), NL = NI / 2, NO = ZS ? 12 : 11, NM = VS ? NMI : ZS ? 8 : 6;
-  static_assert(XT / 32 <= 4, "partial-sum slots assume at most 4 warps per x tile");
+  static_assert(XT / 32 <= XW_MAX, "partial-sum slots assume at most XW_MAX warps per x tile");
+  // with six or more transform lines the eleven (twelve) outputs fit in
+  // place and go through the direct transforms in one round
+  constexpr bool ONE = NL >= 6;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nkx = d.nkx;  // a multiple of 8 for every supported length
   CT *W = (CT *)smraw;                                        // NL buffers x ZB lines x LD
-  ST *St = (ST *)(smraw + round16(sizeof(CT) * NL * ZB * LD));  // NI rows of ZB*nkx inputs
-  double *Sr = (double *)(St + NI * ZB * nkx);  // ZB*N RHS(T)
+  ST *St = (ST *)(smraw + round16(sizeof(CT) * NL * ZB * LD));  // NI rows of ZB*nkx inputs (stg)
+  double *Sr = (double *)(St + (stg ? NI * ZB * nkx : 0));  // ZB*N RHS(T)
   double *Srz = Sr + ZB * N;                    // ZB*N RHS(Z) (ZS)
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
@@ -296,9 +307,10 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
   auto issue = [&](int t) {
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
     const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = d.variant ? 0u : (uint32_t)nzb * N * sizeof(double);
-    mbar_expect_tx(&bar, NI * rb + (ZS ? 2 : 1) * hb);
+    mbar_expect_tx(&bar, (stg ? NI * rb : 0u) + (ZS ? 2 : 1) * hb);
     const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
-    for (int f = 0; f < NI; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
+    if (stg)
+      for (int f = 0; f < NI; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
     if (hb) bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
     if (ZS && hb) bulk_g2s(Srz, d.rhsz + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
   };
@@ -360,10 +372,12 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
     // p*ZB + l packs fields 2p, 2p+1 of z line l as A + iB of the complex
     // spectrum, kx = nkx .. N-nkx (the dealiased gap) are zero, and the
     // imaginary part of mode 0 is dropped (rftsingle.f:85-88)
+    const size_t gt = ((size_t)y * d.mgalz + z0) * nkx;  // the tile's rows in global memory
     auto load = [&](int b, int n) -> CT {
       const int p = b / ZB, l = b - p * ZB;
       if (l >= nzb) return cz<CT>();
-      const ST *A = St + (2 * p) * ZB * nkx + l * nkx, *B = A + ZB * nkx;
+      const ST *A = stg ? St + (2 * p) * ZB * nkx + l * nkx : wzb<ST>(d, 2 * p) + gt + l * nkx;
+      const ST *B = stg ? A + ZB * nkx : wzb<ST>(d, 2 * p + 1) + gt + l * nkx;
       if (n < nkx) {
         const CT a = ccvt<CT>(A[n]), c = ccvt<CT>(B[n]);
         return n == 0 ? cmk<CT>(a.x, c.x) : cmk<CT>(a.x - c.y, a.y + c.x);
@@ -393,13 +407,15 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
       for (int o = 0; o < NO; o++) acc[o] = 0.0;
     }
 
-    Re r0[PT], r1[PT], r2[PT], r3[ZS ? PT : 1];
+    Re r0[ONE ? 1 : PT], r1[ONE ? 1 : PT], r2[ONE ? 1 : PT], r3[ZS && !ONE ? PT : 1];
     double rs = 0.0, mv = 0.0;
 #pragma unroll
     for (int j = 0; j < PT; j++) {
       const int q = threadIdx.x + j * blockDim.x;
-      r0[j] = r1[j] = r2[j] = 0.0;
-      if constexpr (ZS) r3[j] = 0.0;
+      if constexpr (!ONE) {
+        r0[j] = r1[j] = r2[j] = 0.0;
+        if constexpr (ZS) r3[j] = 0.0;
+      }
       if (q < nzb * N) {
         const int l = q / N, pos = q - l * N;
         CT *c0 = W + (size_t)l * LD + F::sk(pos);
@@ -474,10 +490,17 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
         *c1 = from_d2<CT>(make_double2(o[OW], o[ORUU]));
         *c2 = from_d2<CT>(make_double2(o[ORVV], o[ORWW]));
         *c3 = from_d2<CT>(make_double2(o[ORUV], o[ORUW]));
-        r0[j] = (Re)o[ORVW];
-        r1[j] = (Re)o[ODRHO];
-        r2[j] = (Re)o[ODT];
-        if constexpr (ZS) r3[j] = (Re)o[ODZ];
+        if constexpr (ONE) {  // lines 4 and 5 of this point are read above
+          CT *c4 = c3 + (size_t)ZB * LD, *c5 = c4 + (size_t)ZB * LD;
+          *c4 = from_d2<CT>(make_double2(o[ORVW], o[ODRHO]));
+          if constexpr (ZS) *c5 = from_d2<CT>(make_double2(o[ODT], o[ODZ]));  // (Delta T, Delta Z)
+          else *c5 = from_d2<CT>(make_double2(o[ODT], 0.0));
+        } else {
+          r0[j] = (Re)o[ORVW];
+          r1[j] = (Re)o[ODRHO];
+          r2[j] = (Re)o[ODT];
+          if constexpr (ZS) r3[j] = (Re)o[ODZ];
+        }
         if (do_cfl) {
           mu = fmax(mu, fabs(u));
           mv = fmax(mv, fabs(v));
@@ -515,6 +538,17 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
         s_tmax[l] = 0ull;
       }
       s_vmax = 0ull;
+    }
+    if constexpr (ONE) {
+      F::template perm2nat<-1>(W, 6 * ZB, LD, wtwx<CT>(d));
+      x_extract<N1, N2, CT, ST>(d, W, 0, OU, OV, y, z0, nzb);
+      x_extract<N1, N2, CT, ST>(d, W, 1, OW, ORUU, y, z0, nzb);
+      x_extract<N1, N2, CT, ST>(d, W, 2, ORVV, ORWW, y, z0, nzb);
+      x_extract<N1, N2, CT, ST>(d, W, 3, ORUV, ORUW, y, z0, nzb);
+      x_extract<N1, N2, CT, ST>(d, W, 4, ORVW, ODRHO, y, z0, nzb);
+      if (!d.variant) x_extract<N1, N2, CT, ST>(d, W, 5, ODT, ZS ? ODZ : -1, y, z0, nzb);
+      __syncthreads();
+      continue;
     }
     F::template perm2nat<-1>(W, 4 * ZB, LD, wtwx<CT>(d));
     x_extract<N1, N2, CT, ST>(d, W, 0, OU, OV, y, z0, nzb);
@@ -781,8 +815,14 @@ struct Launch {
   }
   static constexpr int nin(bool zs, bool vs) { return (zs ? 12 : 8) + (vs ? 6 : 0); }
   static size_t xsm(bool zs, bool vs) { return round16(sizeof(CT) * (nin(zs, vs) / 2) * G::ZB * G::LD); }
-  static size_t xphys_sm(int nkx, bool zs = false, bool vs = false) {
-    return xsm(zs, vs) + (size_t)nin(zs, vs) * G::ZB * nkx * sizeof(ST) + (size_t)(zs ? 2 : 1) * G::ZB * G::N * sizeof(double);
+  // stg: with the input rows staged in shared memory
+  static size_t xphys_sm(int nkx, bool zs = false, bool vs = false, bool stg = true) {
+    return xsm(zs, vs) + (stg ? (size_t)nin(zs, vs) * G::ZB * nkx * sizeof(ST) : 0) +
+           (size_t)(zs ? 2 : 1) * G::ZB * G::N * sizeof(double);
+  }
+  // the staged form where it fits in a block's shared memory
+  static bool xphys_stg(int nkx, bool zs, bool vs, int limit) {
+    return xphys_sm(nkx, zs, vs, true) + 1024 <= (size_t)limit;
   }
   // resident blocks per SM x SMs, for the persistent kernels
   static int grid_for(const void *fn, int threads, size_t smem, int ntiles) {
@@ -825,10 +865,20 @@ struct Launch {
   template <bool ZS, bool VS>
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
-    const size_t sm = xphys_sm(d.nkx, ZS, VS);
     constexpr int XT = XGeo<N1, N2, ZS || VS>::XT;
-    const int g = grid_for((const void *)k_xphys<N1, N2, CT, ST, ZS, VS>, XT, sm, ntiles);
-    k_xphys<N1, N2, CT, ST, ZS, VS><<<g, XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles);
+    const void *fn = (const void *)k_xphys<N1, N2, CT, ST, ZS, VS>;
+    // stage the input rows (TMA, one tile ahead) where that keeps as many
+    // blocks per SM as reading them in the first transform pass would
+    bool stg = d.xstg && xphys_stg(d.nkx, ZS, VS, d.smem_limit);
+    if (stg) {
+      int a = 0, b = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, fn, XT, xphys_sm(d.nkx, ZS, VS, true));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, XT, xphys_sm(d.nkx, ZS, VS, false));
+      stg = a >= b;
+    }
+    const size_t sm = xphys_sm(d.nkx, ZS, VS, stg);
+    const int g = grid_for(fn, XT, sm, ntiles);
+    k_xphys<N1, N2, CT, ST, ZS, VS><<<g, XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles, (int)stg);
     if constexpr (sizeof(ST) == sizeof(float2)) {
       const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (XT / 32);
       k_msum<N1, N2><<<dim3(d.my, n_out(d)), 128, 0, s>>>(d, nslot);
@@ -919,7 +969,7 @@ inline cudaError_t upload_twiddles() {
   case N: LMC_FFT_FORMS_M(N1, N2, 1, zinv(d, mode, f0, nf, s)) return true;
 #define LMC_FFT_CASE_ZF(N, N1, N2) LMC_FFT_CASE_Z(N, N1, N2, zfwd)
 #define LMC_FFT_CASE_ZS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::zinv_sm(2 * (N / 3));
-#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3, zs, vs);
+#define LMC_FFT_CASE_XS(N, N1, N2) case N: return Launch<N1, N2, double2, double2>::xphys_sm(N / 3, zs, vs, false);
 #define LMC_FFT_CASE_OPT(N, N1, N2)                                                         \
   if ((e = Launch<N1, N2, double2, double2>::optin(limit)) != cudaSuccess) return e;        \
   if ((e = Launch<N1, N2, float2, float2>::optin(limit)) != cudaSuccess) return e;          \

@@ -23,6 +23,8 @@ struct Dev {
   int lpm, base, extra, C;  // y-chunking of a pencil over the lanes of a warp
   int ldy;                  // staging stride of a pencil (odd, >= my)
   int zb_x, kb_z;           // lines per block of the x / z transform kernels
+  int smem_limit;           // opt-in shared memory per block of the device (bytes)
+  int xstg;                 // 1: the x stage stages its input rows where they fit (LMC_XSTG=0: never)
   double ire, peclet, cfl, hxalp, hzbet;
   double gama[3], xi[3], alpha[3], beta[3];
   // y operators: band rows and precomputed scan tables

@@ -470,7 +470,13 @@ struct lmo {
   int *jsp;
   double sigma;
   double *st, *sp, uner[9];
+  /* timing samples (lmo_set_sample): with smp > 1 the parallel loops of a
+   * substep visit only the units (modes, kx planes of a field, physical
+   * lines) whose index is smph modulo smp, i.e. 1/smp of the work */
+  int smp, smph;
 };
+
+static inline int skip_unit(const lmo *o, long u) { return o->smp > 1 && (int)(u % o->smp) != o->smph; }
 
 #define SIDX(o, i, k, j) (((size_t)(i) * (o)->mz + (k)) * (o)->my + (j))
 
@@ -864,6 +870,7 @@ static void phys2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
     cplx *spec = malloc(sizeof(cplx) * nkx * 12);
 #pragma omp for schedule(static)
     for (long L = 0; L < (long)nlines; L++) {
+      if (skip_unit(o, L)) continue;
       int jj = (int)(L / mgalz); /* y index (cross.f:1583) */
       const int vb = o->scalar ? 12 : 8, nin = vb + (o->vs ? 6 : 0), nout = o->scalar ? 12 : 11;
       cplx *sp[18];
@@ -987,7 +994,8 @@ static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
     cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
 #pragma omp for collapse(2) schedule(static)
     for (int f = 0; f < nin; f++)
-      for (int i = 0; i < nkx; i++) zinv_plane(o, i, in8[f], o->ln[f], buf, out);
+      for (int i = 0; i < nkx; i++)
+        if (!skip_unit(o, (long)f * nkx + i)) zinv_plane(o, i, in8[f], o->ln[f], buf, out);
     free(buf); free(out);
   }
   double cfl[4];
@@ -998,7 +1006,8 @@ static void foup2(lmo *o, int rk, double dtxi, double dtgamma, double dtbeta, in
     cplx *buf = malloc(sizeof(cplx) * mgalz), *out = malloc(sizeof(cplx) * mgalz);
 #pragma omp for collapse(2) schedule(static)
     for (int f = 0; f < nout; f++)
-      for (int i = 0; i < nkx; i++) zfwd_plane(o, i, o->ln[f], out11[f], buf, out);
+      for (int i = 0; i < nkx; i++)
+        if (!skip_unit(o, (long)f * nkx + i)) zfwd_plane(o, i, o->ln[f], out11[f], buf, out);
     free(buf); free(out);
   }
   if (do_diag) {
@@ -1158,6 +1167,7 @@ static void strain_inputs(lmo *o, const cplx *ru, const cplx *rv, const cplx *rw
     double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my;
 #pragma omp for schedule(static)
     for (int m = 0; m < o->nmode; m++) {
+      if (skip_unit(o, m)) continue;
       double kx = o->kxv[m / mz], kz = o->kzv[m % mz];
       size_t b = (size_t)m * my;
       deryr2_c(o, ru + b, dy, w1, w2, tt1, tt2);
@@ -1211,6 +1221,7 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
 #pragma omp for schedule(static)
     for (int m = 0; m < o->nmode; m++) {
+      if (skip_unit(o, m)) continue;
       int i = m / mz, k = m % mz;
       double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
       size_t b = (size_t)m * my;
@@ -1294,6 +1305,7 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my;
 #pragma omp for schedule(static)
     for (int m = 0; m < o->nmode; m++) {
+      if (skip_unit(o, m)) continue;
       int i = m / mz, k = m % mz;
       double kx = o->kxv[i], kz = o->kzv[k];
       size_t b = (size_t)m * my;
@@ -1307,6 +1319,7 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     }
 #pragma omp for schedule(static)
     for (int m = 0; m < o->nmode; m++) {
+      if (skip_unit(o, m)) continue;
       int i = m / mz, k = m % mz;
       double kx = o->kxv[i], kz = o->kzv[k];
       size_t b = (size_t)m * my;
@@ -1350,6 +1363,7 @@ static void substep(lmo *o, int r /*0..2*/, int ihist) {
     double *w1 = s, *w2 = s + my, *tt1 = s + 2 * my, *tt2 = s + 3 * my, *sc = s + 4 * my;
 #pragma omp for schedule(static)
     for (int m = 0; m < o->nmode; m++) {
+      if (skip_unit(o, m)) continue;
       int i = m / mz, k = m % mz;
       double kx = o->kxv[i], kz = o->kzv[k], rK = kx * kx + kz * kz;
       size_t b = (size_t)m * my;
@@ -1959,6 +1973,16 @@ int lmo_stats_read(lmo *o, double *prof, double *spec, double *uner, int *counts
     memset(o->sp, 0, sizeof(double) * nsp);
     o->nacumsp = 0;
   }
+  return 0;
+}
+
+/* Timing samples: from now on the parallel loops of a substep visit only
+ * the units whose index is phase modulo stride (stride <= 1: all of them).
+ * The state is then no longer a solution; for timing only. */
+int lmo_set_sample(lmo *o, int stride, int phase) {
+  if (stride < 1 || phase < 0 || (stride > 1 && phase >= stride)) return -1;
+  o->smp = stride;
+  o->smph = phase;
   return 0;
 }
 

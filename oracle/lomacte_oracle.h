@@ -54,6 +54,11 @@ int lmo_set_variant(lmo *o, int variant);
 
 /* One substep with RK coefficient r on the current state (timing samples). */
 int lmo_substep(lmo *o, int r);
+/* Timing samples: the parallel loops of later substeps visit only the
+ * units (modes, kx planes of a field, physical lines) whose index is phase
+ * modulo stride, i.e. 1/stride of a substep's work; stride 1 restores the
+ * full substep.  The state is then no longer a solution (timing only). */
+int lmo_set_sample(lmo *o, int stride, int phase);
 
 /* Diagnostics of the last step, in this order:
  * 0 time (before the step), 1 Deltat used, 2 dm, 3 dw, 4 Re*dw, 5 trapz,

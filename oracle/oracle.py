@@ -54,6 +54,7 @@ def lib():
         L.lmo_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.lmo_set_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.lmo_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.lmo_set_sample.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.lmo_get_diag.argtypes = [ctypes.c_void_p, _dp]
         L.lmo_get_coefs.argtypes = [ctypes.c_void_p] + [_dp] * 7
         for n in ("lmo_deryr", "lmo_deryyr", "lmo_inty8"):
@@ -138,6 +139,11 @@ class Oracle:
 
     def substep(self, r=0):
         lib().lmo_substep(self.h, r)
+
+    def set_sample(self, stride, phase=0):
+        """Later substeps do 1/stride of their work (timing samples only)."""
+        if lib().lmo_set_sample(self.h, int(stride), int(phase)) != 0:
+            raise ValueError("lmo_set_sample rejected its arguments")
 
     # passive scalar Z, advanced as T (lomacte_oracle.h)
     def set_scalar(self, z, schmidt):

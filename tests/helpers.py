@@ -29,3 +29,11 @@ def rel_l2(a, b):
     den = np.linalg.norm(b.ravel())
     num = np.linalg.norm((a - b).ravel())
     return num / den if den > 0 else num
+
+
+def mixing_scalar(p, y):
+    """The passive scalar of the mixing-layer workloads: Z = 0.5 (1 +
+    tanh(y/2)) in the kx = kz = 0 mode, no fluctuation."""
+    z = np.zeros(p.shape, dtype=np.complex128)
+    z[0, 0, :] = 0.5 * (1.0 + np.tanh(np.asarray(y) / 2.0))
+    return z

@@ -29,10 +29,24 @@ def test_xstage_bytes_by_hand():
 
 
 def test_reference_arm_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--nx", "24", "--nz", "24", "--ny", "33",
-                        "--steps", "3", "--warmup", "3"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    """The reference arm: RK3-step accounting of its bounded samples, the
+    JSON contract, and no product library in its process."""
+    code = ("import runpy, sys, io, contextlib; sys.argv = ['bench.py', '--impl', 'reference', '--workload', "
+            "'medium', '--ny', '33', '--steps', '3', '--warmup', '1']; buf = io.StringIO()\n"
+            "with contextlib.redirect_stdout(buf): runpy.run_path('bench.py', run_name='__main__')\n"
+            "print(buf.getvalue().strip().splitlines()[-1])\n"
+            "print(sorted(set(l.split()[-1] for l in open('/proc/self/maps') if 'lomacte' in l)))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
-    d = json.loads(r.stdout.strip().splitlines()[-1])
+    out = r.stdout.strip().splitlines()
+    d = json.loads(out[-2])
     assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["e2e"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
     assert "passive scalar" in d["config"]["workload"] and "T^0.7" in d["config"]["workload"]
+    # each step is one sample of 1/16 of a substep of the 256^2 x 33 slab, i.e. 1/48 RK3 step
+    w = bench.WORKLOADS["medium"]
+    rk3 = 256 * 256 * 33 / 1e6 / (3 * w["ref_stride"])
+    assert abs(d["value"] - rk3 / (d["ms_per_step"] / 1e3)) < 1e-9 * d["value"]
+    assert d["steps"] == 3 and d["warmup"] == 1
+    libs = eval(out[-1])
+    assert libs and all("oracle" in x for x in libs), libs

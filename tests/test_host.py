@@ -118,13 +118,13 @@ def test_footprint_counts_the_viscosity_buffers():
 
 
 def test_viscosity_x_grid_limit():
-    # the x stage's shared memory: mgalx 768 with the scalar, 1152 without
-    ok = Params.from_modes(512, 1, 65, visc=1, sigma=0.7, scalar=1)
-    big = Params.from_modes(768, 1, 65, visc=1, sigma=0.7, scalar=1)
-    big_ns = Params.from_modes(768, 1, 65, visc=1, sigma=0.7)
+    # the x stage's shared memory: mgalx 1152 with the scalar, 1536 without
+    ok = Params.from_modes(768, 1, 65, visc=1, sigma=0.7, scalar=1)
+    big = Params.from_modes(1024, 1, 65, visc=1, sigma=0.7, scalar=1)
+    big_ns = Params.from_modes(1024, 1, 65, visc=1, sigma=0.7)
     assert lm.footprint(ok) > 0 and lm.footprint(big_ns) > 0
     assert lm.footprint(big) == 0
-    assert lm.footprint(Params.from_modes(768, 1, 65, scalar=1)) > 0
+    assert lm.footprint(Params.from_modes(1024, 1, 65, scalar=1)) > 0
 
 
 @pytest.mark.parametrize("lang,cc", [("c", "gcc"), ("c++", "g++")])
@@ -136,3 +136,19 @@ def test_header_compiles_alone(lang, cc, tmp_path):
     r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-x", lang,
                         os.path.join(ROOT, "include", "lomacte_b200.h")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("grid,s,seed", [((32, 32, 65), 4.0, 0), ((64, 64, 129), 8.0, 1), ((48, 1, 65), 4.0, 2)])
+def test_oracle_side_ic_matches_the_library(grid, s, seed):
+    """The CPU arms of bench.py build the initial condition with the oracle's
+    own restatement (oracle/ic.py) so that they never load the library; it
+    is the library's lmc_make_ic up to the round-off of the two y-operator
+    builds."""
+    from oracle.ic import make_ic as oracle_ic
+    p, y, a = case(*grid, s=s, seed=seed)
+    b = oracle_ic(p.mgalx, p.mgalz, y, alp=p.alp, bet=p.bet, s=s, seed=seed)
+    for k in ("vor", "phi", "psi", "scal", "u00"):
+        den = np.linalg.norm(a[k])
+        assert np.linalg.norm(a[k] - b[k]) <= 1e-12 * den, k
+    for k in ("v00", "w00"):
+        assert not np.any(b[k])
