@@ -30,7 +30,8 @@ enum {
   LMC_OK = 0,
   LMC_EINVAL = -1,   /* bad argument or grid */
   LMC_ENOMEM = -2,   /* device allocation failed */
-  LMC_ENAN = -3,     /* non-finite value detected in the state */
+  LMC_ENAN = -3,     /* non-finite value in the step's diagnostics (the
+                        run blew up); lmc_get_diag / lmc_status report it */
   LMC_ETIMEOUT = -4, /* a bounded device wait gave up */
   LMC_ECUDA = -5,    /* CUDA runtime error */
   LMC_ENODEV = -6    /* no CUDA device (the library has no CPU path) */
@@ -169,8 +170,17 @@ int lmc_step(lmc_handle *h, int nsteps);
 int lmc_sync(lmc_handle *h);
 /* Diagnostics of the last completed step (synchronises). */
 int lmc_get_diag(lmc_handle *h, lmc_diag *d);
-/* Device status word (0 ok, else an LMC_E* code); synchronises. */
+/* Device status word (0 ok, else an LMC_E* code); synchronises.  A bounded
+ * device wait that gave up reads LMC_ETIMEOUT; non-finite diagnostics read
+ * LMC_ENAN. */
 int lmc_status(lmc_handle *h);
+/* Failure-path check: runs on the handle's stream one bounded mbarrier wait
+ * that nothing completes, with at most `polls` polls (1 .. 2^24, the limit
+ * of the transform kernels' waits), as when a kernel's bulk copy never
+ * lands; afterwards lmc_status reads LMC_ETIMEOUT (the handle's status word
+ * stays set: use a handle made for the check).  No counterpart in the
+ * reference, which has no device waits. */
+int lmc_wait_selftest(lmc_handle *h, unsigned polls);
 const char *lmc_strerror(int code);
 
 /* The handle's CUDA stream (cudaStream_t as void*) and device pointers of

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "lmc_internal.h"
+#include "lmc_async.cuh"
 #include "lmc_kernels.cuh"
 
 struct lmc_handle {
@@ -231,7 +232,7 @@ const char *lmc_strerror(int code) {
     case LMC_OK: return "ok";
     case LMC_EINVAL: return "invalid argument or grid";
     case LMC_ENOMEM: return "device out of memory";
-    case LMC_ENAN: return "non-finite value in the state";
+    case LMC_ENAN: return "non-finite value in the step's diagnostics";
     case LMC_ETIMEOUT: return "device wait timed out";
     case LMC_ECUDA: return "CUDA runtime error";
     case LMC_ENODEV: return "no CUDA device";
@@ -991,7 +992,35 @@ int lmc_get_diag(lmc_handle *h, lmc_diag *out) {
   out->H00u = dg[10]; out->H00w = dg[11]; out->Deltat_next = dg[12];
   out->step = h->steps;
   out->status = st;
-  return h->err;
+  if (h->err) return h->err;
+  for (int i = 0; i < 13; i++)  // a run that went non-finite
+    if (!std::isfinite(dg[i])) {
+      if (!st) out->status = LMC_ENAN;
+      return LMC_ENAN;
+    }
+  return LMC_OK;
+}
+
+namespace {
+// one bounded wait on an mbarrier that nothing completes: the path every
+// transform kernel's wait takes when its bulk copy never lands
+__global__ void k_wait_selftest(int *status, unsigned polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    lmcd::mbar_init(&bar, 1);
+    lmcd::mbar_wait(&bar, 0, status, polls);
+    lmcd::mbar_inval(&bar);
+  }
+}
+}  // namespace
+
+int lmc_wait_selftest(lmc_handle *h, unsigned polls) {
+  if (!h || polls < 1 || polls > lmcd::LMC_WAIT_LIMIT) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  k_wait_selftest<<<1, 32, 0, h->s>>>(h->d.status, polls);
+  LMC_CK(cudaGetLastError());
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return LMC_OK;
 }
 
 int lmc_status(lmc_handle *h) {

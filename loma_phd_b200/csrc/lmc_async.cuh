@@ -36,9 +36,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait on phase `parity`; false on time-out (status word set)
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status) {
-  for (uint32_t it = 0; it < LMC_WAIT_LIMIT; it++)
+// bounded wait on phase `parity` (at most `limit` polls); false on
+// time-out (status word set)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status,
+                                          uint32_t limit = LMC_WAIT_LIMIT) {
+  for (uint32_t it = 0; it < limit; it++)
     if (mbar_try_wait(bar, parity)) return true;
   atomicExch(status, -4 /* LMC_ETIMEOUT */);
   return false;

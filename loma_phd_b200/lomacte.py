@@ -30,7 +30,7 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
+    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_wait_selftest", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
     "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read", "lmc_load_scalar_f64", "lmc_get_scalar_f64",
     "lmc_physical_f64",
@@ -107,6 +107,7 @@ def _lib():
         L.lmc_profile_start.argtypes = [vp]
         L.lmc_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
+        L.lmc_wait_selftest.argtypes = [vp, ctypes.c_uint]
         L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         L.lmc_use_graphs.argtypes = [vp, ctypes.c_int]
         L.lmc_launches_per_step.argtypes = [vp]
@@ -376,6 +377,15 @@ class Lomacte:
                "lmc_stats_read")
         return StatsData(prof=prof, spec=spec, uner=uner, nacum=int(cnt[0]), nacumsp=int(cnt[1]),
                          planes=list(planes), sigma=self._stats_sigma)
+
+    def wait_selftest(self, polls: int = 1000):
+        """One bounded device wait that nothing completes (lmc_wait_selftest);
+        lmc_status reads LMC_ETIMEOUT afterwards."""
+        _check(_lib().lmc_wait_selftest(self._h, int(polls)), "lmc_wait_selftest")
+
+    def status(self) -> int:
+        """The device status word (lmc_status): 0 or an LMC_E* code."""
+        return int(_lib().lmc_status(self._h))
 
     def diag(self) -> dict:
         d = lmc_diag()

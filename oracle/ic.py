@@ -41,12 +41,13 @@ def urand(seed: int, a: int, b: int, c: int, d: int) -> float:
 
 
 def make_ic(mgalx, mgalz, y, alp=0.25, bet=0.25, s=4.0, u0=-0.5, dm0=1.0, amp=1e-2, swin=2.0,
-            nkmax=8, nymax=4, seed=0):
+            nkmax=8, nymax=4, seed=0, momentum=False):
     """State dict (vor, phi, psi, scal [nkx, mz, my] complex, u00, v00, w00)
     of the seeded mixing layer: rho00 = 1 + (s-1)/(s+1) tanh(-y/(2 dm0)),
     T00 = 1/rho00, rho u00 = rho00 u0 tanh(y/(2 dm0)); solenoidal noise on
     1 <= |k| <= nkmax (mode-index units) windowed by exp(-(y/swin)^2),
-    scaled to rms amp at the mid plane."""
+    scaled to rms amp at the mid plane.  momentum: also return the spectral
+    rho u, rho v, rho w the state was built from (keys ru, rv, rw)."""
     y = np.ascontiguousarray(y, dtype=np.float64)
     my = len(y)
     nkx = (2 * (mgalx // 3)) // 2
@@ -109,11 +110,14 @@ def make_ic(mgalx, mgalz, y, alp=0.25, bet=0.25, s=4.0, u0=-0.5, dm0=1.0, amp=1e
     # 5) psi, Omega_y, phi (initloma3/src/main.f:473-561); zero outside the band
     shp = (nkx, mz, my)
     vor, phi, psi, scal = (np.zeros(shp, dtype=np.complex128) for _ in range(4))
+    mom = [np.zeros(shp, dtype=np.complex128) for _ in range(3)] if momentum else None
     for b, m in enumerate(band):
         i, k = m // mz, m % mz
         ikx, ikz = 1j * kxv[i], 1j * kzv[k]
         k2 = kxv[i] ** 2 + kzv[k] ** 2
         ru, rv, rw = (rho00 * fac * cur[b, c] for c in range(3))
+        if momentum:
+            mom[0][i, k], mom[1][i, k], mom[2][i, k] = ru, rv, rw
         div = ikx * ru + ikz * rw + d1(rv)
         ps = o.lapvdvhom(div, k2)[0] if k2 != 0.0 else np.zeros(my, dtype=np.complex128)
         myv = rv - d1(ps)
@@ -122,4 +126,7 @@ def make_ic(mgalx, mgalz, y, alp=0.25, bet=0.25, s=4.0, u0=-0.5, dm0=1.0, amp=1e
         phi[i, k] = -k2 * myv + d2(myv)
     scal[0, 0] = 1.0 / rho00
     u00 = rho00 * u0 * np.tanh(y / (2.0 * dm0))
-    return dict(vor=vor, phi=phi, psi=psi, scal=scal, u00=u00, v00=np.zeros(my), w00=np.zeros(my), time=0.0)
+    out = dict(vor=vor, phi=phi, psi=psi, scal=scal, u00=u00, v00=np.zeros(my), w00=np.zeros(my), time=0.0)
+    if momentum:
+        out.update(ru=mom[0], rv=mom[1], rw=mom[2])
+    return out

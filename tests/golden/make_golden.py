@@ -1,5 +1,8 @@
-"""Regenerate tests/golden/fft_rect_double.npz from the reference's own FFT
-golden vectors.
+"""Regenerate the fixtures of tests/golden/ from the reference's own files:
+fft_rect_double.npz from its FFT golden vectors, and hre_lomacte3.dat /
+hre_lomacte.dat, verbatim copies of the run-parameter files of the two
+lomacte codes (trunk/lomacte3/hre.dat, trunk/lomacte/hre.dat) that
+tests/test_files.py parses as initcr does.
 
 Source (read as text; nothing of the reference is executed):
   Beovulfo/LoMa_phD branches/reactml/benchmark_fft/cfttest_double.txt
@@ -16,7 +19,7 @@ rffttest: pairs (physx(i), four(i)), i=1..768: four(1..768) is the packed
   physx(1) is overwritten by the transform's Nyquist slot (rft writes
   element n+1 past the 768-long array), so only four(:) is kept.
 
-Usage: python tests/golden/make_golden.py [reference_root]
+Usage: python tests/golden/make_golden.py <reference_root>
 """
 import os
 import sys
@@ -37,7 +40,9 @@ def parse_e14(path):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference_root>  (the Beovulfo/LoMa_phD checkout)")
+    root = sys.argv[1]
     d = os.path.join(root, "branches", "reactml", "benchmark_fft")
     c = parse_e14(os.path.join(d, "cfttest_double.txt")).reshape(-1, 3)
     r = parse_e14(os.path.join(d, "rffttest_double.txt")).reshape(-1, 2)
@@ -45,6 +50,13 @@ def main():
     np.savez(out, cft_phys=c[:, 0], cft_re=c[:, 1], cft_im=c[:, 2],
              rft_physx=r[:, 0], rft_four=r[:, 1])
     print("wrote", out, c.shape, r.shape)
+    here = os.path.dirname(os.path.abspath(__file__))
+    for code in ("lomacte3", "lomacte"):
+        src = os.path.join(root, "trunk", code, "hre.dat")
+        dst = os.path.join(here, f"hre_{code}.dat")
+        with open(src, "rb") as f, open(dst, "wb") as g:
+            g.write(f.read())
+        print("wrote", dst)
 
 
 if __name__ == "__main__":

@@ -1,6 +1,7 @@
 """The reference's file formats: restart images (escru.f:121-139 /
 main.f:361-406), hre.dat (main.f:502-545), the .cf line (cross.f:1172-1176)
 and the y-metrics written into the restart header."""
+import os
 import struct
 
 import numpy as np
@@ -9,6 +10,8 @@ import pytest
 from loma_phd_b200 import Lomacte, y_metrics
 from loma_phd_b200.files import cf_line, fortran_d, read_hre, read_restart, write_restart
 from tests.helpers import FIELDS, case, oracle_for, rel_l2
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def _f32(st):
@@ -102,6 +105,27 @@ def test_hre_dat(tmp_path):
     assert (h.nstep, h.nimag, h.nhist, h.cfl, h.ncfl) == (100, 50, 10, 0.5, 10)
     assert (h.id22, h.nstart, h.ntimes) == (3, 1, 5)
     assert (h.filout, h.filinp, h.filstt) == ("runs/out/mix", "runs/in/mix.002", "runs/stats/mix_01")
+
+
+@pytest.mark.parametrize("code,want", [
+    ("lomacte3", dict(Re=160.0, alp=0.0136295, bet=0.036319, a0=0.0, nstep=15001, nimag=1000, nhist=200, cfl=0.5,
+                      ncfl=10, id22=6, nstart=1, ntimes=1, filout="/share/drive/toni/VDML/s20/01c/s20a",
+                      filinp="/share/drive/toni/VDML/s20/01/s20a.005",
+                      filstt="/share/drive/toni/VDML/s20/01c/s20a_02")),
+    ("lomacte", dict(Re=160.0, alp=0.0182, bet=0.0731, a0=0.0, nstep=21, nimag=10, nhist=5, cfl=0.5, ncfl=10,
+                     id22=1, nstart=1, ntimes=5, filout="/data2/toni/turb/3Dinc",
+                     filinp="/home/toni/SVNlast/branches/initloma/data/finpinc.dat",
+                     filstt="/data2/toni/turb/3Dinc_01")),
+])
+def test_reference_hre_dat(code, want):
+    """The reference's own run-parameter files (trunk/lomacte3/hre.dat,
+    trunk/lomacte/hre.dat, copied by tests/golden/make_golden.py), parsed as
+    initcr does (main.f:502-545): 'CC' lines skipped, list-directed reads of
+    the four parameter records, the first blank-free word of the three a70
+    file-name records."""
+    h = read_hre(os.path.join(GOLDEN, f"hre_{code}.dat"))
+    for k, v in want.items():
+        assert getattr(h, k) == v, (k, getattr(h, k), v)
 
 
 def test_fortran_d_edit():

@@ -72,3 +72,55 @@ def test_solvepsi_neumann(o):
         assert abs(dv[0]) < 1e-12 and abs(dv[-1]) < 1e-12
         r = o.deryyr(v.real) - k2 * v.real - phi.real
         assert np.abs(r[4:-4]).max() < 1e-4 * np.abs(phi).max()
+
+
+def _band(B, v, h):
+    """Rows of a band matrix (entry c of row j at column j - h + c) times v."""
+    n = len(v)
+    out = np.zeros(n, dtype=np.result_type(B, v))
+    for c in range(2 * h + 1):
+        lo, hi = max(0, h - c), min(n, n + h - c)
+        out[lo:hi] += B[lo:hi, c] * v[lo - h + c:hi - h + c]
+    return out
+
+
+def test_initloma3_divergence_residual():
+    """initloma3's check of the decomposition it writes
+    (trunk/initloma3/src/main.f:473-523): the divergence of the seeded
+    momentum, div = i kx rho u + d(rho v)/dy + i kz rho w, is the source of
+    the Dirichlet Poisson problem whose solution is the state's psi
+    (Lapvdvhom).  Known answer: zero residual of the compact-scheme system
+    (dt22 - k^2 dt21) psi = dt21 div on the interior rows, psi = 0 at the
+    walls; solvepsi on the same source has the same interior residual and a
+    zero dpsi/dy at both walls (laps.f:580-764)."""
+    from oracle.ic import make_ic
+    y = stretched_mesh(97)
+    o = Oracle(48, 48, y, 160.0, 0.25, 0.25, nthreads=1)
+    st = make_ic(48, 48, y, s=4.0, seed=5, momentum=True)
+    c = o.coefs()
+    nkx, mz, my = st["psi"].shape
+    kx = 0.25 * np.arange(nkx)
+    kz = 0.25 * np.array([k if k <= (mz - 1) // 2 else k - mz for k in range(mz)])
+    worst = [0.0, 0.0, 0.0]
+    checked = 0
+    for i in range(nkx):
+        for k in range(mz):
+            k2 = kx[i] ** 2 + kz[k] ** 2
+            rv = st["rv"][i, k]
+            if k2 == 0.0 or not np.any(rv):
+                continue
+            dv = o.deryr(rv.real) + 1j * o.deryr(rv.imag)
+            div = 1j * kx[i] * st["ru"][i, k] + dv + 1j * kz[k] * st["rw"][i, k]
+            psi = st["psi"][i, k]
+            lhs = _band(c["dt22"], psi, 2) - k2 * _band(c["dt21"], psi, 2)
+            rhs = _band(c["dt21"], div, 2)
+            scale = np.abs(rhs).max()
+            worst[0] = max(worst[0], np.abs(lhs - rhs)[1:-1].max() / scale)
+            assert psi[0] == 0 and psi[-1] == 0
+            p2, dp2 = o.solvepsi(div, k2)
+            lhs2 = _band(c["dt22"], p2, 2) - k2 * _band(c["dt21"], p2, 2)
+            worst[1] = max(worst[1], np.abs(lhs2 - rhs)[1:-1].max() / scale)
+            worst[2] = max(worst[2], abs(dp2[0]) / np.abs(dp2).max(), abs(dp2[-1]) / np.abs(dp2).max())
+            checked += 1
+    assert checked > 50
+    assert worst[0] < 1e-12 and worst[1] < 1e-12 and worst[2] < 1e-12, worst
