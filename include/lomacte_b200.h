@@ -167,6 +167,20 @@ int lmc_physical_f64(lmc_handle *h, int nplanes, const int *jplanes, double *out
  * substeps of cross.f:307-1141 each).  Asynchronous on the handle's
  * stream; Deltat is computed on the device. */
 int lmc_step(lmc_handle *h, int nsteps);
+/* lmc_step with the transform stage decomposed as the reference's slab
+ * decomposition (chpl2ln / chln2pl and pointers_calc,
+ * trunk/lomacte3/src/change.f:1-211) over nblocks blocks on this device:
+ * block r's inverse and direct z transforms cover its contiguous kx planes,
+ * its x stage covers its contiguous (z, y) lines (the first n mod nblocks
+ * blocks one longer), and the plane -> line and line -> plane exchanges
+ * between the blocks' buffers are device copies -- the data path of a run
+ * whose blocks sit on several GPUs, where the copies become the all-to-all.
+ * The y work is per mode and runs over all modes at once.  Results are
+ * those of lmc_step (FP64: to round-off).  nblocks in [1, nplanes], fixed
+ * for the handle after the first call (its block buffers are kept);
+ * mgalx >= 144 (one z line per x-stage tile); not with the 2014 variant;
+ * no CUDA graphs.  LMC_EINVAL otherwise. */
+int lmc_step_split(lmc_handle *h, int nblocks, int nsteps);
 int lmc_sync(lmc_handle *h);
 /* Diagnostics of the last completed step (synchronises). */
 int lmc_get_diag(lmc_handle *h, lmc_diag *d);

@@ -44,6 +44,14 @@ struct lmc_handle {
   int st_cap = -1;
   size_t st_spec_bytes = 0;
   int nacum = 0, nacumsp = 0;
+  // slab blocks of lmc_step_split: kx planes p0 .. p0+np-1 and (z, y) lines
+  // l0 .. l0+nl-1 of block r, with z-physical buffers of its planes (Z) and
+  // of its lines (X), field by field
+  struct Split {
+    int n = 0;
+    std::vector<int> p0, np, l0, nl;
+    std::vector<std::vector<void *>> Z, X;
+  } split;
   // per-kernel CUDA-event profiling (lmc_profile_start / lmc_profile_read)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -303,6 +311,7 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
   }
   d.my = g.my; d.mgalx = g.mgalx; d.mgalz = g.mgalz; d.nkx = g.nkx; d.mz = g.mz; d.nz1 = g.nz1; d.nmode = g.nmode;
   d.ldy = g.my | 1;
+  d.zp0 = 0; d.zkn = g.nkx; d.xt0 = 0; d.xnt = 0; d.xl0 = 0; d.msum = 1;  // the whole domain
   d.ire = 1.0 / p->Re;
   d.variant = p->variant;
   d.scalar = p->scalar;
@@ -650,7 +659,47 @@ namespace {
 // family, the psi solve beside post1 (it reads only d(rho)/dt).  The 2014
 // variant differentiates the T that its assembly saves, and takes d(rho)
 // from a transform round trip after post1, so it runs in one chain.
-int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
+// The Dev of slab block r: its z transforms (kx planes, buffers Z) or its x
+// stage (lines, buffers X; the mixed form's plane sums after the last block).
+lmc::Dev block_dev(const lmc_handle *h, int r, bool xstage) {
+  lmc::Dev e = h->d;
+  const auto &sp = h->split;
+  const auto &buf = xstage ? sp.X[r] : sp.Z[r];
+  for (int f = 0; f < lmc::NWB; f++) {
+    void *q = f < (int)buf.size() ? buf[f] : nullptr;
+    if (e.prec) e.zbf[f] = (float2 *)q;
+    else e.zb[f] = (double2 *)q;
+  }
+  if (xstage) {
+    e.xt0 = e.xl0 = sp.l0[r];  // one z line per x-stage tile (mgalx >= 144)
+    e.xnt = sp.nl[r];
+    e.msum = r == sp.n - 1;
+  } else {
+    e.zp0 = sp.p0[r];
+    e.zkn = sp.np[r];
+  }
+  return e;
+}
+
+// The plane <-> line exchanges of the slab decomposition (chpl2ln /
+// chln2pl, change.f:1-143) as device copies: block r's planes of block
+// r2's lines, for the first nf z-physical fields.
+int exchange(lmc_handle *h, bool to_lines, int nf, cudaStream_t s) {
+  const auto &sp = h->split;
+  const size_t es = h->d.prec ? sizeof(float2) : sizeof(double2), nkx = (size_t)h->d.nkx;
+  for (int f = 0; f < nf; f++)
+    for (int r = 0; r < sp.n; r++)
+      for (int r2 = 0; r2 < sp.n; r2++) {
+        char *z = (char *)sp.Z[r][f] + (size_t)sp.l0[r2] * sp.np[r] * es;
+        char *x = (char *)sp.X[r2][f] + (size_t)sp.p0[r] * es;
+        const size_t w = (size_t)sp.np[r] * es;
+        if (to_lines) LMC_CK(cudaMemcpy2DAsync(x, nkx * es, z, w, w, sp.nl[r2], cudaMemcpyDeviceToDevice, s));
+        else LMC_CK(cudaMemcpy2DAsync(z, w, x, nkx * es, w, sp.nl[r2], cudaMemcpyDeviceToDevice, s));
+      }
+  return LMC_OK;
+}
+
+int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false, bool split = false) {
   lmc::Dev &d = h->d;
   cudaStream_t s = h->s, s2 = h->s2;
   auto run = [&](int kid, cudaStream_t st, auto &&launch) {
@@ -676,7 +725,21 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
     // the T derivatives and the inverse z transforms of the five inputs
     // made from T (lap T, dT/dx, dT/dy, dT/dz, T) run beside Lapvdvhom, the
     // assembly of rho u_i and the z transforms of rho u_i
-    if (side_t) {
+    if (split) {  // slab blocks: every transform after the y work, block by block
+      if (!fork()) return LMC_ECUDA;
+      run(2, s2, [&] { lmc::launch_tder(d, s2); });
+      if (d.scalar) run(2, s2, [&] { lmc::launch_zder(d, s2); });
+      if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
+      run(0, s, [&] { lmc::launch_lapv(d, s); });
+      run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
+      if (d.visc) run(1, s, [&] { lmc::launch_sgrad(d, s); });
+      if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
+      for (int r = 0; r < h->split.n; r++) {
+        const lmc::Dev e = block_dev(h, r, false);
+        run(3, s, [&] { lmc::launch_zinv(e, s, 0, 0, lmc::n_in(e)); });
+      }
+      if (int rc = exchange(h, true, lmc::n_in(d), s)) return rc;
+    } else if (side_t) {
       if (!fork()) return LMC_ECUDA;
       run(2, s2, [&] { lmc::launch_tder(d, s2); });
       if (d.scalar) run(2, s2, [&] { lmc::launch_zder(d, s2); });
@@ -705,11 +768,23 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false) {
       if (cfl_step) LMC_CK(cudaMemsetAsync(d.cflmax, 0, 4 * sizeof(unsigned long long), s));
     }
     const int do_cfl = cfl_step && rk == 0;
-    run(4, s, [&] {
-      lmc::launch_xphys(d, rk, do_cfl, rk == 0, s);
-      if (d.variant && rk == 0) lmc::launch_cfl14(d, do_cfl, s);
-    });
-    run(5, s, [&] { lmc::launch_zfwd(d, s); });
+    if (split) {
+      for (int r = 0; r < h->split.n; r++) {
+        const lmc::Dev e = block_dev(h, r, true);
+        run(4, s, [&] { lmc::launch_xphys(e, rk, do_cfl, rk == 0, s); });
+      }
+      if (int rc = exchange(h, false, lmc::n_out(d), s)) return rc;
+      for (int r = 0; r < h->split.n; r++) {
+        const lmc::Dev e = block_dev(h, r, false);
+        run(5, s, [&] { lmc::launch_zfwd(e, s); });
+      }
+    } else {
+      run(4, s, [&] {
+        lmc::launch_xphys(d, rk, do_cfl, rk == 0, s);
+        if (d.variant && rk == 0) lmc::launch_cfl14(d, do_cfl, s);
+      });
+      run(5, s, [&] { lmc::launch_zfwd(d, s); });
+    }
     if (st_now) run(10, s, [&] { lmc::launch_stats2(d, h->st, s); });
     if (side_psi) {  // beside post1 and post2, which neither read nor write its data
       if (!fork()) return LMC_ECUDA;
@@ -876,6 +951,49 @@ int lmc_stats_step(lmc_handle *h, int nsteps) {
     h->steps++;
     h->nacum++;  // cross.f:800-801
     h->nacumsp++;
+    if (check_launch(h)) return LMC_ECUDA;
+  }
+  return LMC_OK;
+}
+
+int lmc_step_split(lmc_handle *h, int nblocks, int nsteps) {
+  if (!h || nsteps < 0 || nblocks < 1 || nblocks > h->d.nkx) return LMC_EINVAL;
+  if (h->d.variant || h->d.mgalx < 144) return LMC_EINVAL;  // one z line per x-stage tile
+  if (h->split.n && h->split.n != nblocks) return LMC_EINVAL;
+  if (h->err) return h->err;
+  LMC_CK(cudaSetDevice(h->p.device));
+  auto &sp = h->split;
+  if (!sp.n) {
+    // pointers_calc (change.f:145-211): contiguous blocks, the first
+    // n mod k of them one longer, of the kx planes and of the (z, y) lines
+    const lmc::Dev &d = h->d;
+    const int nlines = d.my * d.mgalz, nz = lmc::n_zbuf(d);
+    const size_t es = d.prec ? sizeof(float2) : sizeof(double2);
+    int p = 0, l = 0;
+    sp.Z.assign(nblocks, {});
+    sp.X.assign(nblocks, {});
+    for (int r = 0; r < nblocks; r++) {
+      const int np = d.nkx / nblocks + (r < d.nkx % nblocks), nl = nlines / nblocks + (r < nlines % nblocks);
+      sp.p0.push_back(p); sp.np.push_back(np); sp.l0.push_back(l); sp.nl.push_back(nl);
+      p += np;
+      l += nl;
+      for (int f = 0; f < nz; f++) {
+        char *z = nullptr, *x = nullptr;
+        int rc = dalloc(h, &z, (size_t)nlines * np * es);
+        if (!rc) rc = dalloc(h, &x, (size_t)nl * d.nkx * es);
+        if (rc) return rc;
+        sp.Z[r].push_back(z);
+        sp.X[r].push_back(x);
+      }
+    }
+    sp.n = nblocks;
+  }
+  const int ncfl = h->p.ncfl > 0 ? h->p.ncfl : 1;
+  for (int n = 0; n < nsteps; n++) {
+    const int cfl_step = (h->p.dt_mode == 0) && (h->steps % ncfl == 0);  // cross.f:240
+    const int rc = enqueue_step(h, cfl_step, false, true);
+    if (rc) return rc;
+    h->steps++;
     if (check_launch(h)) return LMC_ECUDA;
   }
   return LMC_OK;

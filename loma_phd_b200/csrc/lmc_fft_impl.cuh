@@ -103,7 +103,9 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
   ST *St = (ST *)(smraw + round16(sizeof(CT) * KB * LD));
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
-  const int nkb = (d.nkx + KB - 1) / KB, per_f = d.my * nkb, vb = vbase(d);
+  // the kx planes zp0 .. zp0+zkn-1 (a slab block; all planes by default),
+  // written into z-physical rows of zkn values
+  const int nkb = (d.zkn + KB - 1) / KB, per_f = d.my * nkb, vb = vbase(d);
   auto src_of = [&](int f) -> const ST * {
     if constexpr (sizeof(ST) == sizeof(double2)) {
       if (mode == 1) return f == 0 ? d.Told : d.dTs;
@@ -138,12 +140,12 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
   };
   auto lead_of = [&](int t) {
     const int r = t % per_f, y = r / nkb, kb = r - y * nkb;
-    return (int)((((size_t)y * d.nkx + kb * KB) * d.mz) % E);
+    return (int)((((size_t)y * d.nkx + d.zp0 + kb * KB) * d.mz) % E);
   };
   auto issue = [&](int t) {
     const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
-    const int nb = min(KB, d.nkx - kb * KB);
-    const size_t start = ((size_t)y * d.nkx + kb * KB) * d.mz;
+    const int nb = min(KB, d.zkn - kb * KB);
+    const size_t start = ((size_t)y * d.nkx + d.zp0 + kb * KB) * d.mz;
     const int lead = (int)(start % E);
     const uint32_t cnt = (uint32_t)(((nb * d.mz + lead + E - 1) / E) * E);
     const uint32_t bytes = cnt * (uint32_t)sizeof(ST);
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     if (!s_ok) return;
     ph ^= 1;
     const int fr = t / per_f, f = f0 + fr, r = t - fr * per_f, y = r / nkb, kb = r - y * nkb;
-    const int i0 = kb * KB, nb = min(KB, d.nkx - i0);
+    const int i0 = d.zp0 + kb * KB, nb = min(KB, d.zp0 + d.zkn - i0);
     const int lead = lead_of(t);
     // i kx, i kz: of T, Z, and with the variable viscosity of rho u, rho w
     const int mult = mode ? 0 : f >= vb ? (f == vb ? 1 : f == vb + 2 ? 2 : 0)
@@ -189,13 +191,13 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
       issue(t + gridDim.x);
     }
     F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
-    ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.nkx + i0;
+    ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.zkn + (i0 - d.zp0);
     for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
       const int z = idx / KB, il = idx - z * KB;
       // the samples stay in the transform's order (z = k1 + N1 k2 holds the
       // natural sample k2 + N2 k1), except for the export
       const int zr = mode == 2 ? z / N1 + N2 * (z % N1) : z;
-      if (il < nb) dst[(size_t)zr * d.nkx + il] = ccvt<ST>(W[il * LD + F::sk(z)]);
+      if (il < nb) dst[(size_t)zr * d.zkn + il] = ccvt<ST>(W[il * LD + F::sk(z)]);
     }
     __syncthreads();
   }
@@ -211,12 +213,13 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zfwd(Dev d, int mode) 
   extern __shared__ __align__(16) unsigned char smraw[];
   CT *sm = (CT *)smraw;
   constexpr int KB = ZGeo<N1, N2, CT>::KB;
-  const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = blockIdx.x * KB;
-  const int nb = min(KB, d.nkx - i0);
-  const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.nkx + i0;
+  // the kx planes zp0 .. zp0+zkn-1, from z-physical rows of zkn values
+  const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = d.zp0 + blockIdx.x * KB;
+  const int nb = min(KB, d.zp0 + d.zkn - i0);
+  const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.zkn + (i0 - d.zp0);
   for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
     const int z = idx / KB, il = idx - z * KB;
-    if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.nkx + il));
+    if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.zkn + il));
   }
   __syncthreads();
   F::template perm2nat<-1, 2>(sm, nb, G::LD, wtwz<CT>(d));
@@ -247,7 +250,7 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
   ST *A = wzb<ST>(d, fa);
   ST *B = fb >= 0 ? wzb<ST>(d, fb) : nullptr;
   for (int l = 0; l < nzb; l++) {
-    const size_t g0 = ((size_t)y * d.mgalz + z0 + l) * d.nkx;
+    const size_t g0 = ((size_t)y * d.mgalz + z0 + l - d.xl0) * d.nkx;
     const CT *line = sm + (size_t)(p * G::ZB + l) * G::LD;
     for (int k = threadIdx.x; k < d.nkx; k += blockDim.x) {
       const CT c = line[F::sk(k)];
@@ -304,11 +307,15 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
   __shared__ double s_red[3][8];
   __shared__ double s_min[NM], s_est[NO];  // mixed form, per tile
   const int nzk = (d.mgalz + ZB - 1) / ZB;
+  // tile t of this launch is tile xt0 + t of the substep (the x stage of a
+  // slab block of lines, or all of them); its z-physical rows are local to
+  // the block, which starts at line xl0
   auto issue = [&](int t) {
+    t += d.xt0;
     const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
     const uint32_t rb = (uint32_t)nzb * nkx * sizeof(ST), hb = d.variant ? 0u : (uint32_t)nzb * N * sizeof(double);
     mbar_expect_tx(&bar, (stg ? NI * rb : 0u) + (ZS ? 2 : 1) * hb);
-    const size_t g0 = ((size_t)y * d.mgalz + z0) * nkx;
+    const size_t g0 = ((size_t)y * d.mgalz + z0 - d.xl0) * nkx;
     if (stg)
       for (int f = 0; f < NI; f++) bulk_g2s(St + f * ZB * nkx, wzb<ST>(d, f) + g0, rb, &bar);
     if (hb) bulk_g2s(Sr, d.rhst + ((size_t)y * d.mgalz + z0) * N, hb, &bar);
@@ -333,7 +340,7 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
     __syncthreads();
     if (!s_ok) return;
     ph ^= 1;
-    const int y = t / nzk, z0 = (t - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
+    const int tg = d.xt0 + t, y = tg / nzk, z0 = (tg - y * nzk) * ZB, nzb = min(ZB, d.mgalz - z0);
     if constexpr (sizeof(ST) == sizeof(float2)) {  // mixed form: see s_min / s_est below
       const int q = threadIdx.x;
       if (q < NM) s_min[q] = d.mi[(size_t)q * d.my + y];
@@ -372,7 +379,7 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
     // p*ZB + l packs fields 2p, 2p+1 of z line l as A + iB of the complex
     // spectrum, kx = nkx .. N-nkx (the dealiased gap) are zero, and the
     // imaginary part of mode 0 is dropped (rftsingle.f:85-88)
-    const size_t gt = ((size_t)y * d.mgalz + z0) * nkx;  // the tile's rows in global memory
+    const size_t gt = ((size_t)y * d.mgalz + z0 - d.xl0) * nkx;  // the tile's rows in global memory
     auto load = [&](int b, int n) -> CT {
       const int p = b / ZB, l = b - p * ZB;
       if (l >= nzb) return cz<CT>();
@@ -840,13 +847,13 @@ struct Launch {
       f0 = 0;
       nf = mode ? 2 : 8;
     }
-    const int ntiles = nf * d.my * ((d.nkx + ZG::KB - 1) / ZG::KB);
+    const int ntiles = nf * d.my * ((d.zkn + ZG::KB - 1) / ZG::KB);
     const size_t sm = zinv_sm(d.mz);
     const int g = grid_for((const void *)k_zinv<N1, N2, CT, ST>, ZG::ZT, sm, ntiles);
     k_zinv<N1, N2, CT, ST><<<g, ZG::ZT, sm, s>>>(d, ntiles, mode, f0);
   }
   static void zfwd(const Dev &d, int mode, cudaStream_t s) {
-    dim3 g((d.nkx + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : n_out(d)));
+    dim3 g((d.zkn + ZG::KB - 1) / ZG::KB, d.my, mode ? 1 : (d.variant ? 10 : n_out(d)));
     k_zfwd<N1, N2, CT, ST><<<g, ZG::ZT, zsm(), s>>>(d, mode);
   }
   static size_t xexport_sm() { return (size_t)6 * G::ZB * G::LD * sizeof(double2); }
@@ -864,7 +871,7 @@ struct Launch {
   }
   template <bool ZS, bool VS>
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
-    const int ntiles = d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
+    const int ntiles = d.xnt > 0 ? d.xnt : d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
     constexpr int XT = XGeo<N1, N2, ZS || VS>::XT;
     const void *fn = (const void *)k_xphys<N1, N2, CT, ST, ZS, VS>;
     // stage the input rows (TMA, one tile ahead) where that keeps as many
@@ -879,7 +886,7 @@ struct Launch {
     const size_t sm = xphys_sm(d.nkx, ZS, VS, stg);
     const int g = grid_for(fn, XT, sm, ntiles);
     k_xphys<N1, N2, CT, ST, ZS, VS><<<g, XT, sm, s>>>(d, rk, do_cfl, do_diag, ntiles, (int)stg);
-    if constexpr (sizeof(ST) == sizeof(float2)) {
+    if (sizeof(ST) == sizeof(float2) && d.msum) {
       const int nslot = ((d.mgalz + G::ZB - 1) / G::ZB) * (XT / 32);
       k_msum<N1, N2><<<dim3(d.my, n_out(d)), 128, 0, s>>>(d, nslot);
     }

@@ -25,6 +25,12 @@ struct Dev {
   int zb_x, kb_z;           // lines per block of the x / z transform kernels
   int smem_limit;           // opt-in shared memory per block of the device (bytes)
   int xstg;                 // 1: the x stage stages its input rows where they fit (LMC_XSTG=0: never)
+  // Slab blocks (lmc_step_split; the whole domain otherwise): the z
+  // transforms cover kx planes zp0 .. zp0+zkn-1 with z-physical rows of zkn
+  // values; the x stage covers its tiles xt0 .. xt0+xnt-1 (xnt 0: all), whose
+  // z-physical rows start at line xl0; msum 0 skips the mixed form's plane
+  // sums after the x stage (all blocks but the last)
+  int zp0, zkn, xt0, xnt, xl0, msum;
   double ire, peclet, cfl, hxalp, hzbet;
   double gama[3], xi[3], alpha[3], beta[3];
   // y operators: band rows and precomputed scan tables

@@ -30,7 +30,7 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_wait_selftest", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
+    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_wait_selftest", "lmc_step_split", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
     "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read", "lmc_load_scalar_f64", "lmc_get_scalar_f64",
     "lmc_physical_f64",
@@ -108,6 +108,7 @@ def _lib():
         L.lmc_profile_read.argtypes = [vp, ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_int)]
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
         L.lmc_wait_selftest.argtypes = [vp, ctypes.c_uint]
+        L.lmc_step_split.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         L.lmc_use_graphs.argtypes = [vp, ctypes.c_int]
         L.lmc_launches_per_step.argtypes = [vp]
@@ -323,6 +324,11 @@ class Lomacte:
         _check(_lib().lmc_step(self._h, int(n)), "lmc_step")
 
     # passive scalar Z (Params.scalar = 1): reference layout, complex
+    def step_split(self, nblocks: int, n: int = 1):
+        """n RK3 steps with the transform stage split into nblocks slab
+        blocks exchanged by device copies (lmc_step_split)."""
+        _check(_lib().lmc_step_split(self._h, int(nblocks), int(n)), "lmc_step_split")
+
     def load_scalar(self, z):
         a = np.ascontiguousarray(np.asarray(z, dtype=np.complex128).reshape(self.shape))
         _check(_lib().lmc_load_scalar_f64(self._h, _ptr(a.view(np.float64))), "lmc_load_scalar_f64")
