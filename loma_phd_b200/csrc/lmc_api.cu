@@ -739,24 +739,26 @@ int enqueue_step(lmc_handle *h, int cfl_step, bool stats = false, bool split = f
         run(3, s, [&] { lmc::launch_zinv(e, s, 0, 0, lmc::n_in(e)); });
       }
       if (int rc = exchange(h, true, lmc::n_in(d), s)) return rc;
-    } else if (side_t) {
-      if (!fork()) return LMC_ECUDA;
-      run(2, s2, [&] { lmc::launch_tder(d, s2); });
-      if (d.scalar) run(2, s2, [&] { lmc::launch_zder(d, s2); });
-      run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 3, 5); });
-      if (d.scalar) run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 8, 4); });
-      if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
-    }
-    run(0, s, [&] { lmc::launch_lapv(d, s); });
-    run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
-    if (d.visc) run(1, s, [&] { lmc::launch_sgrad(d, s); });  // the strain-rate inputs
-    if (side_t) {
-      run(3, s, [&] { lmc::launch_zinv(d, s, 0, 0, 3); });
-      if (d.visc) run(3, s, [&] { lmc::launch_zinv(d, s, 0, lmc::vbase(d), 6); });
-      if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
     } else {
-      run(2, s, [&] { lmc::launch_tder(d, s); });
-      run(3, s, [&] { lmc::launch_zinv(d, s); });
+      if (side_t) {
+        if (!fork()) return LMC_ECUDA;
+        run(2, s2, [&] { lmc::launch_tder(d, s2); });
+        if (d.scalar) run(2, s2, [&] { lmc::launch_zder(d, s2); });
+        run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 3, 5); });
+        if (d.scalar) run(3, s2, [&] { lmc::launch_zinv(d, s2, 0, 8, 4); });
+        if (cudaEventRecord(h->ev_join, s2) != cudaSuccess) return LMC_ECUDA;
+      }
+      run(0, s, [&] { lmc::launch_lapv(d, s); });
+      run(1, s, [&] { lmc::launch_assemble(d, rk, s); });
+      if (d.visc) run(1, s, [&] { lmc::launch_sgrad(d, s); });  // the strain-rate inputs
+      if (side_t) {
+        run(3, s, [&] { lmc::launch_zinv(d, s, 0, 0, 3); });
+        if (d.visc) run(3, s, [&] { lmc::launch_zinv(d, s, 0, lmc::vbase(d), 6); });
+        if (cudaStreamWaitEvent(s, h->ev_join, 0) != cudaSuccess) return LMC_ECUDA;
+      } else {
+        run(2, s, [&] { lmc::launch_tder(d, s); });
+        run(3, s, [&] { lmc::launch_zinv(d, s); });
+      }
     }
     // statistics of an accumulating step, first substep (cross.f:578-585,
     // 794-812, 1583-1607); id 10 in the profile
