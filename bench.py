@@ -405,6 +405,9 @@ def run_arm(a, w, prec, dev, rank, world, dist, want_e2e, steps, warmup, stats_c
     # substep, lmc_stats_step) beside a plain step, CUDA events on the
     # library's stream, best of three each; plain steps replay a CUDA graph,
     # statistics steps enqueue their kernels directly
+    # the y operators: banded solves against dense GEMMs on the tensor cores
+    # (lmc_yop_tune), on this grid and state
+    yop = {f"op{op}": g.yop_tune(op) for op in (1, 2)} if stats_cost else None
     stats_step = None
     if stats_cost:
         def one(fn):
@@ -453,7 +456,7 @@ def run_arm(a, w, prec, dev, rank, world, dist, want_e2e, steps, warmup, stats_c
     step_bytes = 3 * sum(f(S, Z, P, wb, sc, vs) for f in ALGO.values())
     return {"p": p, "ms": ms, "value": value, "clocks": ck, "roofline": roofline,
             "kernel_share": share, "stage_share": stage_share, "e2e": e2e, "state": state, "Z": zf, "diag": diag,
-            "step_bytes": step_bytes, "stats_step": stats_step,
+            "step_bytes": step_bytes, "stats_step": stats_step, "yop_autotune": yop,
             "launches_per_step": g_launches, "y_family": y_family,
             "step_roofline_frac": (step_bytes * steps / (ms / 1e3) / 1e9) / peak}
 
@@ -622,6 +625,7 @@ def main():
             "stage_share": head["stage_share"],
             "step_roofline_frac": head["step_roofline_frac"],
             "e2e": head["e2e"], "cpu_baseline": cpu, "serving": serving, "stats_step": head["stats_step"],
+            "yop_autotune": head["yop_autotune"],
             "ensemble": ensemble, "medium_grid": medium, "error_long": err_long,
         }
         if mixed and 0 in arms:
@@ -629,7 +633,7 @@ def main():
             line["fp64"] = {"value": f64["value"], "ms_per_step": f64["ms"] / a.steps, "roofline": f64["roofline"],
                             "kernel_share": f64["kernel_share"], "stage_share": f64["stage_share"],
                             "e2e": f64["e2e"], "clocks": f64["clocks"],
-                            "stats_step": f64["stats_step"]}
+                            "stats_step": f64["stats_step"], "yop_autotune": f64["yop_autotune"]}
             line["mixed_over_fp64"] = head["value"] / f64["value"]
             line["error_vs_fp64"] = {"rel_l2": errs, "steps": a.warmup + a.steps,
                                      "note": "mixed vs FP64 GPU path from the same seeded state (e2e steps "

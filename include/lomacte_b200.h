@@ -301,6 +301,24 @@ int lmc_make_ic(const lmc_params *p, const double *y, const lmc_ic_params *ic,
  * Used by the parity tests of the y-kernels. */
 int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev,
              double *out2_dev);
+/* The same operators as dense my x my matrices (column j = the operator
+ * applied to e_j; d/dy and d2/dy2 do not depend on the mode) applied to all
+ * modes as one GEMM on the tensor cores (cuBLAS): op 1 (deryr2) or 2
+ * (deryyr2); method 1 FP64 (DGEMM), method 2 3xTF32 (hi/lo split of both
+ * operands, three TF32 products accumulated in FP32).  Reference layout as
+ * lmc_op_y.  The dense matrices and the GEMM workspace (about 3 x 4 bytes
+ * per point) are made on first use and freed with the handle.  An
+ * alternative to the banded solves, no counterpart in the reference. */
+int lmc_op_y_dense(lmc_handle *h, int op, int method, const double *in_dev, double *out_dev);
+/* Autotuner of the y operator op (1 or 2) on this grid: times, on the
+ * handle's stream with CUDA events (best of three), the banded solve of the
+ * substep (as lmc_op_y) and both dense methods on the current Omega_y, and
+ * their relative L2 difference from the banded result.  out[6]: banded ms,
+ * FP64-GEMM ms, 3xTF32 ms, FP64-GEMM error, 3xTF32 error, choice (0 banded,
+ * 1 FP64 GEMM, 2 3xTF32: the fastest within 1e-12 for the FP64 path, 1e-6
+ * for the mixed forms).  Uses the FP64 staging buffers of the handle; run
+ * between steps. */
+int lmc_yop_tune(lmc_handle *h, int op, double *out);
 /* Compact first y-derivative (the operator of op 1 above) for callers that
  * may not allocate device memory: drivers with a fixed device-memory
  * budget, or time loops that cannot afford the device-wide synchronisation

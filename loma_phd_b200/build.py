@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblomacte_b200.so")
 SOURCES = ["lmc_y_d.cu", "lmc_y_c.cu", "lmc_y_b.cu", "lmc_y_a.cu", "lmc_ytpm.cu", "lmc_fft_c.cu", "lmc_fft_b.cu",
-           "lmc_fft_a.cu", "lmc_api.cu", "lmc_dispatch.cu", "lmc_ykernels.cu", "lmc_noalloc.cu", "lmc_host.cpp"]
+           "lmc_fft_a.cu", "lmc_api.cu", "lmc_dispatch.cu", "lmc_ykernels.cu", "lmc_noalloc.cu", "lmc_yop.cu", "lmc_host.cpp"]
 HEADERS = ["lmc_internal.h", "lmc_kernels.cuh", "lmc_device.cuh", "lmc_fft_impl.cuh", "lmc_async.cuh",
            "lmc_ykernels.cuh", "lmc_ylaunch.h", "lmc_ytpm.cuh", "lmc_stats.cuh"]
 
@@ -69,7 +69,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         for f, l in zip(SOURCES, logs):
             sys.stderr.write(f"==== {f}\n{l}")
     cmd = [nvcc(), "-ccbin", host_cxx(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
-           "-Xcompiler", "-fopenmp", "-o", LIB + ".tmp"] + objs + ["-lgomp"]
+           "-Xcompiler", "-fopenmp", "-o", LIB + ".tmp"] + objs + ["-lcublas", "-lgomp"]
     r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

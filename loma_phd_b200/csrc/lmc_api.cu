@@ -17,6 +17,14 @@
 #include "lmc_async.cuh"
 #include "lmc_kernels.cuh"
 
+namespace lmc {
+// the dense y operators on the tensor cores (lmc_yop.cu)
+struct DenseY;
+DenseY *dense_create(const YOps &ops, size_t ncol, cudaStream_t s, int *rc);
+void dense_destroy(DenseY *z);
+int dense_apply(DenseY *z, int op, int method, const double *in, double *out, cudaStream_t s);
+}  // namespace lmc
+
 struct lmc_handle {
   lmc::Grid g;
   lmc_params p;
@@ -52,6 +60,8 @@ struct lmc_handle {
     std::vector<int> p0, np, l0, nl;
     std::vector<std::vector<void *>> Z, X;
   } split;
+  // dense y operators and their GEMM workspace (lmc_op_y_dense, lmc_yop_tune)
+  lmc::DenseY *yop = nullptr;
   // per-kernel CUDA-event profiling (lmc_profile_start / lmc_profile_read)
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -487,6 +497,7 @@ int lmc_destroy(lmc_handle *h) {
   cudaSetDevice(h->p.device);
   if (h->s) cudaStreamSynchronize(h->s);  // this case's own work only
   drop_graphs(h);
+  lmc::dense_destroy(h->yop);
   for (void *q : h->allocs) {
     if (h->s) cudaFreeAsync(q, h->s);
     else cudaFree(q);
@@ -1200,6 +1211,101 @@ int lmc_op_y(lmc_handle *h, int op, const double *in_dev, double *out_dev, doubl
   if (check_launch(h)) return LMC_ECUDA;
   LMC_CK(cudaStreamSynchronize(h->s));
   return LMC_OK;
+}
+
+namespace {
+// relative L2 difference of two device vectors (sums of squares by atomics:
+// an error estimate, not bit-reproducible)
+__global__ void k_rel_l2(const double *a, const double *b, size_t n, double *acc) {
+  double d2 = 0.0, r2 = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double d = a[i] - b[i];
+    d2 += d * d;
+    r2 += b[i] * b[i];
+  }
+  d2 = lmcd::warp_sum(d2);
+  r2 = lmcd::warp_sum(r2);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(acc, d2);
+    atomicAdd(acc + 1, r2);
+  }
+}
+
+int ensure_dense(lmc_handle *h) {
+  if (h->yop) return LMC_OK;
+  int rc = LMC_OK;
+  h->yop = lmc::dense_create(h->ops, (size_t)2 * h->d.nmode, h->s, &rc);
+  return h->yop ? LMC_OK : rc;
+}
+}  // namespace
+
+int lmc_op_y_dense(lmc_handle *h, int op, int method, const double *in_dev, double *out_dev) {
+  if (!h || op < 1 || op > 2 || method < 1 || method > 2 || !in_dev || !out_dev) return LMC_EINVAL;
+  LMC_CK(cudaSetDevice(h->p.device));
+  if (int rc = ensure_dense(h)) return rc;
+  const lmc::Dev &d = h->d;
+  lmc::launch_ref2dev(d, (const double2 *)in_dev, d.sb[7], h->s);
+  if (int rc = lmc::dense_apply(h->yop, op, method, (const double *)d.sb[7], (double *)d.sb[8], h->s)) return rc;
+  lmc::launch_dev2ref(d, d.sb[8], (double2 *)out_dev, h->s);
+  if (check_launch(h)) return LMC_ECUDA;
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return LMC_OK;
+}
+
+int lmc_yop_tune(lmc_handle *h, int op, double *out) {
+  if (!h || op < 1 || op > 2 || !out) return LMC_EINVAL;
+  if (h->err) return h->err;
+  LMC_CK(cudaSetDevice(h->p.device));
+  if (int rc = ensure_dense(h)) return rc;
+  const lmc::Dev &d = h->d;
+  const size_t n = (size_t)2 * d.nmode * d.my;
+  const double2 *in = d.vor;  // the state's Omega_y, device layout
+  double *ref = (double *)d.sb[8], *alt = (double *)d.sb[9];
+  double *acc = nullptr;
+  LMC_CK(cudaMallocAsync((void **)&acc, 2 * sizeof(double), h->s));
+  cudaEvent_t e0, e1;
+  LMC_CK(cudaEventCreate(&e0));
+  LMC_CK(cudaEventCreate(&e1));
+  auto timed = [&](int method) -> double {  // best of three, ms
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; rep++) {
+      cudaEventRecord(e0, h->s);
+      if (method == 0) lmc::launch_op_y(d, op, in, (double2 *)ref, nullptr, h->s);
+      else if (lmc::dense_apply(h->yop, op, method, (const double *)in, alt, h->s)) return -1.0;
+      cudaEventRecord(e1, h->s);
+      cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) best = ms;
+    }
+    return best;
+  };
+  double err[3] = {0.0, 0.0, 0.0};
+  out[0] = timed(0);
+  for (int m = 1; m <= 2; m++) {
+    out[m] = timed(m);
+    cudaMemsetAsync(acc, 0, 2 * sizeof(double), h->s);
+    k_rel_l2<<<148 * 8, 256, 0, h->s>>>(alt, ref, n, acc);
+    double hs[2] = {0.0, 0.0};
+    cudaMemcpyAsync(hs, acc, sizeof(hs), cudaMemcpyDeviceToHost, h->s);
+    cudaStreamSynchronize(h->s);
+    err[m] = hs[1] > 0.0 ? std::sqrt(hs[0] / hs[1]) : std::sqrt(hs[0]);
+  }
+  out[3] = err[1];
+  out[4] = err[2];
+  // the fastest method whose difference from the banded solve is within
+  // the form's budget (FP64 path 1e-12, mixed forms 1e-6)
+  const double tol = d.prec ? 1e-6 : 1e-12;
+  int best = 0;
+  for (int m = 1; m <= 2; m++)
+    if (out[m] > 0.0 && err[m] <= tol && out[m] < out[best]) best = m;
+  out[5] = best;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(acc, h->s);
+  if (check_launch(h)) return LMC_ECUDA;
+  LMC_CK(cudaStreamSynchronize(h->s));
+  return (out[1] < 0.0 || out[2] < 0.0) ? LMC_ECUDA : LMC_OK;
 }
 
 }  // extern "C"

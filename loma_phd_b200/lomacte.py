@@ -30,7 +30,8 @@ SYMBOLS = (
     "lmc_get_state_f64", "lmc_get_state_f32", "lmc_step", "lmc_sync",
     "lmc_get_diag", "lmc_status", "lmc_strerror", "lmc_stream",
     "lmc_state_device_ptrs", "lmc_make_ic", "lmc_op_y", "lmc_profile_start",
-    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_wait_selftest", "lmc_step_split", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
+    "lmc_profile_read", "lmc_deryr2_noalloc", "lmc_wait_selftest", "lmc_step_split",
+    "lmc_op_y_dense", "lmc_yop_tune", "lmc_y_metrics", "lmc_use_graphs", "lmc_query",
     "lmc_device_bytes", "lmc_footprint", "lmc_launches_per_step", "lmc_y_family",
     "lmc_stats_reset", "lmc_stats_step", "lmc_stats_read", "lmc_load_scalar_f64", "lmc_get_scalar_f64",
     "lmc_physical_f64",
@@ -109,6 +110,8 @@ def _lib():
         L.lmc_deryr2_noalloc.argtypes = [ctypes.c_int, _dp, ctypes.c_int, vp, vp, vp]
         L.lmc_wait_selftest.argtypes = [vp, ctypes.c_uint]
         L.lmc_step_split.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.lmc_op_y_dense.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.lmc_yop_tune.argtypes = [vp, ctypes.c_int, _dp]
         L.lmc_y_metrics.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         L.lmc_use_graphs.argtypes = [vp, ctypes.c_int]
         L.lmc_launches_per_step.argtypes = [vp]
@@ -406,6 +409,22 @@ class Lomacte:
                 return None
             return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
         _check(_lib().lmc_op_y(self._h, op, p(inp), p(out), p(out2)), "lmc_op_y")
+
+    def op_y_dense(self, op: int, method: int, inp, out):
+        """The y operator op (1 d/dy, 2 d2/dy2) as a dense GEMM (method 1
+        FP64, 2 3xTF32) on device buffers in the reference layout."""
+        p = lambda x: ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
+        _check(_lib().lmc_op_y_dense(self._h, int(op), int(method), p(inp), p(out)), "lmc_op_y_dense")
+
+    def yop_tune(self, op: int = 1) -> dict:
+        """Banded solve against the dense GEMMs for the y operator op on the
+        current state (lmc_yop_tune): times in ms, errors, the choice."""
+        out = np.zeros(6)
+        _check(_lib().lmc_yop_tune(self._h, int(op), _ptr(out)), "lmc_yop_tune")
+        names = ("banded", "dense_fp64", "dense_3xtf32")
+        return {"op": op, "ms": dict(zip(names, out[:3].tolist())),
+                "rel_err_vs_banded": {"dense_fp64": float(out[3]), "dense_3xtf32": float(out[4])},
+                "choice": names[int(out[5])]}
 
     def profile_start(self):
         _check(_lib().lmc_profile_start(self._h), "lmc_profile_start")
