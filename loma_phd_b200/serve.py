@@ -26,7 +26,7 @@ from typing import Callable, Dict, List, Optional
 
 import numpy as np
 
-from .lomacte import ICParams, Lomacte, Params, footprint, make_ic, stretched_mesh
+from .lomacte import LMC_ENAN, ICParams, Lomacte, LomacteError, Params, footprint, make_ic, stretched_mesh
 
 
 @dataclasses.dataclass
@@ -41,11 +41,14 @@ class RunRequest:
     amp: float = 1e-2       # perturbation amplitude
     seed: int = 0
     precision: int = 1
-    dt: float = 0.01
+    dt: float = 1e-4        # the initial Deltat of the reference's CFL mode (main.f:559)
     arrival: float = 0.0    # seconds after the start of the stream
 
     def params(self, device: int = 0) -> Params:
-        return Params.from_modes(self.nx, self.nz, self.ny, Re=self.Re, dt_mode=1, dt=self.dt,
+        """Deltat from CFL = 0.5 every 10 steps (the reference's run mode,
+        hre.dat CFL / ncfl), so every request is stable whatever its grid and
+        Reynolds number."""
+        return Params.from_modes(self.nx, self.nz, self.ny, Re=self.Re, dt_mode=0, dt=self.dt, cfl=0.5, ncfl=10,
                                  precision=self.precision, device=device)
 
     @property
@@ -121,6 +124,7 @@ class Server:
         used = 0
         peak_used = 0
         max_conc = 0
+        diverged = 0
         setup: List[float] = []
         pool = ThreadPoolExecutor(max_workers=self.prep_workers)
         t0 = clock()
@@ -161,7 +165,13 @@ class Server:
                     if a.remaining > 0:
                         self._enqueue(a)
                         continue
-                    d = a.case.diag()
+                    try:
+                        d = a.case.diag()
+                    except LomacteError as e:  # a run that went non-finite ends, reported
+                        if e.code != LMC_ENAN:
+                            raise
+                        d = {"status": e.code}
+                        diverged += 1
                     st = a.case.get_state() if self.keep_state else None
                     fin = clock() - t0
                     results.append(RunResult(rid, a.req.arrival, a.admitted, fin, a.req.steps, a.req.mpts, d, st))
@@ -187,6 +197,7 @@ class Server:
             "peak_device_bytes": peak_used,
             "max_concurrent": max_conc,
             "mean_setup_s": float(np.mean(setup)) if setup else None,
+            "diverged": diverged,
         }
         return {"results": sorted(results, key=lambda r: r.rid), "stats": stats}
 
