@@ -101,7 +101,14 @@ ALGO = {
 # with fewer y points (profiles/), scaled to a full launch by ny, as every
 # kernel's traffic grows in proportion to ny at fixed x/z sizes.  None:
 # not captured for that kernel.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    # 768^2 x 33 (mgal 1152^2), mu = T^0.7 + scalar: profiles/kernels_transforms_large_768x33x768.md
+    ("large", False, 1, 1): {"xphys": (4.9096e9, 33)},
+    ("large", True, 1, 1): {"xphys": (8.3872e9, 33)},
+    # 256^2 x 65 (mgal 384^2), mu = T^0.7 + scalar: profiles/kernels_xphys_mu07_scalar_256x65x256.md
+    ("medium", False, 1, 1): {"xphys": (1026.2e6, 65)},
+    ("medium", True, 1, 1): {"xphys": (1791.0e6, 65)},
+}
 
 MIXED_NAMES = {1: "mixed (FP32 storage and FFTs, FP64 state/solves/00 modes)",
                2: "mixed (FP32 storage, FP64 FFT arithmetic, state/solves/00 modes)"}
@@ -145,6 +152,7 @@ def parse():
 def wl(a, name=None):
     """The workload's parameters (ny overridden by --ny for the main one)."""
     w = dict(WORKLOADS[name or a.workload])
+    w["name"] = name or a.workload
     if name is None and a.ny:
         w["ny"] = a.ny
         w["y_cpu"] = min(w["y_cpu"], a.ny)
@@ -446,7 +454,7 @@ def run_arm(a, w, prec, dev, rank, world, dist, want_e2e, steps, warmup, stats_c
               "rhs_and_rk3_update": ("post2",)}
     tot = sum(share.get(k, 0.0) for ks in stages.values() for k in ks)
     stage_share = {n: round(sum(share.get(k, 0.0) for k in ks) / max(tot, 1e-12), 4) for n, ks in stages.items()}
-    tr = NCU_TRAFFIC.get((a.workload, prec == 0, sc, vs), {}).get(top)
+    tr = NCU_TRAFFIC.get((w["name"], prec == 0, sc, vs), {}).get(top)
     traffic = tr[0] * p.my / tr[1] if tr else None
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
