@@ -128,7 +128,9 @@ def parse():
                     help="1: FP32 FFT arithmetic; 2: FP64 FFT arithmetic on FP32 storage")
     ap.add_argument("--no-medium", action="store_true", help="skip the medium-grid line beside the headline")
     ap.add_argument("--error-steps", type=int, default=1000,
-                    help="steps of the medium-grid mixed-vs-FP64 error run (0: skip)")
+                    help="steps of the mixed-vs-FP64 error run (0: skip)")
+    ap.add_argument("--error-workload", default="medium", choices=tuple(WORKLOADS),
+                    help="workload of the error run (the large one takes about 25 GPU-minutes for 1000 steps)")
     ap.add_argument("--serve-requests", type=int, default=16,
                     help="requests of the synthetic serving stream (0: skip)")
     ap.add_argument("--serve-scale", type=float, default=0.05,
@@ -484,30 +486,39 @@ def state_errors(m, r):
 
 
 def error_run(a, dev, nsteps):
-    """Both forms advanced nsteps from the same seeded state of the medium
-    grid: relative L2 per field, the largest relative difference of the
-    momentum-thickness history, and the time per step of each form."""
+    """Both forms advanced nsteps from the same seeded state of the error
+    workload: relative L2 per field, the largest relative difference of the
+    momentum-thickness history (every 10 steps), the Deltat sequences (CFL
+    mode), the simulated time reached and the time per step of each form."""
     import torch
-    w = wl(a, "medium")
+    w = wl(a, a.error_workload)
     res = {}
+    every = 10
     for prec in (0, a.mixed_form):
         p, y, st, z0, g = make_case(a, w, prec, dev, 0)
-        dm = []
+        dm, dts = [], []
         s = torch.cuda.ExternalStream(g.stream, device=dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        for n in range(nsteps // 50):
-            g.step(50)
-            dm.append(g.diag()["dm"])
+        for n in range(nsteps // every):
+            g.step(every)
+            dg = g.diag()
+            dm.append(dg["dm"])
+            dts.append(dg["Deltat"])
         e1.record(s)
         torch.cuda.synchronize()
         res[prec] = {"state": g.get_state(), "Z": g.get_scalar() if a.scalar else None, "dm": np.array(dm),
-                     "ms": e0.elapsed_time(e1) / max(1, nsteps // 50 * 50)}
+                     "dt": np.array(dts), "time": g.diag()["time"] + g.diag()["Deltat"],
+                     "ms": e0.elapsed_time(e1) / max(1, nsteps // every * every)}
         g.close()
+        gc.collect()
     m, r = res[a.mixed_form], res[0]
     dmerr = float(np.abs(m["dm"] - r["dm"]).max() / np.abs(r["dm"]).max()) if len(r["dm"]) else None
-    return {"steps": nsteps // 50 * 50, "grid": f"{w['nx']}x{w['ny']}x{w['nz']}", "form": a.mixed_form,
-            "rel_l2": state_errors(m, r), "dm_history_max_rel": dmerr,
+    dterr = float(np.abs(m["dt"] - r["dt"]).max() / np.abs(r["dt"]).max()) if len(r["dt"]) else None
+    return {"steps": nsteps // every * every, "grid": f"{w['nx']}x{w['ny']}x{w['nz']}", "form": a.mixed_form,
+            "workload": w["desc"], "rel_l2": state_errors(m, r), "dm_history_max_rel": dmerr,
+            "deltat_history_max_rel": dterr, "time_reached": {"mixed": m["time"], "fp64": r["time"]},
+            "dm_final": {"mixed": float(m["dm"][-1]), "fp64": float(r["dm"][-1])} if len(r["dm"]) else None,
             "ms_per_step": {"mixed": m["ms"], "fp64": r["ms"]}, "note": "mixed vs FP64 GPU path, same seeded state"}
 
 
