@@ -562,6 +562,90 @@ struct Four {
     __syncthreads();
   }
 
+  // The first pass of nat2perm for real inputs packed two per line (A + iB)
+  // under the 2/3 rule: only the N/3 lowest modes of A and B are nonzero,
+  // given as rows of nkx = N/3 complex values; the transform input is A + iB
+  // at n < nkx, its conjugate mirror at n > N - nkx and zero in the gap
+  // (the imaginary parts of mode 0 dropped, rftsingle.f:85-88).  With
+  // N2 % 3 == 0 the gap and the mirrored third are fixed ranges of the
+  // sample index j of a task (n = n1 + N1 j), so no sample is tested and
+  // the gap is never loaded.  rows(b, A, B) gives line b's two rows (false:
+  // a padding line, all zero).  Ends with a barrier.
+  template <int SIGN, typename ST, typename R>
+  __device__ static void nat2perm_in3(CT *sm, int nb, int ld, const CT *__restrict__ twN, R &&rows) {
+    static_assert(N2 % 3 == 0, "the 2/3-rule gap must be whole sample rows");
+    constexpr int J1 = N2 / 3, J2 = 2 * N2 / 3;
+    using Re = typename CReal<CT>::R;
+    auto cv = [](const ST &v) { return cmk<CT>((Re)v.x, (Re)v.y); };
+    for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
+      const int b = idx / N1, n1 = idx - b * N1;
+      CT *p = sm + (size_t)b * ld + n1;
+      const ST *A = nullptr, *B = nullptr;
+      const bool ok = rows(b, A, B);
+      CT x[N2];
+#pragma unroll
+      for (int j = 0; j < N2; j++) x[j] = cz<CT>();
+      if (ok) {
+#pragma unroll
+        for (int j = 0; j < J1; j++) {  // A + iB, n = n1 + N1 j < nkx
+          const int n = n1 + N1 * j;
+          const CT a = cv(A[n]), c = cv(B[n]);
+          x[j] = (j == 0 && n1 == 0) ? cmk<CT>(a.x, c.x) : cmk<CT>(a.x - c.y, a.y + c.x);
+        }
+#pragma unroll
+        for (int j = J2; j < N2; j++) {  // conj(A) + i conj(B) at k = N - n < nkx
+          const int k = N - n1 - N1 * j;
+          if (j > J2 || n1 > 0) {
+            const CT a = cv(A[k]), c = cv(B[k]);
+            x[j] = cmk<CT>(a.x + c.y, c.x - a.y);
+          }
+        }
+      }
+      rdft<N2, SIGN>(x);
+#pragma unroll
+      for (int k = 0; k < N2; k++) {
+        CT v = x[k];
+        if (k > 0 && n1 > 0) {
+          CT w = __ldg(twN + n1 * k);
+          if (SIGN > 0) w = cconj(w);
+          v = cmul(v, w);
+        }
+        p[k * (N1 + 1)] = v;
+      }
+    }
+    __syncthreads();
+  }
+
+  // nat2perm of lines whose samples N/3 .. 2N/3 are zero (the 3/2-rule
+  // padding of the z transforms: kz = nz1+1 .. nz1+gap), with N2 % 3 == 0:
+  // the first pass neither reads those samples nor needs them stored.
+  template <int SIGN>
+  __device__ static void nat2perm_gap(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
+    static_assert(N2 % 3 == 0, "the padding gap must be whole sample rows");
+    constexpr int J1 = N2 / 3, J2 = 2 * N2 / 3;
+    for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
+      const int b = idx / N1, n1 = idx - b * N1;
+      CT *p = sm + (size_t)b * ld + n1;
+      CT x[N2];
+#pragma unroll
+      for (int j = 0; j < N2; j++)
+        x[j] = (j < J1 || j > J2 || (j == J2 && n1 > 0)) ? p[j * (N1 + 1)] : cz<CT>();
+      rdft<N2, SIGN>(x);
+#pragma unroll
+      for (int k = 0; k < N2; k++) {
+        CT v = x[k];
+        if (k > 0 && n1 > 0) {
+          CT w = __ldg(twN + n1 * k);
+          if (SIGN > 0) w = cconj(w);
+          v = cmul(v, w);
+        }
+        p[k * (N1 + 1)] = v;
+      }
+    }
+    __syncthreads();
+    nat2perm_p2<SIGN>(sm, nb, ld);
+  }
+
   // the second pass of nat2perm (ends with a barrier)
   template <int SIGN, int U = 1>
   __device__ static void nat2perm_p2(CT *sm, int nb, int ld) {

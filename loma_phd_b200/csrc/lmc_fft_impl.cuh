@@ -169,10 +169,11 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     // i kx, i kz: of T, Z, and with the variable viscosity of rho u, rho w
     const int mult = mode ? 0 : f >= vb ? (f == vb ? 1 : f == vb + 2 ? 2 : 0)
                                         : (f == 4 || f == 9) ? 1 : (f == 6 || f == 11) ? 2 : 0;
-    for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
-      const int il = idx / gap, g = idx - il * gap;
-      W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
-    }
+    if constexpr (N2 % 3 != 0)  // with N2 % 3 == 0 the transform skips the gap
+      for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
+        const int il = idx / gap, g = idx - il * gap;
+        W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
+      }
     for (int il = 0; il < nb; il++) {
       const Re kx = (Re)__ldg(d.kx + i0 + il);
       const ST *row = St + lead + il * d.mz;
@@ -190,7 +191,8 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
       fence_proxy_async();
       issue(t + gridDim.x);
     }
-    F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
+    if constexpr (N2 % 3 == 0) F::template nat2perm_gap<+1>(W, nb, LD, wtwz<CT>(d));
+    else F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
     ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.zkn + (i0 - d.zp0);
     for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
       const int z = idx / KB, il = idx - z * KB;
@@ -396,7 +398,18 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
       }
       return cz<CT>();
     };
-    F::template nat2perm_in<+1>(W, NL * ZB, LD, wtwx<CT>(d), load);
+    if constexpr (N2 % 3 == 0) {  // the gap and the mirrored third by sample row
+      auto rows = [&](int b, const ST *&A, const ST *&B) -> bool {
+        const int p = b / ZB, l = b - p * ZB;
+        if (l >= nzb) return false;
+        A = stg ? St + (2 * p) * ZB * nkx + l * nkx : wzb<ST>(d, 2 * p) + gt + l * nkx;
+        B = stg ? A + ZB * nkx : wzb<ST>(d, 2 * p + 1) + gt + l * nkx;
+        return true;
+      };
+      F::template nat2perm_in3<+1, ST>(W, NL * ZB, LD, wtwx<CT>(d), rows);
+    } else {
+      F::template nat2perm_in<+1>(W, NL * ZB, LD, wtwx<CT>(d), load);
+    }
     // the staged rows are consumed: stage the next tile meanwhile
     if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
       fence_proxy_async();
