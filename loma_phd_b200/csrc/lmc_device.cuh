@@ -616,20 +616,27 @@ struct Four {
     __syncthreads();
   }
 
-  // nat2perm of lines whose samples N/3 .. 2N/3 are zero (the 3/2-rule
-  // padding of the z transforms: kz = nz1+1 .. nz1+gap), with N2 % 3 == 0:
-  // the first pass neither reads those samples nor needs them stored.
-  template <int SIGN>
-  __device__ static void nat2perm_gap(CT *sm, int nb, int ld, const CT *__restrict__ twN) {
+  // The first pass of nat2perm for the 3/2-padded z lines read straight
+  // from their spectral rows: sample n of line b is coefficient n (n < N/3),
+  // zero (the padding N/3 .. 2N/3) or coefficient n - N/3 - 1 (the negative
+  // wavenumbers, n > 2N/3); get(b, k) returns coefficient k of line b.
+  // N2 % 3 == 0, so the three ranges are fixed ranges of the sample row j.
+  // Ends with a barrier.
+  template <int SIGN, typename G>
+  __device__ static void nat2perm_zin(CT *sm, int nb, int ld, const CT *__restrict__ twN, G &&get) {
     static_assert(N2 % 3 == 0, "the padding gap must be whole sample rows");
-    constexpr int J1 = N2 / 3, J2 = 2 * N2 / 3;
+    constexpr int J1 = N2 / 3, J2 = 2 * N2 / 3, SH = N / 3 + 1;
     for (int idx = threadIdx.x; idx < nb * N1; idx += blockDim.x) {
       const int b = idx / N1, n1 = idx - b * N1;
       CT *p = sm + (size_t)b * ld + n1;
       CT x[N2];
 #pragma unroll
-      for (int j = 0; j < N2; j++)
-        x[j] = (j < J1 || j > J2 || (j == J2 && n1 > 0)) ? p[j * (N1 + 1)] : cz<CT>();
+      for (int j = 0; j < N2; j++) {
+        const int n = n1 + N1 * j;
+        if (j < J1) x[j] = get(b, n);
+        else if (j > J2 || (j == J2 && n1 > 0)) x[j] = get(b, n - SH);
+        else x[j] = cz<CT>();
+      }
       rdft<N2, SIGN>(x);
 #pragma unroll
       for (int k = 0; k < N2; k++) {
@@ -643,7 +650,6 @@ struct Four {
       }
     }
     __syncthreads();
-    nat2perm_p2<SIGN>(sm, nb, ld);
   }
 
   // the second pass of nat2perm (ends with a barrier)

@@ -169,30 +169,46 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zinv(Dev d, int ntiles
     // i kx, i kz: of T, Z, and with the variable viscosity of rho u, rho w
     const int mult = mode ? 0 : f >= vb ? (f == vb ? 1 : f == vb + 2 ? 2 : 0)
                                         : (f == 4 || f == 9) ? 1 : (f == 6 || f == 11) ? 2 : 0;
-    if constexpr (N2 % 3 != 0)  // with N2 % 3 == 0 the transform skips the gap
+    if constexpr (N2 % 3 == 0) {
+      // the first pass reads the staged rows: coefficient k of line il
+      auto get = [&](int il, int k) -> CT {
+        CT v = ccvt<CT>(St[lead + il * d.mz + k]);
+        if (mult == 1) v = cik((Re)__ldg(d.kx + i0 + il), v);
+        else if (mult == 2) v = cik((Re)__ldg(d.kz + k), v);
+        if constexpr (sizeof(ST) == sizeof(float2))
+          if (i0 + il == 0 && k == 0) v = cz<CT>();  // 00 mode: added back in FP64 by xphys
+        return v;
+      };
+      F::template nat2perm_zin<+1>(W, nb, LD, wtwz<CT>(d), get);
+      if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {  // the staged rows are consumed
+        fence_proxy_async();
+        issue(t + gridDim.x);
+      }
+      F::template nat2perm_p2<+1>(W, nb, LD);
+    } else {
       for (int idx = threadIdx.x; idx < nb * gap; idx += blockDim.x) {
         const int il = idx / gap, g = idx - il * gap;
         W[il * LD + F::sk(d.nz1 + 1 + g)] = cz<CT>();
       }
-    for (int il = 0; il < nb; il++) {
-      const Re kx = (Re)__ldg(d.kx + i0 + il);
-      const ST *row = St + lead + il * d.mz;
-      for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
-        CT v = ccvt<CT>(row[k]);
-        if (mult == 1) v = cik(kx, v);
-        else if (mult == 2) v = cik((Re)__ldg(d.kz + k), v);
-        if constexpr (sizeof(ST) == sizeof(float2))
-          if (i0 + il == 0 && k == 0) v = cz<CT>();  // 00 mode: added back in FP64 by xphys
-        W[il * LD + F::sk(kz_pad(d, k))] = v;
+      for (int il = 0; il < nb; il++) {
+        const Re kx = (Re)__ldg(d.kx + i0 + il);
+        const ST *row = St + lead + il * d.mz;
+        for (int k = threadIdx.x; k < d.mz; k += blockDim.x) {
+          CT v = ccvt<CT>(row[k]);
+          if (mult == 1) v = cik(kx, v);
+          else if (mult == 2) v = cik((Re)__ldg(d.kz + k), v);
+          if constexpr (sizeof(ST) == sizeof(float2))
+            if (i0 + il == 0 && k == 0) v = cz<CT>();  // 00 mode: added back in FP64 by xphys
+          W[il * LD + F::sk(kz_pad(d, k))] = v;
+        }
       }
+      __syncthreads();
+      if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
+        fence_proxy_async();
+        issue(t + gridDim.x);
+      }
+      F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) {
-      fence_proxy_async();
-      issue(t + gridDim.x);
-    }
-    if constexpr (N2 % 3 == 0) F::template nat2perm_gap<+1>(W, nb, LD, wtwz<CT>(d));
-    else F::template nat2perm<+1>(W, nb, LD, wtwz<CT>(d));
     ST *dst = wzb<ST>(d, f) + (size_t)y * F::N * d.zkn + (i0 - d.zp0);
     for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
       const int z = idx / KB, il = idx - z * KB;
