@@ -442,8 +442,9 @@ int lmc_create(const lmc_params *p, const double *y, lmc_handle **out) {
     }
   }
   if (d.prec) {
-    // partial-sum slots: (mgalz / lines per x tile) tiles x at most 4 warps
-    d.mpart_ld = 8 * g.mgalz;  // one slot per (z tile, warp), at most eight warps per tile
+    // partial-sum slots: one per (z tile, warp), at most mgalz tiles of
+    // lmc::XW_MAX warps
+    d.mpart_ld = lmc::XW_MAX * g.mgalz;
     if ((d.visc && (rc = dalloc(h, &d.vscr, (size_t)3 * g.my))) || (rc = dalloc(h, &d.mi, (size_t)lmc::NMI * g.my)) || (rc = dalloc(h, &h->mo[0], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &h->mo[1], (size_t)12 * g.my)) ||
         (rc = dalloc(h, &d.mpart, (size_t)12 * g.my * d.mpart_ld))) {

@@ -50,16 +50,20 @@ struct Geo {
 // Threads of an x-stage block.  With the passive scalar or the variable
 // viscosity the x stage stages 12 to 18 inputs and transforms 6 to 9 lines
 // per z line, so shared memory admits fewer blocks per SM: those blocks
-// get twice the threads (four warps), and eight warps for lines of 1152
-// points and more (N1 >= 32), of which only one or two blocks fit an SM.
-// XW_MAX warps at most: the partial-sum slots of the mixed form.
-constexpr int XW_MAX = 8;
-template <int N1, int N2, bool WIDE>
+// get twice the threads (four warps), and for lines of 1152 points and
+// more (N1 >= 32), of which only one or two blocks fit an SM, eight warps
+// (FP64 butterflies) or nine (FP32: one task per thread in the first pass
+// of the nine inverse lines, 9 x 32, and four physical points per thread
+// at 1152, kept at two blocks per SM).  At most XW_MAX warps.
+template <int N1, int N2, bool WIDE, bool F32>
 struct XGeo {
   static constexpr int XT = !WIDE ? Geo<N1, N2>::XT
-                            : N1 >= 32 ? 256
+                            : N1 >= 32 ? (F32 ? 288 : 256)
                                        : (2 * Geo<N1, N2>::XT < 128 ? 2 * Geo<N1, N2>::XT : 128);
   static constexpr int PT = (Geo<N1, N2>::ZB * Geo<N1, N2>::N + XT - 1) / XT;
+  // blocks per SM the register budget is sized for (FP32 butterflies; one
+  // block of lines longer than 1152 fits an SM's shared memory)
+  static constexpr int MINB = !F32 ? 1 : (WIDE && N1 >= 32) ? (N1 * N2 <= 1152 ? 2 : 1) : 512 / XT;
 };
 
 // z-transform blocks by butterfly type: twice as many kx lines for FP32
@@ -235,9 +239,31 @@ __global__ void __launch_bounds__(ZGeo<N1, N2, CT>::ZT) k_zfwd(Dev d, int mode) 
   const int f = mode ? ODRHO : (int)blockIdx.z, y = blockIdx.y, i0 = d.zp0 + blockIdx.x * KB;
   const int nb = min(KB, d.zp0 + d.zkn - i0);
   const ST *src = wzb<ST>(d, mode ? 0 : f) + (size_t)y * N1 * N2 * d.zkn + (i0 - d.zp0);
-  for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
-    const int z = idx / KB, il = idx - z * KB;
-    if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.zkn + il));
+  // each z row of the tile is a short run (KB values) at stride zkn: every
+  // thread issues a batch of BT of these loads before storing any
+  constexpr int ZT = ZGeo<N1, N2, CT>::ZT;
+  if constexpr (ZT == KB * N1) {  // thread (z0, il) reads rows z0, z0 + N1, ... of line il
+    constexpr int BT = N2 % 12 == 0 ? 12 : 8;
+    const int il = threadIdx.x % KB, z0 = threadIdx.x / KB;
+    if (il < nb) {
+      const ST *p = src + (size_t)z0 * d.zkn + il;
+      const size_t st = (size_t)N1 * d.zkn;
+      CT *q = sm + il * G::LD;
+      for (int i = 0; i < N2; i += BT) {
+        ST v[BT];
+#pragma unroll
+        for (int u = 0; u < BT; u++)
+          if (i + u < N2) v[u] = __ldg(p + (size_t)(i + u) * st);
+#pragma unroll
+        for (int u = 0; u < BT; u++)
+          if (i + u < N2) q[F::sk(z0 + (i + u) * N1)] = ccvt<CT>(v[u]);
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < F::N * KB; idx += blockDim.x) {
+      const int z = idx / KB, il = idx - z * KB;
+      if (il < nb) sm[il * G::LD + F::sk(z)] = ccvt<CT>(__ldg(src + (size_t)z * d.zkn + il));
+    }
   }
   __syncthreads();
   F::template perm2nat<-1, 2>(sm, nb, G::LD, wtwz<CT>(d));
@@ -299,14 +325,16 @@ __device__ __forceinline__ void x_extract(const Dev &d, const CT *sm, int p, int
 // twelfth output, packed beside Delta T.  VS: the variable viscosity's six
 // more input rows (vbase), with T^sigma in the diffusion of T and Z and
 // the variable part of the stress taken off the products rho u_i u_j.
+// FP32 butterflies: the registers of XGeo::MINB blocks per SM
 template <int N1, int N2, typename CT, typename ST, bool ZS, bool VS>
-// FP32 butterflies: at most about 128 registers, so that eight 64-thread
-// blocks (or the same thread count in larger blocks) share an SM
-__global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == sizeof(float2) ? 512 / XGeo<N1, N2, ZS || VS>::XT : 1) k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles, int stg) {
+__global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS, sizeof(CT) == sizeof(float2)>::XT,
+                                  XGeo<N1, N2, ZS || VS, sizeof(CT) == sizeof(float2)>::MINB)
+    k_xphys(Dev d, int rk, int do_cfl, int do_diag, int ntiles, int stg) {
   using F = Four<N1, N2, CT>;
   using G = Geo<N1, N2>;
   using Re = typename CReal<CT>::R;
-  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, ZS || VS>::PT, XT = XGeo<N1, N2, ZS || VS>::XT;
+  constexpr int N = F::N, ZB = G::ZB, LD = G::LD, PT = XGeo<N1, N2, ZS || VS, sizeof(CT) == sizeof(float2)>::PT,
+                XT = XGeo<N1, N2, ZS || VS, sizeof(CT) == sizeof(float2)>::XT;
   constexpr int VB = ZS ? 12 : 8;  // first viscosity input
   constexpr int NI = VB + (VS ? 6 : 0), NL = NI / 2, NO = ZS ? 12 : 11, NM = VS ? NMI : ZS ? 8 : 6;
   static_assert(XT / 32 <= XW_MAX, "partial-sum slots assume at most XW_MAX warps per x tile");
@@ -322,7 +350,7 @@ __global__ void __launch_bounds__(XGeo<N1, N2, ZS || VS>::XT, sizeof(CT) == size
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ok;
   __shared__ unsigned long long s_tmax[ZB], s_vmax;
-  __shared__ double s_red[3][8];
+  __shared__ double s_red[3][XW_MAX];
   __shared__ double s_min[NM], s_est[NO];  // mixed form, per tile
   const int nzk = (d.mgalz + ZB - 1) / ZB;
   // tile t of this launch is tile xt0 + t of the substep (the x stage of a
@@ -901,7 +929,7 @@ struct Launch {
   template <bool ZS, bool VS>
   static void xphys_zs(const Dev &d, int rk, int do_cfl, int do_diag, cudaStream_t s) {
     const int ntiles = d.xnt > 0 ? d.xnt : d.my * ((d.mgalz + G::ZB - 1) / G::ZB);
-    constexpr int XT = XGeo<N1, N2, ZS || VS>::XT;
+    constexpr int XT = XGeo<N1, N2, ZS || VS, sizeof(CT) == sizeof(float2)>::XT;
     const void *fn = (const void *)k_xphys<N1, N2, CT, ST, ZS, VS>;
     // stage the input rows (TMA, one tile ahead) where that keeps as many
     // blocks per SM as reading them in the first transform pass would

@@ -127,6 +127,9 @@ struct Stats {
 };
 constexpr int NSTAT = 33;
 constexpr int XGRP = 32;  // z-tile groups of the physical-space sums
+// warps of an x-stage block at most: the mixed form's partial-sum slots
+// (Dev::mpart) hold one value per (z tile, warp)
+constexpr int XW_MAX = 9;
 enum {
   ST_UM = 0, ST_VM, ST_WM, ST_RUM, ST_RVM, ST_RWM, ST_TM, ST_W1M, ST_W2M, ST_W3M, ST_THEM,
   ST_UP, ST_VP, ST_WP, ST_UVR, ST_UWR, ST_VWR, ST_W1P, ST_W2P, ST_W3P, ST_TP, ST_EP,
