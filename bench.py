@@ -103,7 +103,7 @@ ALGO = {
 # not captured for that kernel.
 NCU_TRAFFIC = {
     # 768^2 x 33 (mgal 1152^2), mu = T^0.7 + scalar: profiles/kernels_transforms_large_768x33x768.md
-    ("large", False, 1, 1): {"xphys": (4.9096e9, 33)},
+    ("large", False, 1, 1): {"xphys": (5.0270e9, 33)},
     ("large", True, 1, 1): {"xphys": (8.3872e9, 33)},
     # 256^2 x 65 (mgal 384^2), mu = T^0.7 + scalar: profiles/kernels_xphys_mu07_scalar_256x65x256.md
     ("medium", False, 1, 1): {"xphys": (1026.2e6, 65)},
