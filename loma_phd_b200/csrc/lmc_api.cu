@@ -984,6 +984,7 @@ int lmc_step_split(lmc_handle *h, int nblocks, int nsteps) {
     const int nlines = d.my * d.mgalz, nz = lmc::n_zbuf(d);
     const size_t es = d.prec ? sizeof(float2) : sizeof(double2);
     int p = 0, l = 0;
+    sp.p0.clear(); sp.np.clear(); sp.l0.clear(); sp.nl.clear();  // a failed earlier attempt
     sp.Z.assign(nblocks, {});
     sp.X.assign(nblocks, {});
     for (int r = 0; r < nblocks; r++) {
