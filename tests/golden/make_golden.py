@@ -1,8 +1,11 @@
 """Regenerate the fixtures of tests/golden/ from the reference's own files:
-fft_rect_double.npz from its FFT golden vectors, and hre_lomacte3.dat /
+fft_rect_double.npz from its FFT golden vectors, hre_lomacte3.dat /
 hre_lomacte.dat, verbatim copies of the run-parameter files of the two
 lomacte codes (trunk/lomacte3/hre.dat, trunk/lomacte/hre.dat) that
-tests/test_files.py parses as initcr does.
+tests/test_files.py parses as initcr does, and mesh_*.txt, verbatim copies
+of three of the y meshes the reference's initial-condition generator reads
+(trunk/initloma3/data/*.txt, list-directed y(1..my), main.f:726-727) for
+tests/test_reference_meshes.py.
 
 Source (read as text; nothing of the reference is executed):
   Beovulfo/LoMa_phD branches/reactml/benchmark_fft/cfttest_double.txt
@@ -25,6 +28,12 @@ import os
 import sys
 
 import numpy as np
+
+
+# y meshes of the reference: a symmetric s = 8 mesh (453 points), the
+# stretched mesh of the Pantano case (387) and an 801-point mesh whose last
+# point stops short of symmetry
+MESHES = ("meshs8Ly173", "pantanoBmy387", "LOMAmy801")
 
 
 def parse_e14(path):
@@ -54,6 +63,12 @@ def main():
     for code in ("lomacte3", "lomacte"):
         src = os.path.join(root, "trunk", code, "hre.dat")
         dst = os.path.join(here, f"hre_{code}.dat")
+        with open(src, "rb") as f, open(dst, "wb") as g:
+            g.write(f.read())
+        print("wrote", dst)
+    for name in MESHES:
+        src = os.path.join(root, "trunk", "initloma3", "data", name + ".txt")
+        dst = os.path.join(here, f"mesh_{name}.txt")
         with open(src, "rb") as f, open(dst, "wb") as g:
             g.write(f.read())
         print("wrote", dst)
