@@ -1263,11 +1263,14 @@ int lmc_yop_tune(lmc_handle *h, int op, double *out) {
   const size_t n = (size_t)2 * d.nmode * d.my;
   const double2 *in = d.vor;  // the state's Omega_y, device layout
   double *ref = (double *)d.sb[8], *alt = (double *)d.sb[9];
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   double *acc = nullptr;
-  LMC_CK(cudaMallocAsync((void **)&acc, 2 * sizeof(double), h->s));
-  cudaEvent_t e0, e1;
-  LMC_CK(cudaEventCreate(&e0));
-  LMC_CK(cudaEventCreate(&e1));
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+      cudaMallocAsync((void **)&acc, 2 * sizeof(double), h->s) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);  // nothing of a failed set-up is kept
+    if (e1) cudaEventDestroy(e1);
+    return LMC_ECUDA;
+  }
   auto timed = [&](int method) -> double {  // best of three, ms
     float best = 1e30f;
     for (int rep = 0; rep < 3; rep++) {
